@@ -1,0 +1,149 @@
+/*
+ * magtense_b200.h -- C ABI of libmagtense_b200.so, the B200-native micromagnetic
+ * hot path of MagTense (Landau-Lifshitz right-hand side, dense prism demag
+ * tensor, adaptive Runge-Kutta integration).
+ *
+ * Conventions (all as in the reference, MagTense source/MagTenseMicroMag):
+ *  - n = nx*ny*nz cells on a uniform grid, cell index i + j*nx + k*nx*ny.
+ *  - A magnetisation state is one FP64 vector [mx(0..n-1), my(..), mz(..)].
+ *  - "H" arrays are the reference's internal fields, i.e. MINUS the physical
+ *    field (LandauLifshitzEquationSolver.f90:453,494-507,542-544,715-754).
+ *  - alpha is the reference's damping coefficient gamma*alpha_Gilbert.
+ *
+ * Every function returns an int status: 0 on success, a negative MT_ERR_* code
+ * otherwise; nothing here exits, aborts or traps.  mt_last_error() gives a
+ * message for the calling thread's last failure.  Pointers named *_dev are
+ * device pointers (any allocator); everything else is host memory.  Streams
+ * are passed as void* (a cudaStream_t; NULL = legacy default stream).
+ * Distinct handles may be used from different threads concurrently; one handle
+ * must not be used concurrently.
+ */
+#ifndef MAGTENSE_B200_H
+#define MAGTENSE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MT_OK 0
+#define MT_ERR_ARG (-1)          /* invalid argument */
+#define MT_ERR_CUDA (-2)         /* CUDA runtime error */
+#define MT_ERR_NOMEM (-3)        /* device allocation failed */
+#define MT_ERR_STATE (-4)        /* call out of order (e.g. no tensor yet) */
+#define MT_ERR_UNSUPPORTED (-5)  /* feature not on this path */
+#define MT_ERR_SOLVER (-6)       /* integrator stopped (see mt_stats.status) */
+#define MT_ERR_TIMEOUT (-7)      /* a bounded device wait gave up */
+
+typedef struct mt_handle mt_handle;
+
+/* Uniform grid; mirrors MicroMagGrid (MicroMagParameters.f90:57-70). */
+typedef struct {
+    int nx, ny, nz;
+    double Lx, Ly, Lz;
+} mt_grid;
+
+/* Integrator statistics (RKSUITE counters, RKSuitef90.f90:41-100). */
+typedef struct {
+    long long f_evals;     /* right-hand-side evaluations */
+    long long steps;       /* accepted steps */
+    long long bad_steps;   /* rejected steps (after the first step) */
+    long long n_flag3;     /* "too much work" returns (every 5000 evaluations) */
+    long long n_flag4;     /* "problem looks stiff" returns */
+    long long n_out;       /* output samples written */
+    int status;            /* 0 ok; 5 step size underflow; 911 fatal argument */
+    int converged_at;      /* output index where the t_conv test ended the run, -1 if none */
+    long long launches;    /* persistent-kernel launches used */
+    double kernel_ms;      /* device time of those launches (CUDA events on the stream) */
+} mt_stats;
+
+/* ---------------- handle life cycle ---------------- */
+
+/* Replaces the per-process globals of MagTenseCudaBlas.cu:29-92 with a handle.
+ * Allocates nothing on the device yet. */
+int mt_create(const mt_grid* grid, mt_handle** out);
+int mt_destroy(mt_handle* h);
+const char* mt_last_error(void);
+const char* mt_version(void);
+
+/* Per-cell material (loadMicroMagProblem, MagTenseMicroMagPyIO.f90:91-100;
+ * initializeSolution :415-422).  Ms, K0: n values; u_ea: n*3 row-major
+ * (u_ea[i*3+c]); A0 scalar.  Host arrays. */
+int mt_set_material(mt_handle* h, double A0, const double* Ms, const double* K0, const double* u_ea);
+
+/* Time dependence (updateExternalField :485-514, alpha() :281-294).
+ * solver: 1 explicit (field row hext_row, 0-based), 2 dynamic (interpolated).
+ * hext: nt_hext rows of {t, Hx, Hy, Hz} (A/m); alpha_tab: nt_alpha rows of
+ * {t, alpha}, used when alpha0 == 0.  renormalize: rescale each cell's m to
+ * unit length after every accepted step (off in the reference's RKSUITE path). */
+int mt_set_dynamics(mt_handle* h, int solver, double gamma, double alpha0,
+                    const double* alpha_tab, int nt_alpha, const double* hext, int nt_hext,
+                    int hext_row, int renormalize);
+
+/* ---------------- demag tensor ---------------- */
+
+/* Analytical prism tensor of every (receiver, source) pair, FP64 on the GPU and
+ * rounded to FP32 (ComputeDemagfieldTensor uniform branch,
+ * LandauLifshitzEquationSolver.f90:883-986; getN_prism_3D,
+ * TileNComponents.f90:629-724). */
+int mt_assemble_demag(mt_handle* h, void* stream);
+
+/* Reference layout in/out: six column-major n*n FP32 blocks Kxx Kxy Kxz Kyy Kyz
+ * Kzz, K(:,src) = field at every receiver from source src (host memory).  This
+ * is the record layout of writeDemagTensorToDisk/loadDemagTensorFromDisk
+ * (MagTenseMicroMagPyIO.f90:221-271). */
+int mt_load_demag_colmajor(mt_handle* h, const float* Kxx, const float* Kxy, const float* Kxz,
+                           const float* Kyy, const float* Kyz, const float* Kzz);
+int mt_get_demag_colmajor(mt_handle* h, float* Kxx, float* Kxy, float* Kxz,
+                          float* Kyy, float* Kyz, float* Kzz);
+
+/* ---------------- fields and right-hand side ---------------- */
+
+/* Internal demag field Hm = Ms * (-K m) with m rounded to FP32 and an FP32
+ * product (updateDemagfield dense branch :706-767).  m_dev, H_dev: 3n FP64. */
+int mt_demag_field(mt_handle* h, const double* m_dev, double* H_dev, void* stream);
+
+/* All four internal field terms at time t (StoreHeffComponents :306-349). */
+int mt_fields(mt_handle* h, double t, const double* m_dev, double* Hj_dev, double* Hh_dev,
+              double* Hk_dev, double* Hm_dev, void* stream);
+
+/* dm/dt of the Landau-Lifshitz equation (dmdt_fct :220-273). */
+int mt_rhs(mt_handle* h, double t, const double* m_dev, double* dmdt_dev, void* stream);
+
+/* ---------------- time integration ---------------- */
+
+/* MagTense_ODE_RKSuite (ODE_Solvers.f90:124-237) driving RKSUITE-90 method 'M'
+ * (RKSuitef90.f90), executed on the device by one persistent cooperative
+ * kernel.  t: nt requested output times (host); m0_dev: 3n FP64; y_out_dev:
+ * nt*3n FP64 (sample k at y_out_dev + k*3n); t_out, flags: nt host values (the
+ * time each sample was taken at, and the RKSUITE flag of the call that produced
+ * it: 1 normal, 3/4 warning return before t_want was reached).  t_conv: times
+ * at which max|m - m_last| < conv_tol stops the run (ODE_Solvers.f90:210-222).
+ * Blocks the calling thread until done. */
+int mt_integrate(mt_handle* h, const double* t, int nt, const double* m0_dev, double tol,
+                 double thres, const double* t_conv, int nt_conv, double conv_tol,
+                 double* t_out, double* y_out_dev, int* flags, mt_stats* stats, void* stream);
+
+/* ---------------- reference compatibility shims ---------------- */
+/* Exact signatures of the reference's C shim (MagTenseCudaBlasICLWrapper.cxx:13-59,
+ * bound from Fortran in FortranCuda.f90:15-60).  They act on one process-wide
+ * problem like the reference, but return a status instead of exiting. */
+
+/* replaces cu_initDemagMatrices (MagTenseCudaBlas.cu:306-352) */
+int icl_initDemagMatrices(const float* Kxx, const float* Kxy, const float* Kxz,
+                          const float* Kyy, const float* Kyz, const float* Kzz, int* n);
+/* replaces cu_MVMult_GetH (MagTenseCudaBlas.cu:367-407): H = pref * K * M, FP32 host vectors */
+int icl_MVMult_GetH(const float* Mx, const float* My, const float* Mz, float* Hx, float* Hy,
+                    float* Hz, int* n, float* pref);
+/* replaces cu_destroy (MagTenseCudaBlas.cu:420-497) */
+int icl_destroy(void);
+/* replace cu_initDemagMatrices_sparse / cu_MVMult_GetH_sparse (MagTenseCudaBlas.cu:106-297):
+ * thresholded-sparse demag is not on this path; they return MT_ERR_UNSUPPORTED. */
+int icl_initDemagMatrices_sparse(int* n, int* nnz, int* mat_no, float* values, int* colInds,
+                                 int* rowInds);
+int icl_MVMult_GetH_sparse(const float* Mx, const float* My, const float* Mz, float* Hx, float* Hy,
+                           float* Hz, const int* n, const float* pref);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MAGTENSE_B200_H */

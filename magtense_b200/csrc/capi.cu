@@ -1,0 +1,555 @@
+// extern "C" entry points of libmagtense_b200.so (declared in include/magtense_b200.h).
+//
+// A handle replaces the process-wide state of the reference's CUDA shim
+// (MagTenseCudaBlas.cu:29-92): it owns the device copy of the demag tensor,
+// the per-cell material vectors and the integrator workspace.  The caller owns
+// every m / H / output device buffer.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "../../include/magtense_b200.h"
+#include "common.cuh"
+#include "fields.cuh"
+#include "integrate.cuh"
+#include "llg.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                              \
+    do {                                                                                            \
+        cudaError_t _e = (expr);                                                                    \
+        if (_e != cudaSuccess)                                                                      \
+            return fail(_e == cudaErrorMemoryAllocation ? MT_ERR_NOMEM : MT_ERR_CUDA, "%s: %s (%s:%d)", \
+                        #expr, cudaGetErrorString(_e), __FILE__, __LINE__);                         \
+    } while (0)
+
+const double kMu0 = 4.0 * 3.141592653589793 * 1e-7;   // (4*pi)*1e-7 as the reference evaluates it
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc((void**)p, sizeof(T) * count);
+}
+
+}  // namespace
+
+struct mt_handle {
+    int nx = 0, ny = 0, nz = 0, n = 0, ldk = 0;
+    double L[3] = {0, 0, 0}, d[3] = {0, 0, 0};
+    int device = 0, num_sms = 0;
+    // material
+    double* Jfact = nullptr; double* Kfact = nullptr; float* Mfact = nullptr; double* A6 = nullptr;
+    bool have_material = false;
+    // dynamics
+    int solver = 2; double gamma = 0.0, alpha0 = 0.0; int hext_row = 0; int renorm = 0;
+    double* hext = nullptr; int nt_hext = 0; double* alpha_tab = nullptr; int nt_alpha = 0;
+    bool have_dynamics = false;
+    // tensor
+    float* K = nullptr; bool have_K = false;
+    // scratch
+    float* m32 = nullptr;
+};
+
+namespace {
+
+void free_ptr(void* p)
+{
+    if (p) cudaFree(p);
+}
+
+void axis_setup(int nn, double L, double* d)
+{
+    *d = (nn > 1) ? L / nn : L;
+}
+
+DevProb make_prob(const mt_handle* h)
+{
+    DevProb P;
+    memset(&P, 0, sizeof(P));
+    P.n = h->n; P.nx = h->nx; P.ny = h->ny; P.nz = h->nz; P.ldk = h->ldk;
+    P.K = h->K;
+    const int nn[3] = {h->nx, h->ny, h->nz};
+    for (int a = 0; a < 3; ++a) {
+        const double d2 = h->d[a] * h->d[a];
+        P.lapc[a] = 1.0 / d2;
+        P.diag_b[a] = nn[a] > 1 ? -1.0 / d2 : 0.0;
+        P.diag_i[a] = nn[a] > 1 ? -2.0 / d2 : 0.0;
+    }
+    P.Jfact = h->Jfact; P.Kfact = h->Kfact; P.Mfact = h->Mfact; P.A6 = h->A6;
+    P.solver = h->solver; P.hext_row = h->hext_row; P.nt_hext = h->nt_hext; P.nt_alpha = h->nt_alpha;
+    P.hext = h->hext; P.alpha_tab = h->alpha_tab;
+    P.gamma = h->gamma; P.alpha0 = h->alpha0;
+    return P;
+}
+
+int check_ready(const mt_handle* h, bool need_material, bool need_dynamics)
+{
+    if (!h) return fail(MT_ERR_ARG, "null handle");
+    if (!h->have_K) return fail(MT_ERR_STATE, "no demag tensor: call mt_assemble_demag or mt_load_demag_colmajor first");
+    if (need_material && !h->have_material) return fail(MT_ERR_STATE, "no material: call mt_set_material first");
+    if (need_dynamics && !h->have_dynamics) return fail(MT_ERR_STATE, "no dynamics: call mt_set_dynamics first");
+    return MT_OK;
+}
+
+int ensure_tensor(mt_handle* h)
+{
+    if (h->K) return MT_OK;
+    const size_t cnt = (size_t)h->n * 6 * (size_t)h->ldk;
+    CUDA_TRY(dalloc(&h->K, cnt));
+    return MT_OK;
+}
+
+int ensure_m32(mt_handle* h)
+{
+    if (h->m32) return MT_OK;
+    CUDA_TRY(dalloc(&h->m32, 3 * (size_t)h->ldk));
+    return MT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* mt_last_error(void) { return g_last_error.c_str(); }
+const char* mt_version(void) { return "magtense_b200 0.1 (sm_100a)"; }
+
+int mt_create(const mt_grid* g, mt_handle** out)
+{
+    if (!g || !out) return fail(MT_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (g->nx < 1 || g->ny < 1 || g->nz < 1) return fail(MT_ERR_ARG, "grid counts must be >= 1");
+    const long long n = (long long)g->nx * g->ny * g->nz;
+    if (n > 200000) return fail(MT_ERR_ARG, "n = %lld cells exceeds the dense-tensor limit", n);
+    if (!(g->Lx > 0 && g->Ly > 0 && g->Lz > 0)) return fail(MT_ERR_ARG, "grid extents must be > 0");
+    mt_handle* h = new mt_handle();
+    h->nx = g->nx; h->ny = g->ny; h->nz = g->nz; h->n = (int)n;
+    h->ldk = (int)((n + 3) & ~3LL);
+    h->L[0] = g->Lx; h->L[1] = g->Ly; h->L[2] = g->Lz;
+    axis_setup(g->nx, g->Lx, &h->d[0]);
+    axis_setup(g->ny, g->Ly, &h->d[1]);
+    axis_setup(g->nz, g->Lz, &h->d[2]);
+    cudaError_t e = cudaGetDevice(&h->device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device);
+    if (e == cudaSuccess) e = integrate_upload_tables();
+    if (e != cudaSuccess) {
+        delete h;
+        return fail(MT_ERR_CUDA, "CUDA init: %s", cudaGetErrorString(e));
+    }
+    *out = h;
+    return MT_OK;
+}
+
+int mt_destroy(mt_handle* h)
+{
+    if (!h) return MT_OK;
+    free_ptr(h->Jfact); free_ptr(h->Kfact); free_ptr(h->Mfact); free_ptr(h->A6);
+    free_ptr(h->hext); free_ptr(h->alpha_tab); free_ptr(h->K); free_ptr(h->m32);
+    delete h;
+    return MT_OK;
+}
+
+int mt_set_material(mt_handle* h, double A0, const double* Ms, const double* K0, const double* u_ea)
+{
+    if (!h || !Ms || !K0 || !u_ea) return fail(MT_ERR_ARG, "null argument");
+    const int n = h->n;
+    std::vector<double> jf(n), kf(n), a6(6 * (size_t)n);
+    std::vector<float> mf(n);
+    for (int i = 0; i < n; ++i) {
+        if (!(Ms[i] != 0.0) || !std::isfinite(Ms[i])) return fail(MT_ERR_ARG, "Ms[%d] must be finite and nonzero", i);
+        jf[i] = A0 / (kMu0 * Ms[i]);
+        kf[i] = K0[i] / (kMu0 * Ms[i]);
+        mf[i] = (float)Ms[i];
+        const double ux = u_ea[i * 3 + 0], uy = u_ea[i * 3 + 1], uz = u_ea[i * 3 + 2];
+        a6[0 * (size_t)n + i] = ux * ux; a6[1 * (size_t)n + i] = ux * uy; a6[2 * (size_t)n + i] = ux * uz;
+        a6[3 * (size_t)n + i] = uy * uy; a6[4 * (size_t)n + i] = uy * uz; a6[5 * (size_t)n + i] = uz * uz;
+    }
+    if (!h->Jfact) {
+        CUDA_TRY(dalloc(&h->Jfact, n)); CUDA_TRY(dalloc(&h->Kfact, n));
+        CUDA_TRY(dalloc(&h->Mfact, n)); CUDA_TRY(dalloc(&h->A6, 6 * (size_t)n));
+    }
+    CUDA_TRY(cudaMemcpy(h->Jfact, jf.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->Kfact, kf.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->Mfact, mf.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->A6, a6.data(), sizeof(double) * 6 * (size_t)n, cudaMemcpyHostToDevice));
+    h->have_material = true;
+    return MT_OK;
+}
+
+int mt_set_dynamics(mt_handle* h, int solver, double gamma, double alpha0, const double* alpha_tab, int nt_alpha,
+                    const double* hext, int nt_hext, int hext_row, int renormalize)
+{
+    if (!h) return fail(MT_ERR_ARG, "null handle");
+    if (solver != 1 && solver != 2) return fail(MT_ERR_UNSUPPORTED, "solver %d: only explicit (1) and dynamic (2)", solver);
+    if (nt_hext < 0 || nt_alpha < 0) return fail(MT_ERR_ARG, "negative table length");
+    if (nt_hext > 0 && !hext) return fail(MT_ERR_ARG, "null hext table");
+    if (nt_alpha > 0 && !alpha_tab) return fail(MT_ERR_ARG, "null alpha table");
+    if (solver == 1 && (hext_row < 0 || hext_row >= nt_hext))
+        return fail(MT_ERR_ARG, "hext_row %d outside the table (%d rows)", hext_row, nt_hext);
+    free_ptr(h->hext); h->hext = nullptr;
+    free_ptr(h->alpha_tab); h->alpha_tab = nullptr;
+    CUDA_TRY(dalloc(&h->hext, 4 * (size_t)std::max(nt_hext, 1)));
+    CUDA_TRY(dalloc(&h->alpha_tab, 2 * (size_t)std::max(nt_alpha, 1)));
+    CUDA_TRY(cudaMemset(h->hext, 0, sizeof(double) * 4 * std::max(nt_hext, 1)));
+    CUDA_TRY(cudaMemset(h->alpha_tab, 0, sizeof(double) * 2 * std::max(nt_alpha, 1)));
+    if (nt_hext > 0) CUDA_TRY(cudaMemcpy(h->hext, hext, sizeof(double) * 4 * nt_hext, cudaMemcpyHostToDevice));
+    if (nt_alpha > 0) CUDA_TRY(cudaMemcpy(h->alpha_tab, alpha_tab, sizeof(double) * 2 * nt_alpha, cudaMemcpyHostToDevice));
+    h->solver = solver; h->gamma = gamma; h->alpha0 = alpha0; h->nt_alpha = nt_alpha; h->nt_hext = nt_hext;
+    h->hext_row = hext_row; h->renorm = renormalize ? 1 : 0;
+    h->have_dynamics = true;
+    return MT_OK;
+}
+
+int mt_assemble_demag(mt_handle* h, void* stream)
+{
+    if (!h) return fail(MT_ERR_ARG, "null handle");
+    int rc = ensure_tensor(h);
+    if (rc) return rc;
+    CUDA_TRY(launch_assemble(h->nx, h->ny, h->nz, h->L, h->d, h->n, h->ldk, h->K, (cudaStream_t)stream));
+    h->have_K = true;
+    return MT_OK;
+}
+
+int mt_load_demag_colmajor(mt_handle* h, const float* Kxx, const float* Kxy, const float* Kxz, const float* Kyy,
+                           const float* Kyz, const float* Kzz)
+{
+    if (!h || !Kxx || !Kxy || !Kxz || !Kyy || !Kyz || !Kzz) return fail(MT_ERR_ARG, "null argument");
+    int rc = ensure_tensor(h);
+    if (rc) return rc;
+    const float* blocks[6] = {Kxx, Kxy, Kxz, Kyy, Kyz, Kzz};
+    float* tmp = nullptr;
+    const size_t nn = (size_t)h->n * h->n;
+    CUDA_TRY(dalloc(&tmp, nn));
+    for (int c = 0; c < 6; ++c) {
+        cudaError_t e = cudaMemcpy(tmp, blocks[c], sizeof(float) * nn, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = launch_colmajor_to_rows(tmp, c, h->n, h->ldk, h->K, 0);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) { cudaFree(tmp); return fail(MT_ERR_CUDA, "tensor upload: %s", cudaGetErrorString(e)); }
+    }
+    cudaFree(tmp);
+    h->have_K = true;
+    return MT_OK;
+}
+
+int mt_get_demag_colmajor(mt_handle* h, float* Kxx, float* Kxy, float* Kxz, float* Kyy, float* Kyz, float* Kzz)
+{
+    if (!h || !Kxx || !Kxy || !Kxz || !Kyy || !Kyz || !Kzz) return fail(MT_ERR_ARG, "null argument");
+    if (!h->have_K) return fail(MT_ERR_STATE, "no demag tensor");
+    float* blocks[6] = {Kxx, Kxy, Kxz, Kyy, Kyz, Kzz};
+    float* tmp = nullptr;
+    const size_t nn = (size_t)h->n * h->n;
+    CUDA_TRY(dalloc(&tmp, nn));
+    for (int c = 0; c < 6; ++c) {
+        cudaError_t e = launch_rows_to_colmajor(h->K, c, h->n, h->ldk, tmp, 0);
+        if (e == cudaSuccess) e = cudaMemcpy(blocks[c], tmp, sizeof(float) * nn, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) { cudaFree(tmp); return fail(MT_ERR_CUDA, "tensor download: %s", cudaGetErrorString(e)); }
+    }
+    cudaFree(tmp);
+    return MT_OK;
+}
+
+int mt_demag_field(mt_handle* h, const double* m_dev, double* H_dev, void* stream)
+{
+    int rc = check_ready(h, true, false);
+    if (rc) return rc;
+    if (!m_dev || !H_dev) return fail(MT_ERR_ARG, "null device pointer");
+    if ((rc = ensure_m32(h))) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    DevProb P = make_prob(h);
+    CUDA_TRY(launch_m_to_f32(m_dev, h->n, h->ldk, h->m32, s));
+    CUDA_TRY(launch_field(0, P, m_dev, h->m32, 0.0, H_dev, nullptr, nullptr, nullptr, nullptr, 0.f, h->num_sms, s));
+    return MT_OK;
+}
+
+int mt_fields(mt_handle* h, double t, const double* m_dev, double* Hj, double* Hh, double* Hk, double* Hm, void* stream)
+{
+    int rc = check_ready(h, true, true);
+    if (rc) return rc;
+    if (!m_dev || !Hj || !Hh || !Hk || !Hm) return fail(MT_ERR_ARG, "null device pointer");
+    if ((rc = ensure_m32(h))) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    DevProb P = make_prob(h);
+    CUDA_TRY(launch_m_to_f32(m_dev, h->n, h->ldk, h->m32, s));
+    CUDA_TRY(launch_field(1, P, m_dev, h->m32, t, Hj, Hh, Hk, Hm, nullptr, 0.f, h->num_sms, s));
+    return MT_OK;
+}
+
+int mt_rhs(mt_handle* h, double t, const double* m_dev, double* dmdt_dev, void* stream)
+{
+    int rc = check_ready(h, true, true);
+    if (rc) return rc;
+    if (!m_dev || !dmdt_dev) return fail(MT_ERR_ARG, "null device pointer");
+    if ((rc = ensure_m32(h))) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    DevProb P = make_prob(h);
+    CUDA_TRY(launch_m_to_f32(m_dev, h->n, h->ldk, h->m32, s));
+    CUDA_TRY(launch_field(2, P, m_dev, h->m32, t, dmdt_dev, nullptr, nullptr, nullptr, nullptr, 0.f, h->num_sms, s));
+    return MT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// integration driver
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+
+struct IntegAlloc {
+    std::vector<void*> ptrs;
+    template <typename T>
+    cudaError_t get(T** p, size_t count)
+    {
+        cudaError_t e = dalloc(p, count);
+        if (e == cudaSuccess) ptrs.push_back((void*)*p);
+        return e;
+    }
+    ~IntegAlloc()
+    {
+        for (void* p : ptrs) cudaFree(p);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+int mt_integrate(mt_handle* h, const double* t, int nt, const double* m0_dev, double tol, double thres,
+                 const double* t_conv, int nt_conv, double conv_tol, double* t_out, double* y_out_dev, int* flags,
+                 mt_stats* stats, void* stream)
+{
+    int rc = check_ready(h, true, true);
+    if (rc) return rc;
+    if (!t || nt < 2 || !m0_dev || !t_out || !y_out_dev || !stats) return fail(MT_ERR_ARG, "bad argument (nt >= 2 required)");
+    if (nt_conv < 0 || (nt_conv > 0 && !t_conv)) return fail(MT_ERR_ARG, "bad convergence-time list");
+    cudaStream_t s = (cudaStream_t)stream;
+    memset(stats, 0, sizeof(*stats));
+    stats->converged_at = -1;
+    const int n = h->n, n3 = 3 * n;
+
+    // ---- setup_r1 checks and initial state (RKSuitef90.f90:596-856) ----
+    const double eps = 2.220446049250313e-16;
+    const double round_off = 10.0 * eps, sqrrmc = sqrt(eps), cubrmc = pow(eps, 1.0 / 3.0);
+    const double sqtiny = sqrt(2.2250738585072014e-308);
+    const double cdiff = 1.0 / 18.0;   // min nonzero |c_i - c_j| of the pair (2/9 - 1/6)
+    const double toosml = round_off / cdiff;
+    const double t_start = t[0], t_end = t[nt - 1];
+    if (t_start == t_end) { stats->status = 911; return fail(MT_ERR_ARG, "T_START = T_END"); }
+    if (tol > 0.01 || tol < round_off) { stats->status = 911; return fail(MT_ERR_ARG, "tol %g outside (%g, 0.01)", tol, round_off); }
+    if (thres < sqtiny) { stats->status = 911; return fail(MT_ERR_ARG, "threshold %g below %g", thres, sqtiny); }
+    const double hmin0 = std::max(sqtiny, toosml * std::max(fabs(t_start), fabs(t_end)));
+    if (fabs(t_end - t_start) < hmin0) { stats->status = 911; return fail(MT_ERR_ARG, "T_END and T_START not distinguishable"); }
+
+    // ---- merged output / convergence times (ODE_Solvers.f90:183-193) ----
+    std::vector<double> comb;
+    comb.reserve(nt + nt_conv);
+    for (int i = 0; i < nt + nt_conv; ++i) {
+        const double v = (i < nt) ? t[i] : t_conv[i - nt];
+        bool dup = (i > 0 && v == 0.0);   // simple_unique compares with its zero-filled output
+        for (double c : comb) if (c == v) { dup = true; break; }
+        if (i == 0 || !dup) comb.push_back(v);
+    }
+    std::sort(comb.begin(), comb.end());
+    std::vector<int> cflags(comb.size(), 0);
+    for (size_t k = 0; k < comb.size(); ++k) {
+        for (int q = 0; q < nt; ++q) if (t[q] == comb[k]) { cflags[k] |= 1; break; }
+        for (int q = 0; q < nt_conv; ++q) if (t_conv[q] == comb[k]) { cflags[k] |= 2; break; }
+    }
+
+    // ---- buffers ----
+    IntegAlloc A;
+    IntegBufs B;
+    memset(&B, 0, sizeof(B));
+    for (int k = 0; k < 4; ++k) {
+        CUDA_TRY(A.get(&B.pool[k], n3));
+        CUDA_TRY(A.get(&B.pool32[k], 3 * (size_t)h->ldk));
+        CUDA_TRY(cudaMemsetAsync(B.pool32[k], 0, sizeof(float) * 3 * h->ldk, s));
+    }
+    for (int k = 0; k < 3; ++k) CUDA_TRY(A.get(&B.deriv[k], n3));
+    for (int k = 2; k <= 11; ++k) if (k != 8) CUDA_TRY(A.get(&B.stg[k], n3));
+    for (int k = 1; k <= 5; ++k) CUDA_TRY(A.get(&B.p[k], n3));
+    CUDA_TRY(A.get(&B.errest, n3));
+    CUDA_TRY(A.get(&B.weights, n3));
+    CUDA_TRY(A.get(&B.ylast, n3));
+    CUDA_TRY(A.get(&B.ystep, n3));
+    B.y_out = y_out_dev;
+    const int grid = integrate_grid_size(n, h->num_sms);
+    CUDA_TRY(A.get(&B.partials, 2 * (size_t)grid * 4));
+    CUDA_TRY(A.get(&B.gs, 1));
+    CUDA_TRY(A.get(&B.state, 1));
+    double* d_comb = nullptr; int* d_cflags = nullptr; double* d_tout = nullptr; int* d_flags = nullptr;
+    CUDA_TRY(A.get(&d_comb, comb.size()));
+    CUDA_TRY(A.get(&d_cflags, comb.size()));
+    CUDA_TRY(A.get(&d_tout, nt));
+    CUDA_TRY(A.get(&d_flags, nt));
+    CUDA_TRY(cudaMemcpyAsync(d_comb, comb.data(), sizeof(double) * comb.size(), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(d_cflags, cflags.data(), sizeof(int) * comb.size(), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemsetAsync(d_tout, 0, sizeof(double) * nt, s));
+    CUDA_TRY(cudaMemsetAsync(d_flags, 0, sizeof(int) * nt, s));
+    // y <- m0 (with its FP32 shadow), first sample, convergence reference
+    CUDA_TRY(cudaMemcpyAsync(B.pool[0], m0_dev, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(launch_m_to_f32(m0_dev, n, h->ldk, B.pool32[0], s));
+    CUDA_TRY(cudaMemcpyAsync(y_out_dev, m0_dev, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(B.ylast, m0_dev, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(cudaMemsetAsync(B.weights, 0, sizeof(double) * n3, s));
+
+    RKS st;
+    memset(&st, 0, sizeof(st));
+    st.t = t_start; st.t_old = t_start; st.t_start = t_start; st.t_end = t_end;
+    st.dir = (t_end - t_start) >= 0 ? 1.0 : -1.0;
+    st.tol = tol;
+    st.h = std::max(fabs(t_end - t_start) / 8.0, hmin0);
+    st.at_t_start = 1; st.phase2 = 1;
+    st.iy = 0; st.iyold = 1; st.ia0 = 2; st.ia1 = 3;
+    st.dyp = 0; st.dypold = 1; st.d8 = 2;
+    st.ci = 1; st.ko = 1;
+    st.converged_at = -1;
+    CUDA_TRY(cudaMemcpyAsync(B.state, &st, sizeof(st), cudaMemcpyHostToDevice, s));
+
+    IntegParams Q;
+    memset(&Q, 0, sizeof(Q));
+    Q.thres = thres; Q.round_off = round_off; Q.sqrrmc = sqrrmc; Q.cubrmc = cubrmc; Q.sqtiny = sqtiny;
+    Q.toosml = toosml; Q.conv_tol = conv_tol;
+    Q.comb_t = d_comb; Q.comb_flags = d_cflags; Q.ncomb = (int)comb.size(); Q.nt = nt;
+    Q.t_out = d_tout; Q.flags_out = d_flags;
+    Q.renorm = h->renorm;
+    {   // about 0.25 s of work per launch
+        const double bytes = 24.0 * (double)n * (double)h->ldk;
+        const double t_eval = bytes / 3.0e12 + 15e-6;
+        long long b = (long long)(0.25 / t_eval);
+        Q.evals_per_launch = std::min(100000LL, std::max(64LL, b));
+    }
+    // co-residency of the persistent grid
+    const size_t smem = integrate_smem_bytes(n, h->ldk, grid);
+    if (smem > 227 * 1024) return fail(MT_ERR_UNSUPPORTED, "integrator shared memory %zu exceeds 227 KB", smem);
+    DevProb P = make_prob(h);
+    RKS hs;
+    long long last_evals = -1;
+    int last_ci = -1;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    CUDA_TRY(cudaEventCreate(&ev0));
+    CUDA_TRY(cudaEventCreate(&ev1));
+    struct EvGuard { cudaEvent_t a, b; ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); } } evg{ev0, ev1};
+    double kernel_ms = 0.0;
+    long long launches = 0;
+    for (;;) {
+        CUDA_TRY(cudaMemsetAsync(B.gs, 0, sizeof(GridSync), s));
+        CUDA_TRY(cudaEventRecord(ev0, s));
+        CUDA_TRY(launch_integrate(P, B, Q, grid, s));
+        CUDA_TRY(cudaEventRecord(ev1, s));
+        GridSync gs_h;
+        CUDA_TRY(cudaMemcpyAsync(&gs_h, B.gs, sizeof(gs_h), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaMemcpyAsync(&hs, B.state, sizeof(hs), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        float ms = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, ev0, ev1));
+        kernel_ms += ms;
+        launches++;
+        stats->launches = launches;
+        stats->kernel_ms = kernel_ms;
+        if (gs_h.err != 0 || gs_h.abort)
+            return fail(MT_ERR_TIMEOUT, "integrator grid barrier gave up (code %d at %d)", gs_h.err, gs_h.err_where);
+        if (hs.finished) break;
+        const long long evals = hs.full_f_count + hs.f_count;
+        if (evals == last_evals && hs.ci == last_ci) return fail(MT_ERR_SOLVER, "integrator made no progress");
+        last_evals = evals;
+        last_ci = hs.ci;
+    }
+    std::vector<int> fl(nt);
+    CUDA_TRY(cudaMemcpy(t_out, d_tout, sizeof(double) * nt, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(fl.data(), d_flags, sizeof(int) * nt, cudaMemcpyDeviceToHost));
+    t_out[0] = t[0];
+    fl[0] = 0;
+    if (flags) memcpy(flags, fl.data(), sizeof(int) * nt);
+    stats->f_evals = hs.full_f_count + hs.f_count;
+    stats->steps = hs.step_count;
+    stats->bad_steps = hs.bad_step_count;
+    stats->n_flag3 = hs.n_flag3;
+    stats->n_flag4 = hs.n_flag4;
+    stats->n_out = hs.ko;
+    stats->status = hs.status;
+    stats->converged_at = hs.converged_at;
+    if (hs.status != 0) return fail(MT_ERR_SOLVER, "integrator stopped with RKSUITE flag %d", hs.status);
+    return MT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// reference compatibility shims (one process-wide problem)
+// ---------------------------------------------------------------------------
+static mt_handle* g_icl = nullptr;
+
+int icl_initDemagMatrices(const float* Kxx, const float* Kxy, const float* Kxz, const float* Kyy, const float* Kyz,
+                          const float* Kzz, int* n)
+{
+    if (!n || *n < 1) return fail(MT_ERR_ARG, "n must be >= 1");
+    if (g_icl) { mt_destroy(g_icl); g_icl = nullptr; }
+    mt_grid g = {*n, 1, 1, 1.0, 1.0, 1.0};
+    int rc = mt_create(&g, &g_icl);
+    if (rc) return rc;
+    rc = mt_load_demag_colmajor(g_icl, Kxx, Kxy, Kxz, Kyy, Kyz, Kzz);
+    if (rc) { mt_destroy(g_icl); g_icl = nullptr; }
+    return rc;
+}
+
+int icl_MVMult_GetH(const float* Mx, const float* My, const float* Mz, float* Hx, float* Hy, float* Hz, int* n,
+                    float* pref)
+{
+    if (!g_icl) return fail(MT_ERR_STATE, "icl_initDemagMatrices has not been called");
+    if (!n || *n != g_icl->n || !pref || !Mx || !My || !Mz || !Hx || !Hy || !Hz) return fail(MT_ERR_ARG, "bad argument");
+    mt_handle* h = g_icl;
+    const int nn = h->n;
+    int rc = ensure_m32(h);
+    if (rc) return rc;
+    IntegAlloc A;
+    float *dm = nullptr, *dh = nullptr;
+    CUDA_TRY(A.get(&dm, 3 * (size_t)nn));
+    CUDA_TRY(A.get(&dh, 3 * (size_t)nn));
+    CUDA_TRY(cudaMemcpy(dm, Mx, sizeof(float) * nn, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(dm + nn, My, sizeof(float) * nn, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(dm + 2 * nn, Mz, sizeof(float) * nn, cudaMemcpyHostToDevice));
+    CUDA_TRY(launch_pack3_f32(dm, dm + nn, dm + 2 * nn, nn, h->ldk, h->m32, 0));
+    DevProb P = make_prob(h);
+    CUDA_TRY(launch_field(3, P, nullptr, h->m32, 0.0, nullptr, nullptr, nullptr, nullptr, dh, *pref, h->num_sms, 0));
+    CUDA_TRY(cudaMemcpy(Hx, dh, sizeof(float) * nn, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(Hy, dh + nn, sizeof(float) * nn, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(Hz, dh + 2 * nn, sizeof(float) * nn, cudaMemcpyDeviceToHost));
+    return MT_OK;
+}
+
+int icl_destroy(void)
+{
+    if (g_icl) { mt_destroy(g_icl); g_icl = nullptr; }
+    return MT_OK;
+}
+
+int icl_initDemagMatrices_sparse(int*, int*, int*, float*, int*, int*)
+{
+    return fail(MT_ERR_UNSUPPORTED, "thresholded-sparse demag is not on this path (dense tensor only)");
+}
+
+int icl_MVMult_GetH_sparse(const float*, const float*, const float*, float*, float*, float*, const int*, const float*)
+{
+    return fail(MT_ERR_UNSUPPORTED, "thresholded-sparse demag is not on this path (dense tensor only)");
+}
+
+}  // extern "C"

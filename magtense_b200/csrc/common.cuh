@@ -1,0 +1,127 @@
+// Shared device helpers: bounded grid barrier, block reductions, cache-global
+// loads, exact (non-contracted) FP64 arithmetic.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define MT_DEV __device__ __forceinline__
+
+// Error codes recorded by kernels in GridSync::err (host maps them to MT_ERR_*).
+enum { KERR_NONE = 0, KERR_BARRIER_TIMEOUT = 1, KERR_BAD_CONFIG = 2 };
+
+// Grid-wide barrier state for the persistent cooperative kernels.  count is
+// reset to 0 by the host before every launch.
+struct GridSync {
+    unsigned int count;
+    unsigned int gen;
+    int abort;
+    int err;
+    int err_where;
+    int pad[3];
+};
+
+MT_DEV unsigned ld_acquire_u32(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+MT_DEV void st_release_u32(unsigned* p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+MT_DEV int ld_volatile_i32(const int* p) { return *(volatile const int*)p; }
+MT_DEV uint64_t globaltimer_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Barrier across all CTAs of a cooperative launch.  Every wait is bounded: after
+// kSpinLimit polls or kTimeoutNs nanoseconds the waiting CTA records
+// KERR_BARRIER_TIMEOUT, raises abort and returns false; CTAs that see abort
+// return false at once.  Returns true when all CTAs arrived.
+constexpr long long kSpinLimit = 20000000LL;
+constexpr uint64_t kTimeoutNs = 4000000000ULL;
+
+MT_DEV bool grid_sync(GridSync* gs, int where)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        if (ld_volatile_i32(&gs->abort)) {
+            ok = 0;
+        } else {
+            unsigned g = ld_acquire_u32(&gs->gen);
+            __threadfence();
+            unsigned prev = atomicAdd(&gs->count, 1u);
+            if (prev == gridDim.x - 1) {
+                atomicExch(&gs->count, 0u);
+                __threadfence();
+                st_release_u32(&gs->gen, g + 1u);
+            } else {
+                long long it = 0;
+                uint64_t t0 = globaltimer_ns();
+                while (ld_acquire_u32(&gs->gen) == g) {
+                    if (ld_volatile_i32(&gs->abort)) { ok = 0; break; }
+                    if (++it > kSpinLimit || (it & 1023) == 0 && globaltimer_ns() - t0 > kTimeoutNs) {
+                        if (atomicCAS(&gs->err, 0, KERR_BARRIER_TIMEOUT) == 0) gs->err_where = where;
+                        atomicExch(&gs->abort, 1);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
+            __threadfence();
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Block-wide reductions; the result is returned to every thread.  scratch must
+// hold 32 doubles.  Deterministic (fixed tree).
+MT_DEV double warp_max(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+MT_DEV double warp_sum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+template <bool IsMax>
+MT_DEV double block_reduce(double v, double* scratch)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    v = IsMax ? warp_max(v) : warp_sum(v);
+    __syncthreads();
+    if (lane == 0) scratch[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        double w = (lane < nw) ? scratch[lane] : (IsMax ? -1.0 : 0.0);
+        if (IsMax && lane >= nw) w = scratch[0];
+        w = IsMax ? warp_max(w) : warp_sum(w);
+        if (lane == 0) scratch[0] = w;
+    }
+    __syncthreads();
+    double r = scratch[0];
+    __syncthreads();
+    return r;
+}
+
+// Exact IEEE double arithmetic with no FMA contraction, so that elementwise
+// results match a CPU evaluation of the same expression bit for bit.
+MT_DEV double xmul(double a, double b) { return __dmul_rn(a, b); }
+MT_DEV double xadd(double a, double b) { return __dadd_rn(a, b); }
+MT_DEV double xsub(double a, double b) { return __dsub_rn(a, b); }
+
+MT_DEV double ldcg(const double* p) { return __ldcg(p); }
+MT_DEV float ldcg(const float* p) { return __ldcg(p); }
+
+static inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }

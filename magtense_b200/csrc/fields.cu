@@ -1,0 +1,123 @@
+// Stand-alone (non-persistent) field kernels behind mt_demag_field, mt_fields,
+// mt_rhs and icl_MVMult_GetH.  One CTA owns a few receiver cells and streams
+// their tensor records (demag_cta in llg.cuh), then applies the per-cell
+// epilogue.
+#include "common.cuh"
+#include "llg.cuh"
+#include "fields.cuh"
+
+namespace {
+
+// m (3n FP64) -> FP32 [3][ldk] with zero padding (updateDemagfield :576-578)
+__global__ void m_to_f32_kernel(const double* __restrict__ m, int n, int ldk, float* __restrict__ m32)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 3 * ldk) return;
+    const int a = e / ldk, i = e - a * ldk;
+    m32[e] = (i < n) ? (float)m[(size_t)a * n + i] : 0.0f;
+}
+
+// three FP32 host-layout vectors -> [3][ldk]
+__global__ void pack3_f32_kernel(const float* __restrict__ x, const float* __restrict__ y,
+                                 const float* __restrict__ z, int n, int ldk, float* __restrict__ m32)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 3 * ldk) return;
+    const int a = e / ldk, i = e - a * ldk;
+    const float* src = a == 0 ? x : (a == 1 ? y : z);
+    m32[e] = (i < n) ? src[i] : 0.0f;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kFieldThreads)
+field_kernel(DevProb P, const double* __restrict__ m, const float* __restrict__ m32, double t, int cells_per_cta,
+             double* o0, double* o1, double* o2, double* o3, float* h32, float pref)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int JC = P.ldk < kDemagJC ? P.ldk : kDemagJC;
+    float* sm_m = reinterpret_cast<float*>(smem);
+    float* sm_part = sm_m + 3 * JC;
+    float* sm_S = sm_part + 3 * kDemagMaxUnits;
+    const int c0 = blockIdx.x * cells_per_cta;
+    const int nc = min(cells_per_cta, P.n - c0);
+    if (nc <= 0) return;
+    demag_cta(P, m32, c0, nc, sm_m, sm_part, sm_S);
+    const int n = P.n;
+    if (MODE == 3) {   // raw product H = pref * K m (FP32), reference shim
+        for (int e = threadIdx.x; e < 3 * nc; e += blockDim.x) {
+            const int cell = e / 3, a = e - cell * 3;
+            h32[(size_t)a * n + c0 + cell] = __fmul_rn(pref, sm_S[e]);
+        }
+        return;
+    }
+    const TimeScalars ts = time_scalars(P, t);
+    for (int cell = threadIdx.x; cell < nc; cell += blockDim.x) {
+        const int i = c0 + cell;
+        if (MODE == 0) {
+            const float ms = __ldg(&P.Mfact[i]);
+            for (int a = 0; a < 3; ++a) o0[(size_t)a * n + i] = (double)__fmul_rn(-sm_S[cell * 3 + a], ms);
+        } else if (MODE == 1) {
+            CellFields F = cell_fields(P, m, i, &sm_S[cell * 3], ts);
+            for (int a = 0; a < 3; ++a) {
+                o0[(size_t)a * n + i] = F.hj[a];
+                o1[(size_t)a * n + i] = F.hh[a];
+                o2[(size_t)a * n + i] = F.hk[a];
+                o3[(size_t)a * n + i] = F.hm[a];
+            }
+        } else {
+            double o[3];
+            cell_rhs(P, m, i, &sm_S[cell * 3], ts, o);
+            for (int a = 0; a < 3; ++a) o0[(size_t)a * n + i] = o[a];
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_m_to_f32(const double* m, int n, int ldk, float* m32, cudaStream_t s)
+{
+    const int tot = 3 * ldk;
+    m_to_f32_kernel<<<(tot + 255) / 256, 256, 0, s>>>(m, n, ldk, m32);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack3_f32(const float* x, const float* y, const float* z, int n, int ldk, float* m32,
+                             cudaStream_t s)
+{
+    const int tot = 3 * ldk;
+    pack3_f32_kernel<<<(tot + 255) / 256, 256, 0, s>>>(x, y, z, n, ldk, m32);
+    return cudaGetLastError();
+}
+
+int field_cells_per_cta(int n, int num_sms)
+{
+    int target = 2 * num_sms;
+    int c = (n + target - 1) / target;
+    if (c < 1) c = 1;
+    if (c > 1024) c = 1024;
+    return c;
+}
+
+cudaError_t launch_field(int mode, const DevProb& P, const double* m, const float* m32, double t, double* o0,
+                         double* o1, double* o2, double* o3, float* h32, float pref, int num_sms, cudaStream_t s)
+{
+    const int cpc = field_cells_per_cta(P.n, num_sms);
+    const int grid = (P.n + cpc - 1) / cpc;
+    const size_t smem = demag_smem_bytes(P.ldk, cpc);
+    cudaError_t e = cudaSuccess;
+#define MT_LAUNCH(M)                                                                                       \
+    do {                                                                                                   \
+        e = cudaFuncSetAttribute(field_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        if (e != cudaSuccess) return e;                                                                    \
+        field_kernel<M><<<grid, kFieldThreads, smem, s>>>(P, m, m32, t, cpc, o0, o1, o2, o3, h32, pref);   \
+    } while (0)
+    switch (mode) {
+        case 0: MT_LAUNCH(0); break;
+        case 1: MT_LAUNCH(1); break;
+        case 2: MT_LAUNCH(2); break;
+        case 3: MT_LAUNCH(3); break;
+        default: return cudaErrorInvalidValue;
+    }
+#undef MT_LAUNCH
+    return cudaGetLastError();
+}

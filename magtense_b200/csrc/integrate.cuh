@@ -1,0 +1,57 @@
+// Shared declarations of the persistent integrator (integrate.cu) and its host driver (capi.cu).
+#pragma once
+#include "common.cuh"
+#include "llg.cuh"
+
+constexpr int kIntegThreads = 512;
+
+// Scalar state of RKSUITE (rk_comm_real_1d, RKSuitef90.f90:41-100) plus the
+// output driver position.  Kept identical in every thread of the persistent
+// kernel and stored in global memory between launches.
+struct RKS {
+    double t, t_old, t_start, t_end, dir, h, h_old, h_average, tol, errold, tlast, range_t_end;
+    long long f_count, full_f_count, step_count, bad_step_count, stiff_bad_step_count;
+    long long n_flag3, n_flag4;
+    int at_t_start, at_t_end, phase2, chkeff, hit_t_end_count, intrp_ready;
+    int iy, iyold, ia0, ia1;       // roles of the four state/argument buffers
+    int dyp, dypold, d8;           // roles of the three derivative buffers
+    int in_range;                  // a range_integrate call is in progress
+    int ci;                        // next entry of the merged output-time list
+    int ko;                        // next output slot
+    int finished, status, converged_at;
+};
+
+struct IntegBufs {
+    double* pool[4];       // 3n FP64: y, y_old and two stage-argument buffers (rotating)
+    float* pool32[4];      // FP32 shadows [3][ldk] of pool (demag product input)
+    double* deriv[3];      // 3n FP64: yp, yp_old, stage 8 (rotating)
+    double* stg[12];       // stages 2..7 and 9..11 (index = stage number)
+    double* p[6];          // interpolant coefficients 1..5
+    double* errest;
+    double* weights;
+    double* ylast;         // last sample checked for convergence
+    double* ystep;         // sample buffer when the sample is not stored
+    double* y_out;         // nt * 3n
+    double* partials;      // 2 * grid * 4 reduction partials
+    GridSync* gs;
+    RKS* state;
+};
+
+struct IntegParams {
+    double thres;
+    double round_off, sqrrmc, cubrmc, sqtiny, toosml;
+    double conv_tol;
+    const double* comb_t;      // merged, unique, sorted output + convergence times
+    const int* comb_flags;     // bit 0: store sample, bit 1: convergence check
+    int ncomb, nt;
+    double* t_out;             // device, nt
+    int* flags_out;            // device, nt
+    long long evals_per_launch;
+    int renorm;
+};
+
+cudaError_t integrate_upload_tables();
+int integrate_grid_size(int n, int num_sms);
+size_t integrate_smem_bytes(int n, int ldk, int grid);
+cudaError_t launch_integrate(const DevProb& P, const IntegBufs& B, const IntegParams& Q, int grid,
+                             cudaStream_t stream);

@@ -1,0 +1,174 @@
+"""Device-side solver object: one handle of libmagtense_b200.so plus torch-owned buffers.
+
+PyTorch provides device memory and streams; all arithmetic runs in the
+library's sm_100a kernels.  Vectors follow the reference layout
+``[mx(0..n-1), my, mz]`` in FP64 (LandauLifshitzEquationSolver.f90:121,234-236).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check
+
+MU0 = 4 * np.pi * 1e-7
+
+
+def _stream(stream=None):
+    s = torch.cuda.current_stream() if stream is None else stream
+    return C.c_void_p(s.cuda_stream)
+
+
+def _dptr(t: torch.Tensor):
+    return C.c_void_p(t.data_ptr())
+
+
+def _np_d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def grid_points(res, grid_L) -> np.ndarray:
+    """Cell centres (n, 3), x fastest (setupGrid, LandauLifshitzEquationSolver.f90:815-872)."""
+    nx, ny, nz = (int(v) for v in res)
+    axes = []
+    for nn, L in zip((nx, ny, nz), grid_L):
+        if nn > 1:
+            d = L / nn
+            axes.append(np.array([(-(L / 2.0) + i * d) + d / 2.0 for i in range(nn)]))
+        else:
+            axes.append(np.zeros(1))
+    X = np.empty((nz, ny, nx, 3))
+    X[..., 0] = axes[0][None, None, :]
+    X[..., 1] = axes[1][None, :, None]
+    X[..., 2] = axes[2][:, None, None]
+    return X.reshape(nx * ny * nz, 3)
+
+
+class Solver:
+    """Uniform-grid micromagnetic problem resident on one GPU."""
+
+    def __init__(self, res, grid_L, *, A0=1.3e-11, Ms=8e5, K0=0.0, u_ea=None, device=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("magtense_b200 needs a CUDA device (no CPU path exists)")
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        nx, ny, nz = (int(v) for v in res)
+        self.res = (nx, ny, nz)
+        self.grid_L = tuple(float(v) for v in grid_L)
+        self.n = nx * ny * nz
+        L = _lib.lib()
+        g = _lib.Grid(nx, ny, nz, *self.grid_L)
+        h = C.c_void_p()
+        with torch.cuda.device(self.device):
+            check(L.mt_create(C.byref(g), C.byref(h)), "mt_create")
+        self._h = h
+        self.set_material(A0, Ms, K0, u_ea)
+        self._have_tensor = False
+
+    # ---------------------------------------------------------------- setup
+    def set_material(self, A0, Ms, K0, u_ea=None):
+        n = self.n
+        self.A0 = float(A0)
+        self.Ms = _np_d(np.broadcast_to(np.asarray(Ms, dtype=np.float64), (n,)))
+        self.K0 = _np_d(np.broadcast_to(np.asarray(K0, dtype=np.float64), (n,)))
+        self.u_ea = np.zeros((n, 3)) if u_ea is None else _np_d(np.asarray(u_ea, dtype=np.float64).reshape(n, 3))
+        check(_lib.lib().mt_set_material(self._h, self.A0, self.Ms.ctypes.data_as(_lib.D),
+                                         self.K0.ctypes.data_as(_lib.D), self.u_ea.ctypes.data_as(_lib.D)),
+              "mt_set_material")
+
+    def set_dynamics(self, *, solver=2, gamma=0.0, alpha=0.0, alpha_tab=None, hext=None, hext_row=0,
+                     renormalize=False):
+        at = np.zeros((1, 2)) if alpha_tab is None else _np_d(alpha_tab).reshape(-1, 2)
+        he = np.zeros((2, 4)) if hext is None else _np_d(hext).reshape(-1, 4)
+        self._tables = (at, he)
+        check(_lib.lib().mt_set_dynamics(self._h, int(solver), float(gamma), float(alpha),
+                                         at.ctypes.data_as(_lib.D), at.shape[0], he.ctypes.data_as(_lib.D),
+                                         he.shape[0], int(hext_row), int(bool(renormalize))), "mt_set_dynamics")
+
+    def assemble(self, stream=None):
+        """FP64 analytical prism tensor of every cell pair, stored FP32 on the device."""
+        with torch.cuda.device(self.device):
+            check(_lib.lib().mt_assemble_demag(self._h, _stream(stream)), "mt_assemble_demag")
+        self._have_tensor = True
+
+    def load_tensor_colmajor(self, blocks):
+        """Six (n, n) FP32 blocks Kxx Kxy Kxz Kyy Kyz Kzz, K[:, src] column-major as the reference."""
+        bl = [np.asfortranarray(np.asarray(b, dtype=np.float32).reshape(self.n, self.n)) for b in blocks]
+        ptrs = [b.ctypes.data_as(_lib.F) for b in bl]
+        with torch.cuda.device(self.device):
+            check(_lib.lib().mt_load_demag_colmajor(self._h, *ptrs), "mt_load_demag_colmajor")
+        self._have_tensor = True
+
+    def get_tensor_colmajor(self):
+        """The six FP32 blocks as (n, n) arrays with K[i, j] = field at receiver i from source j."""
+        out = [np.empty((self.n, self.n), dtype=np.float32, order="F") for _ in range(6)]
+        with torch.cuda.device(self.device):
+            check(_lib.lib().mt_get_demag_colmajor(self._h, *[o.ctypes.data_as(_lib.F) for o in out]),
+                  "mt_get_demag_colmajor")
+        return out
+
+    # ---------------------------------------------------------------- fields
+    def _vec(self, m):
+        m = torch.as_tensor(m, dtype=torch.float64, device=self.device).reshape(3 * self.n)
+        return m.contiguous()
+
+    def demag_field(self, m, stream=None):
+        """Internal demag field -Ms K m (FP32 product), shape (3, n)."""
+        m = self._vec(m)
+        out = torch.empty(3 * self.n, dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            check(_lib.lib().mt_demag_field(self._h, _dptr(m), _dptr(out), _stream(stream)), "mt_demag_field")
+        return out.view(3, self.n)
+
+    def fields(self, t, m, stream=None):
+        """(H_exc, H_ext, H_ani, H_dem), each (3, n), the reference's internal sign."""
+        m = self._vec(m)
+        outs = [torch.empty(3 * self.n, dtype=torch.float64, device=self.device) for _ in range(4)]
+        with torch.cuda.device(self.device):
+            check(_lib.lib().mt_fields(self._h, float(t), _dptr(m), *[_dptr(o) for o in outs], _stream(stream)),
+                  "mt_fields")
+        return tuple(o.view(3, self.n) for o in outs)
+
+    def rhs(self, t, m, stream=None):
+        m = self._vec(m)
+        out = torch.empty(3 * self.n, dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            check(_lib.lib().mt_rhs(self._h, float(t), _dptr(m), _dptr(out), _stream(stream)), "mt_rhs")
+        return out
+
+    # ---------------------------------------------------------------- integrate
+    def integrate(self, t, m0, *, tol=1e-4, thres=1e-6, t_conv=None, conv_tol=1e-4, y_out=None, stream=None):
+        """MagTense_ODE_RKSuite on the device.
+
+        Returns (t_out[nt] numpy, y_out (nt, 3n) cuda FP64, flags[nt] numpy, stats dict).
+        """
+        t = _np_d(t).reshape(-1)
+        nt = t.shape[0]
+        m0 = self._vec(m0)
+        tc = np.zeros(1) if t_conv is None else _np_d(t_conv).reshape(-1)
+        if y_out is None:
+            y_out = torch.zeros((nt, 3 * self.n), dtype=torch.float64, device=self.device)
+        t_out = np.zeros(nt)
+        flags = np.zeros(nt, dtype=np.int32)
+        st = _lib.Stats()
+        with torch.cuda.device(self.device):
+            rc = _lib.lib().mt_integrate(self._h, t.ctypes.data_as(_lib.D), nt, _dptr(m0), float(tol), float(thres),
+                                         tc.ctypes.data_as(_lib.D), tc.shape[0], float(conv_tol),
+                                         t_out.ctypes.data_as(_lib.D), _dptr(y_out), flags.ctypes.data_as(_lib.I),
+                                         C.byref(st), _stream(stream))
+        check(rc, "mt_integrate")
+        return t_out, y_out, flags, st.as_dict()
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _lib.lib().mt_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

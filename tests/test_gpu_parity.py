@@ -1,0 +1,255 @@
+"""Parity of the sm_100a path (through the C ABI) with the CPU oracle.
+
+Tolerances: tensor entries within 2 FP32 ulp (FP64 libm differences before the
+FP32 rounding); demag field and right-hand side within 1e-5 of the largest
+component (FP32 product, summation order of the reference's MKL SGEMV is not
+pinned); trajectories within 1e-5 in m (<m>(t) target 1e-4).
+"""
+import ctypes
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+MU0 = 4 * np.pi * 1e-7
+FILM = ([20, 5, 1], [125e-9, 31.25e-9, 3e-9])
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    torch.cuda.set_device(0)
+    return torch
+
+
+def rand_m(n, seed):
+    rng = np.random.default_rng(seed)
+    m = rng.standard_normal((3, n))
+    return m / np.linalg.norm(m, axis=0)
+
+
+def assert_ulp_close(a, b, max_ulp=2, frac_ok=1.0):
+    a = np.asarray(a, dtype=np.float32)
+    b = np.asarray(b, dtype=np.float32)
+    ia = a.view(np.int32).astype(np.int64)
+    ib = b.view(np.int32).astype(np.int64)
+    ia = np.where(ia < 0, -(ia & 0x7FFFFFFF), ia)
+    ib = np.where(ib < 0, -(ib & 0x7FFFFFFF), ib)
+    d = np.abs(ia - ib)
+    tiny = np.abs(a - b) <= 1e-12
+    bad = (d > max_ulp) & ~tiny
+    assert bad.mean() <= 1 - frac_ok + 1e-12, (bad.sum(), d.max())
+
+
+@pytest.mark.parametrize("res,L", [FILM, ([6, 5, 4], [30e-9, 25e-9, 20e-9]), ([80, 20, 1], [500e-9, 125e-9, 3e-9])])
+def test_tensor_assembly_matches_oracle(torch_cuda, oracle, res, L):
+    from magtense_b200 import Solver
+    s = Solver(res, L)
+    s.assemble()
+    blocks = s.get_tensor_colmajor()
+    n = s.n
+    rows = np.arange(n) if n <= 200 else np.random.default_rng(0).choice(n, 64, replace=False)
+    K32, _ = oracle.assemble(res, L, rows=rows)
+    for c in range(6):
+        assert_ulp_close(blocks[c][rows, :], K32[c], max_ulp=2)
+
+
+def test_demag_field_matches_oracle(torch_cuda, oracle):
+    from magtense_b200 import Solver
+    res, L = [16, 8, 2], [80e-9, 40e-9, 10e-9]
+    s = Solver(res, L, Ms=8e5)
+    s.assemble()
+    m = rand_m(s.n, 1)
+    H = s.demag_field(torch_cuda.as_tensor(m.reshape(-1), device="cuda")).cpu().numpy()
+    P = oracle.Problem(res, L, mode=0)
+    Href = P.fields(0.0, m)[3]
+    assert np.abs(H - Href).max() <= 1e-5 * np.abs(Href).max()
+    P64 = oracle.Problem(res, L, mode=1)
+    H64 = P64.fields(0.0, m)[3]
+    assert np.abs(H - H64).max() <= 1e-5 * np.abs(H64).max()
+
+
+def test_fields_and_rhs_match_oracle(torch_cuda, oracle):
+    from magtense_b200 import Solver
+    res, L = [12, 6, 3], [60e-9, 30e-9, 15e-9]
+    n = 216
+    rng = np.random.default_rng(2)
+    u = rng.standard_normal((n, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    Ms = rng.uniform(7.5e5, 8.5e5, n)
+    hext = np.array([[0.0, 1e4, -2e4, 3e3], [1e-9, -1e4, 2e4, 0.0]])
+    s = Solver(res, L, Ms=Ms, K0=5e3, u_ea=u)
+    s.assemble()
+    s.set_dynamics(solver=2, gamma=2.211e5, alpha=2.211e5 * 0.1, hext=hext)
+    P = oracle.Problem(res, L, mode=0, Ms=Ms, K0=5e3, u_ea=u, gamma=2.211e5, alpha=2.211e5 * 0.1, hext=hext)
+    m = rand_m(n, 3)
+    t = 0.3e-9
+    mt = torch_cuda.as_tensor(m.reshape(-1), device="cuda")
+    got = [g.cpu().numpy() for g in s.fields(t, mt)]
+    ref = P.fields(t, m)
+    for g, r, name in zip(got[:3], ref[:3], ("exchange", "Zeeman", "anisotropy")):
+        np.testing.assert_allclose(g, r, rtol=1e-14, atol=1e-14 * np.abs(r).max(), err_msg=name)
+    assert np.abs(got[3] - ref[3]).max() <= 1e-5 * np.abs(ref[3]).max()
+    d = s.rhs(t, mt).cpu().numpy()
+    dref = P.rhs(t, m)
+    assert np.abs(d - dref).max() <= 1e-5 * np.abs(dref).max()
+
+
+def _film_problem(torch_cuda, oracle, alpha, gamma, hext, tol=1e-6, renorm=False, res=FILM[0], L=FILM[1]):
+    from magtense_b200 import Solver
+    s = Solver(res, L)
+    s.assemble()
+    s.set_dynamics(solver=2, gamma=gamma, alpha=alpha, hext=hext, renormalize=renorm)
+    P = oracle.Problem(res, L, mode=0, gamma=gamma, alpha=alpha, hext=hext)
+    P.set_renorm(renorm)
+    return s, P
+
+
+def compare_runs(got, ref, atol, min_matched=0.95):
+    """Compare samples taken at the same time by both runs.  A sample that came
+    from a flag-3/4 return sits at the internal time instead of the requested
+    one (RKSuitef90.f90:1374-1387, ODE_Solvers.f90:225-231); which outputs get
+    displaced depends on the evaluation count, so only matching times compare."""
+    t_g, y_g, f_g, st_g = got
+    t_r, y_r, f_r, st_r = ref
+    same = t_g == t_r
+    assert same.mean() >= min_matched, (same.mean(), st_g, st_r)
+    err = np.abs(y_g[same] - y_r[same]).max()
+    assert err < atol, (err, st_g, st_r)
+    return err
+
+
+@pytest.mark.parametrize("renorm", [False, True])
+def test_integration_matches_oracle(torch_cuda, oracle, renorm):
+    hx, hy = -24.6e-3 / MU0, 4.3e-3 / MU0
+    hext = np.array([[0.0, hx, hy, 0.0], [0.3e-9, hx, hy, 0.0]])
+    s, P = _film_problem(torch_cuda, oracle, 2.211e5 * 0.02, 2.211e5, hext, renorm=renorm)
+    m0 = np.ones((3, s.n)) / np.sqrt(3) + 0.01 * np.random.default_rng(7).standard_normal((3, s.n))
+    m0 /= np.linalg.norm(m0, axis=0)
+    t = np.linspace(0, 0.3e-9, 61)
+    t_g, y_g, f_g, st_g = s.integrate(t, torch_cuda.as_tensor(m0.reshape(-1), device="cuda"), tol=1e-6)
+    ref = P.solve(t, m0.reshape(-1), tol=1e-6)
+    compare_runs((t_g, y_g.cpu().numpy(), f_g, st_g), ref, atol=1e-5)
+    assert abs(st_g["steps"] - ref[3]["steps"]) <= 2
+
+
+def test_relaxation_with_flag_returns_matches_oracle(torch_cuda, oracle):
+    """Long, strongly damped run: more than 5000 evaluations, so the 'too much
+    work' returns (and the stiffness test behind them) are exercised.  Near
+    equilibrium the step size at tol = thres = 1e-6 is set by the FP32 rounding
+    of the demag product (absolute error target ~1e-12 on components of ~1e-6),
+    so the two FP32 runs take different step sequences and displace different
+    samples; the samples both take at the requested times must agree."""
+    hext = np.array([[0.0, 0.0, 0.0, 0.0], [2e-9, 0.0, 0.0, 0.0]])
+    s, P = _film_problem(torch_cuda, oracle, 2.211e5 * 1.0, 2.211e5, hext)
+    m0 = np.ones((3, s.n)) / np.sqrt(3) + 0.01 * np.random.default_rng(8).standard_normal((3, s.n))
+    m0 /= np.linalg.norm(m0, axis=0)
+    t = np.linspace(0, 2e-9, 401)
+    got = s.integrate(t, torch_cuda.as_tensor(m0.reshape(-1), device="cuda"), tol=1e-6)
+    ref = P.solve(t, m0.reshape(-1), tol=1e-6)
+    assert ref[3]["f_evals"] > 5000 and ref[3]["n_flag3"] >= 1
+    assert got[3]["n_flag3"] >= 1 and np.all(got[0][got[2] == 3] < t[got[2] == 3])
+    compare_runs((got[0], got[1].cpu().numpy(), got[2], got[3]), ref, atol=1e-4, min_matched=0.5)
+    # the final relaxed state agrees well inside the <m> target
+    mg = got[1][-1].cpu().numpy().reshape(3, -1).mean(1)
+    mr = ref[1][-1].reshape(3, -1).mean(1)
+    assert np.abs(mg - mr).max() < 1e-4, (mg, mr, got[3], ref[3])
+
+
+def test_icl_shims(torch_cuda, oracle):
+    from magtense_b200 import _lib
+    L = _lib.lib()
+    res, Lg = [10, 6, 2], [50e-9, 30e-9, 10e-9]
+    n = 120
+    K32, _ = oracle.assemble(res, Lg)
+    blocks = [np.asfortranarray(K32[c]) for c in range(6)]
+    F = ctypes.POINTER(ctypes.c_float)
+    nn = ctypes.c_int(n)
+    _lib.check(L.icl_initDemagMatrices(*[b.ctypes.data_as(F) for b in blocks], ctypes.byref(nn)), "init")
+    m = rand_m(n, 9).astype(np.float32)
+    H = [np.zeros(n, np.float32) for _ in range(3)]
+    pref = ctypes.c_float(-1.0)
+    _lib.check(L.icl_MVMult_GetH(*[np.ascontiguousarray(m[a]).ctypes.data_as(F) for a in range(3)],
+                                 *[h.ctypes.data_as(F) for h in H], ctypes.byref(nn), ctypes.byref(pref)), "mv")
+    K = K32.astype(np.float64)
+    blk = [[0, 1, 2], [1, 3, 4], [2, 4, 5]]
+    ref = np.array([-sum(K[blk[a][b]] @ m[b].astype(np.float64) for b in range(3)) for a in range(3)])
+    assert np.abs(np.array(H) - ref).max() <= 1e-5 * np.abs(ref).max()
+    assert L.icl_MVMult_GetH_sparse(*[h.ctypes.data_as(F) for h in H], *[h.ctypes.data_as(F) for h in H],
+                                    ctypes.byref(nn), ctypes.byref(pref)) == -5
+    assert L.icl_destroy() == 0
+
+
+def test_micromag_problem_dropin(torch_cuda, oracle):
+    from magtense_b200 import MicromagProblem
+    res, L = FILM
+    n = 100
+    m0 = np.zeros((n, 3))
+    m0[:] = 1 / np.sqrt(3)
+    hnist = np.array([-24.6, 4.3, 0.0]) / 1000 / MU0
+    prob = MicromagProblem(res, L, m0=m0, alpha=4.42e3, gamma=2.21e5, tol=1e-6)
+    t_out, M, pts, Hx, He, Hd, Ha = prob.run_simulation(0.1e-9, 21, lambda t: np.expand_dims(t > -1, 1) * hnist, 20)
+    assert M.shape == (21, n, 1, 3) and pts.shape == (n, 3) and Hx.shape == (21, n, 1, 3)
+    hext = np.zeros((20, 4))
+    hext[:, 0] = np.linspace(0, 0.1e-9, 20)
+    hext[:, 1:] = hnist
+    P = oracle.Problem(res, L, mode=0, gamma=2.21e5, alpha=4.42e3, hext=hext)
+    to, yo, fo, so = P.solve(np.linspace(0, 0.1e-9, 21), np.concatenate([m0[:, 0], m0[:, 1], m0[:, 2]]), tol=1e-6)
+    ym = M[:, :, 0, :].transpose(0, 2, 1).reshape(21, -1)
+    assert np.abs(ym - yo).max() < 1e-5
+    np.testing.assert_allclose(pts, oracle.grid(res, L)[0])
+
+
+def test_return_fields_and_tensor_file(torch_cuda, oracle, tmp_path):
+    from magtense_b200 import MicromagProblem, Solver, save_demag_tensor
+    res, L = [8, 4, 1], [50e-9, 25e-9, 3e-9]
+    s = Solver(res, L)
+    s.assemble()
+    path = str(tmp_path / "demag_tensor.bin")
+    save_demag_tensor(path, s.get_tensor_colmajor())
+    assert os.path.getsize(path) == 6 * 32 * 32 * 4
+    kw = dict(m0=1 / np.sqrt(3), alpha=4.42e3, gamma=2.21e5, tol=1e-6, ReturnHall=1)
+    fct = lambda t: np.expand_dims(t > -1, 1) * np.array([1e4, 0, 0])
+    a = MicromagProblem(res, L, **kw).run_simulation(0.05e-9, 6, fct, 3)
+    b = MicromagProblem(res, L, filename=path, **kw).run_simulation(0.05e-9, 6, fct, 3)
+    np.testing.assert_array_equal(a[1], b[1])
+    Hext = a[4]
+    np.testing.assert_allclose(Hext[:, :, 0, 0], -1e4)
+    assert np.abs(a[5]).max() > 0 and np.abs(a[3]).max() > 0
+
+
+def test_explicit_mode_chains_fields(torch_cuda, oracle):
+    from magtense_b200 import MicromagProblem
+    res, L = [8, 4, 1], [50e-9, 25e-9, 3e-9]
+    n = 32
+    fields = np.array([[2e4, 0, 0], [-2e4, 0, 0]])
+    prob = MicromagProblem(res, L, solver="explicit", m0=1 / np.sqrt(3), alpha=2.21e5, gamma=0.0, tol=1e-6)
+    t_out, M, *_ = prob.run_simulation(0.05e-9, 6, lambda t: fields, 2)
+    assert M.shape == (6, n, 2, 3)
+    hext = np.zeros((2, 4))
+    hext[:, 0] = [0.0, 0.05e-9]
+    hext[:, 1:] = fields
+    P = oracle.Problem(res, L, solver=1, mode=0, gamma=0.0, alpha=2.21e5, hext=hext)
+    m = np.full(3 * n, 1 / np.sqrt(3))
+    for i in range(2):
+        P.set_hext_ind(i)
+        to, yo, _, _ = P.solve(np.linspace(0, 0.05e-9, 6), m, tol=1e-6)
+        got = M[:, :, i, :].transpose(0, 2, 1).reshape(6, -1)
+        assert np.abs(got - yo).max() < 1e-5
+        m = yo[-1]
+
+
+def test_argument_errors_raise(torch_cuda):
+    from magtense_b200 import MTError, Solver
+    s = Solver([4, 2, 1], [20e-9, 10e-9, 3e-9])
+    with pytest.raises(MTError):
+        s.rhs(0.0, np.zeros(24))          # no tensor yet
+    s.assemble()
+    s.set_dynamics(solver=2, alpha=1.0)
+    with pytest.raises(MTError):
+        s.integrate(np.array([0.0, 1e-12]), np.ones(24) / np.sqrt(3), tol=0.5)   # tol outside (round_off, 0.01)
+    with pytest.raises(MTError):
+        s.integrate(np.array([1e-12, 1e-12]), np.ones(24) / np.sqrt(3))          # t_start == t_end

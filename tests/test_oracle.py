@@ -1,0 +1,273 @@
+"""CPU tests of the oracle (oracle/mt_oracle.c) against the reference's own
+fixtures and against analytic known answers.  No GPU needed."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+MU0 = 4 * np.pi * 1e-7
+
+
+def full3(N6):
+    xx, xy, xz, yy, yz, zz = N6
+    return np.array([[xx, xy, xz], [xy, yy, yz], [xz, yz, zz]])
+
+
+# ---------------------------------------------------------------- prism tensor
+def test_cube_self_term(oracle):
+    N = oracle.prism_tensor(1, 1, 1, 0, 0, 0)
+    np.testing.assert_allclose(N[[0, 3, 5]], -1 / 3, rtol=0, atol=1e-15)
+    np.testing.assert_allclose(N[[1, 2, 4]], 0, atol=1e-15)
+
+
+def test_superposition_is_exact(oracle):
+    # a (2a,b,c) prism equals two (a,b,c) prisms side by side
+    rng = np.random.default_rng(1)
+    for _ in range(50):
+        a, b, c = rng.uniform(0.5, 2.0, 3)
+        r = rng.uniform(-4, 4, 3)
+        big = oracle.prism_tensor(2 * a, b, c, *r)
+        small = oracle.prism_tensor(a, b, c, *(r - [a / 2, 0, 0])) + oracle.prism_tensor(a, b, c, *(r + [a / 2, 0, 0]))
+        np.testing.assert_allclose(big, small, rtol=1e-9, atol=1e-12)
+
+
+def test_trace_outside_zero_inside_minus_one(oracle):
+    rng = np.random.default_rng(2)
+    for _ in range(30):
+        abc = rng.uniform(0.5, 2.0, 3)
+        out = abc * rng.uniform(0.7, 3.0, 3) * rng.choice([-1, 1], 3)
+        N = oracle.prism_tensor(*abc, *out)
+        assert abs(N[0] + N[3] + N[5]) < 1e-12
+        inside = abc * rng.uniform(-0.45, 0.45, 3)
+        N = oracle.prism_tensor(*abc, *inside)
+        assert abs(N[0] + N[3] + N[5] + 1.0) < 1e-12
+
+
+def test_even_in_position(oracle):
+    rng = np.random.default_rng(3)
+    for _ in range(30):
+        abc = rng.uniform(0.5, 2.0, 3)
+        r = rng.uniform(-5, 5, 3)
+        np.testing.assert_allclose(oracle.prism_tensor(*abc, *r), oracle.prism_tensor(*abc, *(-r)), rtol=1e-9,
+                                   atol=1e-13)
+
+
+def test_far_field_is_dipole(oracle):
+    a, b, c = 1.0, 0.7, 0.4
+    V = a * b * c
+    for r in ([40.0, 3.0, -7.0], [-10.0, 35.0, 20.0]):
+        r = np.array(r)
+        d = np.linalg.norm(r)
+        u = r / d
+        dip = V / (4 * np.pi * d ** 3) * (3 * np.outer(u, u) - np.eye(3))
+        np.testing.assert_allclose(full3(oracle.prism_tensor(a, b, c, *r)), dip, rtol=0, atol=5e-3 * np.abs(dip).max())
+
+
+def _rot(angles):
+    def rx(a):
+        c, s = np.cos(a), np.sin(a)
+        return np.array([[1, 0, 0], [0, c, -s], [0, s, c]])
+
+    def ry(a):
+        c, s = np.cos(a), np.sin(a)
+        return np.array([[c, 0, s], [0, 1, 0], [-s, 0, c]])
+
+    def rz(a):
+        c, s = np.cos(a), np.sin(a)
+        return np.array([[c, -s, 0], [s, c, 0], [0, 0, 1]])
+
+    # getRotationMatrices, DemagFieldGetSolution.f90:925-948
+    RX, RY, RZ = rx(-angles[0]), ry(-angles[1]), rz(-angles[2])
+    return RZ @ RY @ RX, RX.T @ RY.T @ RZ.T
+
+
+def test_prism_field_against_reference_fem_fixture(oracle):
+    """The reference's COMSOL validation of a rotated prism (python/examples/
+    magnetostatics/validation.py:8-20): |B| along three lines."""
+    fx = np.load(GOLDEN / "fem_prism_normH.npz")
+    size, offset = [0.6, 0.1, 0.3], np.array([0.5, 0.4, 0.1])
+    R, Rinv = _rot([np.pi / 2, -np.pi / 3, np.pi / 4])
+    ea = np.array([0.35355339, 0.61237244, 0.70710678])
+    M = 1.2 / MU0 * np.around(ea / np.linalg.norm(ea), 9)
+    for ax, c in enumerate("xyz"):
+        T = fx[f"line_{c}"]
+        pts = np.tile(offset, (len(T), 1))
+        pts[:, ax] = T[:, 0]
+        B = np.array([np.linalg.norm(Rinv @ (full3(oracle.prism_tensor(*size, *(R @ (p - offset)))) @ (R @ M))) * MU0
+                      for p in pts])
+        err = np.abs(B - T[:, 1])
+        assert np.median(err) < 3e-4, (c, np.median(err))
+        assert np.mean(err) < 2e-3, (c, np.mean(err))
+
+
+# ---------------------------------------------------------------- grid and tensor
+def test_grid_matches_setup_grid(oracle):
+    pts, d = oracle.grid([80, 20, 1], [500e-9, 125e-9, 3e-9])
+    assert d[0] == 500e-9 / 80 and d[2] == 3e-9
+    assert pts[0, 0] == (-(500e-9 / 2) + 0 * d[0]) + d[0] / 2
+    assert np.all(pts[:, 2] == 0)
+    assert pts[81, 1] == pts[80, 1] and pts[80, 1] > pts[0, 1]
+
+
+def test_assemble_rows_equal_full(oracle):
+    res, L = [6, 4, 2], [30e-9, 20e-9, 6e-9]
+    K, K64 = oracle.assemble(res, L, fp32=True, fp64=True)
+    rows = np.array([0, 7, 19, 47])
+    Kr, _ = oracle.assemble(res, L, rows=rows)
+    np.testing.assert_array_equal(Kr, K[:, rows, :])
+    np.testing.assert_array_equal(K, K64.astype(np.float32))
+    # self term of a cubic-ish cell and symmetry of the assembled matrix
+    n = 48
+    for c in range(6):
+        np.testing.assert_allclose(K64[c], K64[c].T, rtol=1e-9, atol=1e-14)
+    assert K64[0, 0, 0] < 0 and K64[3, 0, 0] < 0
+
+
+def test_tensor_sum_rule(oracle):
+    # the summed tensor over all sources of a long bar approaches the bar's own tensor
+    res, L = [20, 4, 2], [100e-9, 20e-9, 10e-9]
+    _, K64 = oracle.assemble(res, L, fp32=False, fp64=True)
+    n = 160
+    tot = K64.sum(axis=2)           # field at each receiver from uniform m
+    pts, _ = oracle.grid(res, L)
+    for i in (0, 37, 159):
+        whole = oracle.prism_tensor(*L, *pts[i])
+        np.testing.assert_allclose(tot[:, i], whole, rtol=1e-9, atol=1e-12)
+
+
+# ---------------------------------------------------------------- fields
+def _reference_exchange_csr(nx, ny, nz, d):
+    """The CSR of ComputeExchangeTerm3D_Uniform (LandauLifshitzEquationSolver.f90:1194-1522) as a dense matrix."""
+    n = nx * ny * nz
+    A = np.zeros((n, n))
+
+    def add_axis(nn, stride, dd):
+        for i in range(n):
+            k = (i // stride) % nn
+            if k == 0:
+                A[i, i] += -1.0 / dd ** 2
+                A[i, i + stride] += 1.0 / dd ** 2
+            elif k == nn - 1:
+                A[i, i - stride] += 1.0 / dd ** 2
+                A[i, i] += -1.0 / dd ** 2
+            else:
+                A[i, i - stride] += 1.0 / dd ** 2
+                A[i, i] += -2.0 / dd ** 2
+                A[i, i + stride] += 1.0 / dd ** 2
+
+    add_axis(nx, 1, d[0])
+    add_axis(ny, nx, d[1])
+    if nz > 1:
+        add_axis(nz, nx * ny, d[2])
+    return A
+
+
+@pytest.mark.parametrize("res", [[6, 5, 1], [5, 4, 3]])
+def test_exchange_matches_reference_csr(oracle, res):
+    L = [30e-9, 25e-9, 9e-9]
+    P = oracle.Problem(res, L, mode=0, alpha=1.0)
+    n = P.n
+    rng = np.random.default_rng(4)
+    m = rng.standard_normal((3, n))
+    Hj, Hh, Hk, Hm = P.fields(0.0, m)
+    _, d = oracle.grid(res, L)
+    A = _reference_exchange_csr(*res, d)
+    Jf = 1.3e-11 / (MU0 * 8e5)
+    np.testing.assert_allclose(Hj, (-2.0 * (A @ m.T).T) * Jf, rtol=1e-12, atol=1e-12 * np.abs(Hj).max())
+
+
+def test_anisotropy_and_zeeman(oracle):
+    res, L = [4, 3, 1], [20e-9, 15e-9, 3e-9]
+    n = 12
+    rng = np.random.default_rng(5)
+    u = rng.standard_normal((n, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    hext = np.array([[0.0, 1e3, -2e3, 5e2], [1e-9, 3e3, 0.0, -5e2]])
+    P = oracle.Problem(res, L, mode=0, K0=5e3, u_ea=u, alpha=1.0, hext=hext)
+    m = rng.standard_normal((3, n))
+    Hj, Hh, Hk, Hm = P.fields(0.25e-9, m)
+    k = 5e3 / (MU0 * 8e5)
+    ref = -2 * k * (u * (u * m.T).sum(1, keepdims=True)).T
+    np.testing.assert_allclose(Hk, ref, rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(Hh[:, 0], -(0.75 * hext[0, 1:] + 0.25 * hext[1, 1:]), rtol=1e-14)
+    # outside the table the applied field is zero (util.f90:47-50)
+    _, Hh2, _, _ = P.fields(-1e-12, m)
+    assert np.all(Hh2 == 0)
+
+
+def test_demag_ref_and_fp64_agree(oracle):
+    res, L = [10, 4, 2], [50e-9, 20e-9, 10e-9]
+    rng = np.random.default_rng(6)
+    m = rng.standard_normal((3, 80))
+    m /= np.linalg.norm(m, axis=0)
+    P32 = oracle.Problem(res, L, mode=0)
+    P64 = oracle.Problem(res, L, mode=1)
+    H32 = P32.fields(0, m)[3]
+    H64 = P64.fields(0, m)[3]
+    assert np.abs(H32 - H64).max() / np.abs(H64).max() < 1e-5
+    rows = np.array([0, 13, 79])
+    Kr, _ = oracle.assemble(res, L, rows=rows)
+    Hr = oracle.demag_rows(Kr, None, m, 8e5, mode=0)
+    np.testing.assert_array_equal(Hr, H32[:, rows])
+
+
+def test_interp1_semantics(oracle):
+    tab = np.array([[0.0, 1.0], [1.0, 3.0], [3.0, 7.0]])
+    assert oracle.interp1(tab, 1, 0.5) == 2.0
+    assert oracle.interp1(tab, 1, 0.0) == 1.0
+    assert oracle.interp1(tab, 1, 3.0) == 7.0
+    assert oracle.interp1(tab, 1, 2.0) == 5.0
+    assert oracle.interp1(tab, 1, -0.1) == 0.0
+    assert oracle.interp1(tab, 1, 3.5) == 0.0
+
+
+# ---------------------------------------------------------------- integrator
+def test_linear_ode_accuracy(oracle):
+    lam = np.array([-1.0, -2.0, -0.5, -3.0])
+    t = np.linspace(0, 2, 41)
+    to, yo, fl, st = oracle.solve_linear(lam, t, np.ones(4), tol=1e-6)
+    assert st["status"] == 0 and st["n_out"] == 41
+    np.testing.assert_array_equal(to, t)
+    assert np.abs(yo - np.exp(np.outer(t, lam))).max() < 1e-6
+    # FSAL: 7 new evaluations per accepted step plus 3 per interpolated step window
+    assert st["f_evals"] >= 7 * st["steps"]
+
+
+def test_too_much_work_flag_displaces_sample(oracle):
+    """Every 5000 evaluations step_integrate returns flag 3 before stepping, and the
+    driver stores y(t) at the current internal time (RKSuitef90.f90:1374-1387;
+    ODE_Solvers.f90:225-231)."""
+    lam = np.array([-1.0, 2.0])
+    t = np.linspace(0, 20.0, 401)
+    to, yo, fl, st = oracle.solve_linear(lam, t, np.ones(2), tol=1e-10)
+    assert st["f_evals"] > 5000
+    assert st["n_flag3"] >= 1
+    k = np.nonzero(fl == 3)[0]
+    assert len(k) == st["n_flag3"]
+    assert np.all(to[k] < t[k]) and np.all(to[k] > t[k - 1])
+    ok = fl == 1
+    np.testing.assert_array_equal(to[ok], t[ok])
+
+
+def test_setup_errors(oracle):
+    P = oracle.Problem([3, 2, 1], [15e-9, 10e-9, 3e-9], mode=0, alpha=1.0)
+    m0 = np.ones(18) / np.sqrt(3)
+    _, _, _, st = P.solve(np.array([0.0, 0.0]), m0)
+    assert st["status"] < 0
+    _, _, _, st = P.solve(np.array([0.0, 1e-12]), m0, tol=0.5)
+    assert st["status"] < 0
+
+
+def test_micromag_small_run_conserves_norm(oracle):
+    res, L = [10, 3, 1], [62.5e-9, 18.75e-9, 3e-9]
+    hext = np.array([[0.0, -2e4, 3e3, 0.0], [1e-9, -2e4, 3e3, 0.0]])
+    P = oracle.Problem(res, L, mode=0, gamma=2.211e5, alpha=2.211e5 * 0.02, hext=hext)
+    n = P.n
+    m0 = np.tile(np.array([1.0, 1.0, 1.0])[:, None] / np.sqrt(3), (1, n))
+    to, yo, fl, st = P.solve(np.linspace(0, 0.1e-9, 11), m0.reshape(-1), tol=1e-6)
+    norms = np.linalg.norm(yo.reshape(11, 3, n), axis=1)
+    assert np.abs(norms - 1).max() < 1e-5
+    P.set_renorm(True)
+    to2, yo2, _, _ = P.solve(np.linspace(0, 0.1e-9, 11), m0.reshape(-1), tol=1e-6)
+    assert np.abs(yo2 - yo).max() < 1e-4
