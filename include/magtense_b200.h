@@ -123,6 +123,35 @@ int mt_integrate(mt_handle* h, const double* t, int nt, const double* m0_dev, do
                  double thres, const double* t_conv, int nt_conv, double conv_tol,
                  double* t_out, double* y_out_dev, int* flags, mt_stats* stats, void* stream);
 
+/* ---------------- batched instances sharing one geometry ---------------- */
+/* B independent problems on the same grid, material and demag tensor, each
+ * with its own applied-field table, damping and initial state (the dataset
+ * workflow of python/scripts/database.py:19-87 and db_utils.py:50-82, run as
+ * one call).  Every instance keeps its own RKSUITE 'M' step control; the demag
+ * products of all instances form one GEMM per right-hand-side evaluation. */
+typedef struct mt_batch mt_batch;
+
+#define MT_PREC_FP32 0     /* FP32 SIMT product, same arithmetic as the single-instance path */
+#define MT_PREC_BF16X3 1   /* tcgen05, K and m split into BF16 hi+lo, 3 products, FP32 accumulate */
+#define MT_PREC_BF16X2 2   /* tcgen05, K split hi+lo, m in BF16, 2 products, FP32 accumulate */
+
+int mt_batch_create(const mt_grid* grid, int B, int precision, mt_batch** out);
+int mt_batch_destroy(mt_batch* b);
+/* shared material, as mt_set_material */
+int mt_batch_set_material(mt_batch* b, double A0, const double* Ms, const double* K0, const double* u_ea);
+/* per-instance time dependence: alpha0[B]; hext[B][nt_hext][4] (rows {t,Hx,Hy,Hz});
+ * solver 1 (explicit) uses row 0 of each instance's table */
+int mt_batch_set_dynamics(mt_batch* b, int solver, double gamma, const double* alpha0, const double* hext,
+                          int nt_hext, int renormalize);
+int mt_batch_assemble_demag(mt_batch* b, void* stream);
+/* m0_dev: B*3n FP64; y_out_dev: B*nt*3n FP64 or NULL; t_out, flags: B*nt host;
+ * stats: B entries (kernel_ms/launches of the whole batch in stats[0]). */
+int mt_batch_integrate(mt_batch* b, const double* t, int nt, const double* m0_dev, double tol, double thres,
+                       const double* t_conv, int nt_conv, double conv_tol, double* t_out, double* y_out_dev,
+                       int* flags, mt_stats* stats, void* stream);
+/* demag field of all instances with the batch's precision: H_dev = -Ms K m, B*3n FP64 */
+int mt_batch_demag_field(mt_batch* b, const double* m_dev, double* H_dev, void* stream);
+
 /* ---------------- reference compatibility shims ---------------- */
 /* Exact signatures of the reference's C shim (MagTenseCudaBlasICLWrapper.cxx:13-59,
  * bound from Fortran in FortranCuda.f90:15-60).  They act on one process-wide

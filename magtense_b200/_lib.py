@@ -68,6 +68,14 @@ SIGNATURES = {
     "mt_rhs": [VP, C.c_double, VP, VP, VP],
     "mt_integrate": [VP, D, C.c_int, VP, C.c_double, C.c_double, D, C.c_int, C.c_double, D, VP, I,
                      C.POINTER(Stats), VP],
+    "mt_batch_create": [C.POINTER(Grid), C.c_int, C.c_int, C.POINTER(VP)],
+    "mt_batch_destroy": [VP],
+    "mt_batch_set_material": [VP, C.c_double, D, D, D],
+    "mt_batch_set_dynamics": [VP, C.c_int, C.c_double, D, D, C.c_int, C.c_int],
+    "mt_batch_assemble_demag": [VP, VP],
+    "mt_batch_integrate": [VP, D, C.c_int, VP, C.c_double, C.c_double, D, C.c_int, C.c_double, D, VP, I,
+                           C.POINTER(Stats), VP],
+    "mt_batch_demag_field": [VP, VP, VP, VP],
     "icl_initDemagMatrices": [F, F, F, F, F, F, I],
     "icl_MVMult_GetH": [F, F, F, F, F, F, I, F],
     "icl_destroy": [],

@@ -1,0 +1,1207 @@
+// Batched adaptive integration of B Landau-Lifshitz instances sharing one
+// geometry, in ONE persistent cooperative kernel.
+//
+// Every instance runs its own RKSUITE-90 method 'M' (per-instance t, h, phases,
+// counters, flags, dense output), exactly as the single-instance integrator
+// (integrate.cu) and the reference (RKSuitef90.f90: step_integrate_r1
+// :1185-1587, step_r1 :1726-1978, stiff_r1 :1981-2367, interpolate_r1
+// :2655-2997, range_integrate_r1 :942-1183; driver ODE_Solvers.f90:124-237).
+// The control flow is written once, synchronously, as a coroutine: it yields
+// when it needs a right-hand side f(t, y) or a norm over all its cells.  The
+// kernel advances all instances in lock-step "ticks":
+//
+//   P2  resolve pending reductions, advance each instance to its next yield
+//   B1  grid barrier (stage arguments of all cells visible)
+//   G   demag product of every (cell block x instance block) tile -> partial H
+//   Bh  grid barrier (partial H visible)
+//   P1  for instances that asked for f: sum the partials, apply the LL
+//       epilogue (exchange, anisotropy, Zeeman at the instance's own t,
+//       cross products) on the owned cells, advance to the next yield
+//   B2  grid barrier (reduction partials visible)
+//
+// Tile (cb, ib, s): receiver cells [128 cb, 128 cb + 128) for all three field
+// components, instances [64 ib, 64 ib + 64), source range split s of S.  The
+// coroutines of instances [64 ib + s*64/S, ...) on cells of block cb run in
+// the same CTA, one warp per instance, so the epilogue reads only H the CTA
+// group produced for its own cells.  Stage arguments alternate between two
+// buffers so no argument is rewritten while another CTA may still read it
+// (every rewrite of the same buffer is separated by a grid barrier).
+#include "batch.cuh"
+#include "gemm_tc.cuh"
+
+namespace {
+
+struct BS45b { double a[12][12]; double b[9]; double c[12]; double e[8]; double r[12][7]; };
+__constant__ BS45b cB;
+
+// destination ids of right-hand-side results
+enum { DST_STG = 0, DST_DERIV = 20 };
+
+struct BCtx {
+    DevProb P;
+    BatchBufs F;
+    BatchParams Q;
+    int cb, ib, s;          // tile coordinates of this CTA
+    int c0, nc;             // owned cells
+    int i0, ni;             // owned instances (coroutines)
+    size_t n3;              // 3n
+    int lane, warp, nwarps;
+    unsigned char* smem;
+    BInst* sinst;           // shared-memory copies of the owned coroutines
+    long long tick;
+};
+
+// per-instance vector addressing
+MT_DEV double* VPOOL(const BCtx& X, int k, int b) { return X.F.pool + ((size_t)k * X.Q.Bp + b) * X.n3; }
+MT_DEV double* VDER(const BCtx& X, int k, int b) { return X.F.deriv + ((size_t)k * X.Q.Bp + b) * X.n3; }
+MT_DEV double* VSTG(const BCtx& X, int k, int b) { return X.F.stg + ((size_t)k * X.Q.Bp + b) * X.n3; }
+MT_DEV double* VP(const BCtx& X, int k, int b) { return X.F.p + ((size_t)k * X.Q.Bp + b) * X.n3; }
+MT_DEV double* VONE(const BCtx& X, double* base, int b) { return base + (size_t)b * X.n3; }
+
+MT_DEV double* dst_ptr(const BCtx& X, int id, int b)
+{
+    if (id >= DST_DERIV) return VDER(X, id - DST_DERIV, b);
+    return VSTG(X, id, b);
+}
+
+// own elements of one instance, lane-strided: component a, cell i, index q = a*n + i
+#define FOR_OWN_W(X, q)                                                                       \
+    for (int _e = (X).lane; _e < 3 * (X).nc; _e += 32)                                        \
+        if ([[maybe_unused]] const int _a = _e / (X).nc, _i = (X).c0 + (_e - _a * (X).nc),   \
+                      q = _a * (X).P.n + _i; true)
+
+// write the stage argument (FP64) and the GEMM operand copy for one element
+MT_DEV void put_arg(const BCtx& X, int argi, int b, int q, double v)
+{
+    VPOOL(X, argi, b)[q] = v;
+    const int n = X.P.n;
+    const int a = q / n, i = q - a * n;
+    const float f = (float)v;
+    if (X.Q.prec == kPrecFP32) {
+        X.F.m32[((size_t)b * 3 + a) * X.P.ldk + i] = f;
+    } else {
+        const size_t col = (size_t)b * X.Q.Kd + (size_t)a * X.Q.np + i;
+        const __nv_bfloat16 hi = __float2bfloat16_rn(f);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(f - __bfloat162float(hi));
+        X.F.mhi[col] = __bfloat16_as_ushort(hi);
+        X.F.mlo[col] = __bfloat16_as_ushort(lo);
+    }
+}
+
+MT_DEV double warp_red(double v, bool is_max)
+{
+    return is_max ? warp_max(v) : warp_sum(v);
+}
+
+// post a reduction of K values (per-lane partials v[]) for instance b
+MT_DEV void post_reduce(const BCtx& X, BInst& I, int b, const double* v, int K, bool is_max)
+{
+    for (int k = 0; k < K; ++k) {
+        const double r = warp_red(v[k], is_max);
+        if (X.lane == 0) X.F.partials[((size_t)b * kRedSlots + k) * X.Q.CB + X.cb] = r;
+    }
+    I.req = 2;
+    I.red_k = K;
+    I.red_max = is_max ? 1 : 0;
+}
+
+MT_DEV void resolve_reduce(const BCtx& X, BInst& I, int b)
+{
+    for (int k = 0; k < I.red_k; ++k) {
+        double r = 0.0;
+        for (int c = 0; c < X.Q.CB; ++c) {
+            const double x = ldcg(&X.F.partials[((size_t)b * kRedSlots + k) * X.Q.CB + c]);
+            r = (c == 0) ? x : (I.red_max ? fmax(r, x) : r + x);
+        }
+        I.red[k] = r;
+    }
+    I.req = 0;
+}
+
+// time-dependent scalars of instance b
+MT_DEV TimeScalars inst_scalars(const BCtx& X, int b, double t)
+{
+    DevProb P = X.P;
+    P.hext = X.F.hext + (size_t)b * X.Q.nt_hext * 4;
+    P.nt_hext = X.Q.nt_hext;
+    P.alpha0 = X.F.alpha0[b];
+    return time_scalars(P, t);
+}
+
+// ---------------------------------------------------------------------------
+// The coroutine.  Yield points: Y_RHS (after writing the argument), Y_RED
+// (after posting partials).  Control flow mirrors rk_range_integrate /
+// rk_step_integrate / rk_step / rk_stiff / rk_interpolate in integrate.cu.
+// ---------------------------------------------------------------------------
+#define CO_YIELD(I, lbl) do { (I).pc = (lbl); return; case (lbl):; } while (0)
+#define Y_RHS(I, lbl, t_, argi_, dst_) do { (I).req = 1; (I).t_rhs = (t_); (I).rhs_arg = (argi_); \
+                                           (I).rhs_dst = (dst_); CO_YIELD(I, lbl); } while (0)
+
+enum {
+    L_START = 0, L_DRIVER, L_FIRSTF, L_FIRSTF_RED, L_STIFF1, L_STIFF2, L_STIFF_AJ, L_STIFF_AJ_RED, L_STEPB,
+    L_STAGE, L_STEPA, L_FINAL, L_INTERP, L_CONV, L_DONE, L_STIFF_NORM,
+    L_STIFF_LOOP = 100,   // + 10 * which vector (1,2,3) + sub
+};
+
+MT_DEV void copy_own(const BCtx& X, const double* src, double* dst)
+{
+    FOR_OWN_W(X, q) dst[q] = ldcg(&src[q]);
+    __syncwarp();
+}
+
+MT_DEV void advance(BCtx& X, BInst& I, int b)
+{
+    RKS& s = I.s;
+    const double thr = X.Q.thres;
+    const size_t n3 = X.n3;
+    (void)n3;
+    switch (I.pc) {
+    case L_START:
+    // ================================ driver loop over output times
+    for (;;) {
+        if (s.ci >= X.Q.ncomb) { s.finished = 1; break; }
+        I.t_want = X.Q.comb_t[s.ci];
+        I.cf = X.Q.comb_flags[s.ci];
+        I.dst_slot = ((I.cf & 1) && s.ko < X.Q.nt) ? 1 : 0;
+        // ---- range_integrate prologue
+        if (s.at_t_start) {
+            s.range_t_end = s.t_end;
+            s.tlast = s.t_start;
+            I.t_got = s.t_start;
+            s.h = fmin(fabs(s.h), fabs(xsub(I.t_want, s.t_start)));
+            s.h = fmax(s.h, fmax(X.Q.sqtiny, xmul(X.Q.toosml, fmax(fabs(s.t_start), fabs(s.t_end)))));
+        } else if (s.tlast == s.range_t_end) {
+            s.status = 911; s.finished = 1; break;
+        }
+        if (xmul(s.dir, xsub(I.t_want, s.tlast)) <= 0.0 || xmul(s.dir, xsub(I.t_want, s.range_t_end)) > 0.0) {
+            s.status = 911; s.finished = 1; break;
+        }
+        I.flag = 1;
+        // ---- range_integrate loop
+        for (;;) {
+            if (xmul(s.dir, xsub(s.t, I.t_want)) >= 0.0) {
+                // ---------------- interpolate
+                if (!s.intrp_ready) {
+                    for (I.i_stage = 9; I.i_stage <= 11; ++I.i_stage) {
+                        {
+                            const int i = I.i_stage;
+                            const int argi = (i == 10) ? s.ia0 : s.ia1;
+                            const double* yold = VPOOL(X, s.iyold, b);
+                            const double* k1 = VDER(X, s.dypold, b);
+                            const double* k8 = VDER(X, s.dyp, b);
+                            FOR_OWN_W(X, q) {
+                                double e = xmul(cB.a[i][1], ldcg(&k1[q]));
+                                for (int j = 2; j <= i - 1; ++j) {
+                                    const double* sj = (j == 8) ? k8 : VSTG(X, j, b);
+                                    e = xadd(e, xmul(cB.a[i][j], ldcg(&sj[q])));
+                                }
+                                put_arg(X, argi, b, q, xadd(ldcg(&yold[q]), xmul(s.h_old, e)));
+                            }
+                            __syncwarp();
+                            I.tstg = xadd(s.t_old, xmul(cB.c[i], s.h_old));
+                            I.argi = argi;
+                        }
+                        Y_RHS(I, L_INTERP + 1000 + 0, I.tstg, I.argi, DST_STG + I.i_stage);
+                        s.f_count++;
+                    }
+                    {
+                        const double ho = s.h_old;
+                        const double* k1 = VDER(X, s.dypold, b);
+                        const double* k8 = VDER(X, s.dyp, b);
+                        FOR_OWN_W(X, q) {
+                            const double K1 = ldcg(&k1[q]), K3 = ldcg(&VSTG(X, 3, b)[q]), K4 = ldcg(&VSTG(X, 4, b)[q]);
+                            const double K5 = ldcg(&VSTG(X, 5, b)[q]), K6 = ldcg(&VSTG(X, 6, b)[q]);
+                            const double K7 = ldcg(&VSTG(X, 7, b)[q]), K8 = ldcg(&k8[q]), K9 = ldcg(&VSTG(X, 9, b)[q]);
+                            const double K10 = ldcg(&VSTG(X, 10, b)[q]), K11 = ldcg(&VSTG(X, 11, b)[q]);
+#define R(i, j) cB.r[i][j]
+#define M(a, b2) xmul(a, b2)
+#define A(a, b2) xadd(a, b2)
+                            const double p5 = A(A(M(R(5, 6), K5), A(A(M(R(10, 6), K10), M(R(8, 6), K8)), A(M(R(7, 6), K7), M(R(6, 6), K6)))),
+                                                A(A(A(M(R(4, 6), K4), M(R(9, 6), K9)), A(M(R(3, 6), K3), M(R(11, 6), K11))), M(R(1, 6), K1)));
+                            const double p4 = A(A(A(M(R(10, 5), K10), M(R(9, 5), K9)), A(A(M(R(7, 5), K7), M(R(6, 5), K6)), M(R(5, 5), K5))),
+                                                A(A(A(M(R(4, 5), K4), M(R(8, 5), K8)), A(M(R(3, 5), K3), M(R(11, 5), K11))), M(R(1, 5), K1)));
+                            const double p3 = A(A(A(A(M(R(4, 4), K4), M(R(8, 4), K8)), A(M(R(7, 4), K7), M(R(6, 4), K6))), M(R(5, 4), K5)),
+                                                A(A(A(M(R(10, 4), K10), M(R(9, 4), K9)), A(M(R(3, 4), K3), M(R(11, 4), K11))), M(R(1, 4), K1)));
+                            const double p2 = A(A(A(M(R(5, 3), K5), M(R(6, 3), K6)),
+                                                  A(A(A(M(R(3, 3), K3), M(R(9, 3), K9)), A(M(R(10, 3), K10), M(R(8, 3), K8))), M(R(1, 3), K1))),
+                                                A(A(M(R(4, 3), K4), M(R(11, 3), K11)), M(R(7, 3), K7)));
+                            const double p1 = A(A(A(M(R(5, 2), K5), A(A(M(R(6, 2), K6), M(R(8, 2), K8)), M(R(1, 2), K1))),
+                                                  A(A(M(R(3, 2), K3), M(R(9, 2), K9)), M(R(10, 2), K10))),
+                                                A(A(M(R(4, 2), K4), M(R(11, 2), K11)), M(R(7, 2), K7)));
+#undef R
+#undef M
+#undef A
+                            VP(X, 5, b)[q] = xmul(ho, p5); VP(X, 4, b)[q] = xmul(ho, p4); VP(X, 3, b)[q] = xmul(ho, p3);
+                            VP(X, 2, b)[q] = xmul(ho, p2); VP(X, 1, b)[q] = xmul(ho, p1);
+                        }
+                        __syncwarp();
+                        s.intrp_ready = 1;
+                    }
+                }
+                {
+                    const double sigma = xsub(I.t_want, s.t) / s.h_old;
+                    const double* y = VPOOL(X, s.iy, b);
+                    const double* yp = VDER(X, s.dyp, b);
+                    double* dst = I.dst_slot ? X.F.y_out ? X.F.y_out + ((size_t)b * X.Q.nt + s.ko) * X.n3 : VONE(X, X.F.ystep, b)
+                                             : VONE(X, X.F.ystep, b);
+                    FOR_OWN_W(X, q) {
+                        double v = xmul(ldcg(&VP(X, 5, b)[q]), sigma);
+                        v = xmul(xadd(v, ldcg(&VP(X, 4, b)[q])), sigma);
+                        v = xmul(xadd(v, ldcg(&VP(X, 3, b)[q])), sigma);
+                        v = xmul(xadd(v, ldcg(&VP(X, 2, b)[q])), sigma);
+                        v = xmul(xadd(v, ldcg(&VP(X, 1, b)[q])), sigma);
+                        dst[q] = xadd(xmul(xadd(v, xmul(s.h_old, ldcg(&yp[q]))), sigma), ldcg(&y[q]));
+                    }
+                    __syncwarp();
+                    I.t_got = I.t_want;
+                }
+                break;
+            }
+            // ---------------- step_integrate
+            if (s.full_f_count + s.f_count >= I.budget_mark) {
+                // per-launch budget exhausted: park here; the next launch resumes
+                I.req = 4;
+                CO_YIELD(I, L_DRIVER);
+            }
+            I.ier = 1;
+            if (s.at_t_start) {
+                {   // the GEMM operand holds the argument of the next request
+                    const double* y = VPOOL(X, s.iy, b);
+                    FOR_OWN_W(X, q) put_arg(X, s.iy, b, q, ldcg(&y[q]));
+                    __syncwarp();
+                }
+                Y_RHS(I, L_FIRSTF, s.t, s.iy, DST_DERIV + s.dyp);
+                s.f_count++;
+                {
+                    const double* y = VPOOL(X, s.iy, b);
+                    const double* yp = VDER(X, s.dyp, b);
+                    double* w = X.F.weights + (size_t)b * X.n3;
+                    double mx = -1.0;
+                    FOR_OWN_W(X, q) {
+                        const double yq = ldcg(&y[q]);
+                        const double wq = fmax(fabs(yq), thr);
+                        w[q] = wq;
+                        if (yq != 0.0) mx = fmax(mx, fabs(ldcg(&yp[q])) / wq);
+                    }
+                    __syncwarp();
+                    post_reduce(X, I, b, &mx, 1, true);
+                }
+                CO_YIELD(I, L_FIRSTF_RED);
+                {
+                    s.phase2 = 1;
+                    s.h = fabs(s.h);
+                    const double ypnorm = fmax(0.0, I.red[0] < 0.0 ? -1.0 : I.red[0]);
+                    const double tau = pow(s.tol, 0.2);
+                    if (xmul(s.h, ypnorm) > tau) s.h = tau / ypnorm;
+                    I.hmin = fmax(X.Q.sqtiny, xmul(X.Q.toosml, fmax(fabs(s.t_start), fabs(s.t_end))));
+                    s.h = xmul(s.dir, fmax(s.h, I.hmin));
+                }
+            } else if (s.at_t_end) {
+                I.ier = 911;
+            }
+            if (I.ier == 1) {
+                I.phase3 = 1;
+                I.failed = 0;
+                for (;;) {   // take_step
+                    s.h = copysign(fabs(s.h), s.dir);
+                    s.at_t_end = xmul(s.dir, xsub(xadd(s.t, s.h), s.t_end)) >= 0.0;
+                    if (s.at_t_end) s.h = xsub(s.t_end, s.t);
+                    else if (xmul(s.dir, xsub(xadd(s.t, xmul(2.0, s.h)), s.t_end)) >= 0.0) s.h = xsub(s.t_end, s.t) / 2.0;
+                    I.hmin = fmax(X.Q.sqtiny, xmul(X.Q.toosml, fmax(fabs(s.t), fabs(xadd(s.t, s.h)))));
+                    if (fabs(s.h) < I.hmin) { I.ier = 5; break; }
+                    if (s.chkeff) {
+                        s.hit_t_end_count++;
+                        if (s.hit_t_end_count >= 100 && s.hit_t_end_count >= s.step_count / 3) {
+                            I.ier = 2; s.hit_t_end_count = 0; break;
+                        }
+                    }
+                    if (!I.failed) {
+                        // ---------------- stiffness diagnosis (stiff_r1)
+                        {
+                            const int toomch = s.f_count > 5000;
+                            if (toomch) { I.ier = 3; s.full_f_count += s.f_count; s.f_count = 0; }
+                            I.sure = 0;
+                            I.lots = 0;
+                            if ((s.step_count - 10) % 40 == 0) {
+                                I.lots = s.stiff_bad_step_count >= 10;
+                                s.stiff_bad_step_count = 0;
+                            }
+                            I.maybe = toomch || I.lots;
+                        }
+                        if (I.maybe) {
+                            {
+                                double* w = X.F.weights + (size_t)b * X.n3;
+                                const double* y = VPOOL(X, s.iy, b);
+                                const double* yo = VPOOL(X, s.iyold, b);
+                                FOR_OWN_W(X, q) w[q] = fmax(xmul(0.5, xadd(fabs(ldcg(&y[q])), fabs(ldcg(&yo[q])))), thr);
+                                __syncwarp();
+                                const double rat = fabs(s.h / s.h_average);
+                                I.maybe = 0.2 < rat && rat < 5.0;
+                                if (I.maybe) I.maybe = xmul(7.0, fabs(xsub(s.t_end, s.t) / s.h_average)) > 5000.0;
+                            }
+                            if (I.maybe) {
+                                {
+                                    const double* w = X.F.weights + (size_t)b * X.n3;
+                                    const double* v0 = X.F.errest + (size_t)b * X.n3;
+                                    const double* y = VPOOL(X, s.iy, b);
+                                    double v[2] = {0.0, 0.0};
+                                    FOR_OWN_W(X, q) {
+                                        const double wq = ldcg(&w[q]);
+                                        v[0] += (ldcg(&v0[q]) / wq) * (ldcg(&v0[q]) / wq);
+                                        v[1] += (ldcg(&y[q]) / wq) * (ldcg(&y[q]) / wq);
+                                    }
+                                    post_reduce(X, I, b, v, 2, false);
+                                }
+                                CO_YIELD(I, L_STIFF1);
+                                I.v0v0 = I.red[0];
+                                I.scale = xmul(sqrt(I.red[1]), X.Q.sqrrmc);
+                                if (I.scale == 0.0) { I.scale = xmul(I.v0v0, X.Q.sqrrmc); I.maybe = I.scale > 0.0; }
+                            }
+                        }
+                        if (I.maybe) {
+                            if (I.v0v0 == 0.0) {
+                                {
+                                    double* v0 = X.F.errest + (size_t)b * X.n3;
+                                    const double* w = X.F.weights + (size_t)b * X.n3;
+                                    double v = 0.0;
+                                    FOR_OWN_W(X, q) { v0[q] = 1.0; const double wq = ldcg(&w[q]); v += (1.0 / wq) * (1.0 / wq); }
+                                    post_reduce(X, I, b, &v, 1, false);
+                                }
+                                CO_YIELD(I, L_STIFF2);
+                                I.v0v0 = I.red[0];
+                            }
+                            {
+                                double* v0 = X.F.errest + (size_t)b * X.n3;
+                                const double v0nrm = sqrt(I.v0v0);
+                                FOR_OWN_W(X, q) v0[q] = ldcg(&v0[q]) / v0nrm;
+                                __syncwarp();
+                                I.v0v0 = 1.0;
+                                I.rold = 0.0; I.rho = 0.0;
+                                I.root_re[0] = I.root_re[1] = I.root_im[0] = I.root_im[1] = 0.0;
+                                I.ntry = 1;
+                            }
+                            for (;;) {
+                                // v1 = J v0 (approx_jacobian), wip(v1,v1), wip(v1,v0)
+                                {
+                                    const double temp1 = I.scale / sqrt(I.v0v0);
+                                    const double* y = VPOOL(X, s.iy, b);
+                                    const double* v0 = X.F.errest + (size_t)b * X.n3;
+                                    FOR_OWN_W(X, q) put_arg(X, s.ia1, b, q, xadd(ldcg(&y[q]), xmul(temp1, ldcg(&v0[q]))));
+                                    __syncwarp();
+                                    I.tstg = temp1;
+                                }
+                                Y_RHS(I, L_STIFF_LOOP + 11, s.t, s.ia1, DST_STG + 2);
+                                s.f_count++;
+                                {
+                                    const double fac = s.h_average / I.tstg;
+                                    double* v1 = VSTG(X, 2, b);
+                                    const double* yp = VDER(X, s.dyp, b);
+                                    const double* v0 = X.F.errest + (size_t)b * X.n3;
+                                    const double* w = X.F.weights + (size_t)b * X.n3;
+                                    double v[2] = {0.0, 0.0};
+                                    FOR_OWN_W(X, q) {
+                                        const double x = xmul(fac, xsub(ldcg(&v1[q]), ldcg(&yp[q])));
+                                        v1[q] = x;
+                                        const double wq = ldcg(&w[q]);
+                                        v[0] += (x / wq) * (x / wq);
+                                        v[1] += (x / wq) * (ldcg(&v0[q]) / wq);
+                                    }
+                                    post_reduce(X, I, b, v, 2, false);
+                                }
+                                CO_YIELD(I, L_STIFF_LOOP + 12);
+                                I.v1v1 = I.red[0]; I.v1v0 = I.red[1];
+                                if (sqrt(I.v1v1) > 1.0e10 * sqrt(I.v0v0)) { I.maybe = 0; break; }
+                                if (I.ntry == 1) {
+                                    I.rold = I.v1v0 / I.v0v0;
+                                    if (fabs(I.rold) < X.Q.cubrmc) { I.maybe = 0; break; }
+                                } else {
+                                    const double ratio = I.v1v0 / I.v0v0;
+                                    I.rho = fabs(ratio);
+                                    const double det = I.v0v0 * I.v1v1 - I.v1v0 * I.v1v0;
+                                    const bool big = det == 0.0 || (fabs(det / I.v0v0) <= fabs(I.v1v1) * 1e-6 &&
+                                                                    fabs(ratio - I.rold) <= 0.001 * I.rho);
+                                    if (big) { I.root_re[0] = ratio; I.root_im[0] = 0; I.root_re[1] = 0; I.root_im[1] = 0; }
+                                    I.rold = ratio;
+                                    if (big) break;
+                                }
+                                // v2 = J v1
+                                {
+                                    const double temp1 = I.scale / sqrt(I.v1v1);
+                                    const double* y = VPOOL(X, s.iy, b);
+                                    const double* v1 = VSTG(X, 2, b);
+                                    FOR_OWN_W(X, q) put_arg(X, s.ia1, b, q, xadd(ldcg(&y[q]), xmul(temp1, ldcg(&v1[q]))));
+                                    __syncwarp();
+                                    I.tstg = temp1;
+                                }
+                                Y_RHS(I, L_STIFF_LOOP + 21, s.t, s.ia1, DST_STG + 3);
+                                s.f_count++;
+                                {
+                                    const double fac = s.h_average / I.tstg;
+                                    double* v2 = VSTG(X, 3, b);
+                                    const double* yp = VDER(X, s.dyp, b);
+                                    const double* v0 = X.F.errest + (size_t)b * X.n3;
+                                    const double* v1 = VSTG(X, 2, b);
+                                    const double* w = X.F.weights + (size_t)b * X.n3;
+                                    double v[3] = {0.0, 0.0, 0.0};
+                                    FOR_OWN_W(X, q) {
+                                        const double x = xmul(fac, xsub(ldcg(&v2[q]), ldcg(&yp[q])));
+                                        v2[q] = x;
+                                        const double wq = ldcg(&w[q]);
+                                        v[0] += (x / wq) * (x / wq);
+                                        v[1] += (x / wq) * (ldcg(&v0[q]) / wq);
+                                        v[2] += (x / wq) * (ldcg(&v1[q]) / wq);
+                                    }
+                                    post_reduce(X, I, b, v, 3, false);
+                                }
+                                CO_YIELD(I, L_STIFF_LOOP + 22);
+                                I.v2v2 = I.red[0]; I.v2v0 = I.red[1]; I.v2v1 = I.red[2];
+                                {
+                                    const double ratio = I.v2v1 / I.v1v1;
+                                    I.rho = fabs(ratio);
+                                    const double det = I.v1v1 * I.v2v2 - I.v2v1 * I.v2v1;
+                                    const bool big = det == 0.0 || (fabs(det / I.v1v1) <= fabs(I.v2v2) * 1e-6 &&
+                                                                    fabs(ratio - I.rold) <= 0.001 * I.rho);
+                                    if (big) { I.root_re[0] = ratio; I.root_im[0] = 0; I.root_re[1] = 0; I.root_im[1] = 0; }
+                                    I.rold = ratio;
+                                    if (big) break;
+                                    const double det1 = I.v0v0 * I.v1v1 - I.v1v0 * I.v1v0;
+                                    I.alpha1 = (-I.v0v0 * I.v2v1 + I.v1v0 * I.v2v0) / det1;
+                                    I.beta1 = (I.v1v0 * I.v2v1 - I.v1v1 * I.v2v0) / det1;
+                                }
+                                // v3 = J v2
+                                {
+                                    const double temp1 = I.scale / sqrt(I.v2v2);
+                                    const double* y = VPOOL(X, s.iy, b);
+                                    const double* v2 = VSTG(X, 3, b);
+                                    FOR_OWN_W(X, q) put_arg(X, s.ia1, b, q, xadd(ldcg(&y[q]), xmul(temp1, ldcg(&v2[q]))));
+                                    __syncwarp();
+                                    I.tstg = temp1;
+                                }
+                                Y_RHS(I, L_STIFF_LOOP + 31, s.t, s.ia1, DST_STG + 4);
+                                s.f_count++;
+                                {
+                                    const double fac = s.h_average / I.tstg;
+                                    double* v3 = VSTG(X, 4, b);
+                                    const double* yp = VDER(X, s.dyp, b);
+                                    const double* v1 = VSTG(X, 2, b);
+                                    const double* v2 = VSTG(X, 3, b);
+                                    const double* w = X.F.weights + (size_t)b * X.n3;
+                                    double v[3] = {0.0, 0.0, 0.0};
+                                    FOR_OWN_W(X, q) {
+                                        const double x = xmul(fac, xsub(ldcg(&v3[q]), ldcg(&yp[q])));
+                                        v3[q] = x;
+                                        const double wq = ldcg(&w[q]);
+                                        v[0] += (x / wq) * (x / wq);
+                                        v[1] += (x / wq) * (ldcg(&v1[q]) / wq);
+                                        v[2] += (x / wq) * (ldcg(&v2[q]) / wq);
+                                    }
+                                    post_reduce(X, I, b, v, 3, false);
+                                }
+                                CO_YIELD(I, L_STIFF_LOOP + 32);
+                                I.v3v3 = I.red[0]; I.v3v1 = I.red[1]; I.v3v2 = I.red[2];
+                                {
+                                    const double ratio = I.v3v2 / I.v2v2;
+                                    I.rho = fabs(ratio);
+                                    const double det = I.v2v2 * I.v3v3 - I.v3v2 * I.v3v2;
+                                    const bool big = det == 0.0 || (fabs(det / I.v2v2) <= fabs(I.v3v3) * 1e-6 &&
+                                                                    fabs(ratio - I.rold) <= 0.001 * I.rho);
+                                    if (big) { I.root_re[0] = ratio; I.root_im[0] = 0; I.root_re[1] = 0; I.root_im[1] = 0; }
+                                    I.rold = ratio;
+                                    if (big) break;
+                                    const double det2 = I.v1v1 * I.v2v2 - I.v2v1 * I.v2v1;
+                                    const double alpha2 = (-I.v1v1 * I.v3v2 + I.v2v1 * I.v3v1) / det2;
+                                    const double beta2 = (I.v2v1 * I.v3v2 - I.v2v2 * I.v3v1) / det2;
+                                    const double res2 = fabs(I.v3v3 + alpha2 * I.v3v2 + beta2 * I.v3v1 + alpha2 * I.v3v2 +
+                                                             alpha2 * alpha2 * I.v2v2 + alpha2 * beta2 * I.v2v1 + beta2 * I.v3v1 +
+                                                             beta2 * alpha2 * I.v2v1 + beta2 * beta2 * I.v1v1);
+                                    if (res2 <= fabs(I.v3v3) * 1e-6) {
+                                        // quadratic roots (both roots as tabulated in the vendored code)
+                                        double pr_re, pr_im, r_re, r_im;
+                                        {
+                                            const double tmp = I.alpha1 / 2.0;
+                                            const double x = tmp * tmp - I.beta1;
+                                            const double sgn = signbit(tmp * 0.0 + 0.0 * tmp) ? -1.0 : 1.0;
+                                            const double sre = x >= 0 ? sqrt(x) : 0.0, sim = x >= 0 ? 0.0 : sgn * sqrt(-x);
+                                            if (sre == 0.0 && sim == 0.0) { pr_re = -tmp; pr_im = 0.0; }
+                                            else { pr_re = -tmp + sre; pr_im = sim; }
+                                        }
+                                        {
+                                            const double tmp = alpha2 / 2.0;
+                                            const double x = tmp * tmp - beta2;
+                                            const double sgn = signbit(tmp * 0.0 + 0.0 * tmp) ? -1.0 : 1.0;
+                                            const double sre = x >= 0 ? sqrt(x) : 0.0, sim = x >= 0 ? 0.0 : sgn * sqrt(-x);
+                                            if (sre == 0.0 && sim == 0.0) { r_re = -tmp; r_im = 0.0; }
+                                            else { r_re = -tmp + sre; r_im = sim; }
+                                        }
+                                        I.root_re[0] = I.root_re[1] = r_re;
+                                        I.root_im[0] = I.root_im[1] = r_im;
+                                        I.rho = hypot(pr_re, pr_im);
+                                        const double dist = hypot(r_re - pr_re, r_im - pr_im);
+                                        if (dist <= 0.001 * I.rho) break;
+                                    }
+                                }
+                                I.ntry++;
+                                if (I.ntry > 8) { I.maybe = 0; break; }
+                                {
+                                    const double v3nrm = sqrt(I.v3v3);
+                                    double* v0 = X.F.errest + (size_t)b * X.n3;
+                                    const double* v3 = VSTG(X, 4, b);
+                                    FOR_OWN_W(X, q) v0[q] = ldcg(&v3[q]) / v3nrm;
+                                    __syncwarp();
+                                    I.v0v0 = 1.0;
+                                }
+                            }
+                            if (I.maybe) {
+                                if (I.root_re[0] < 0.0) {
+                                    if (!(hypot(I.root_re[1], I.root_im[1]) >= 0.9 * I.rho && I.root_re[1] > 0.0)) {
+                                        if (fabs(I.root_im[0]) <= fabs(I.root_re[0]) * 5.2) I.sure = I.rho >= 0.9 * 3.9;
+                                    }
+                                }
+                            }
+                        }
+                        if (I.sure) I.ier = 4;
+                        if (I.ier != 1) break;
+                    }
+                    // ---------------- step_r1 (one attempt with phase-2 restarts)
+                    I.htry = s.h;
+                    for (;;) {
+                        if (s.phase2) {
+                            double* w = X.F.weights + (size_t)b * X.n3;
+                            const double* y = VPOOL(X, s.iy, b);
+                            FOR_OWN_W(X, q) w[q] = fmax(thr, fabs(ldcg(&y[q])));
+                            __syncwarp();
+                        }
+                        I.flag = 0;   // restart marker
+                        for (I.i_stage = 2; I.i_stage <= 8; ++I.i_stage) {
+                            {
+                                const int i = I.i_stage;
+                                const int argi = (i & 1) ? s.ia1 : s.ia0;
+                                const double* y = VPOOL(X, s.iy, b);
+                                const double* yp = VDER(X, s.dyp, b);
+                                double* es = X.F.errest + (size_t)b * X.n3;
+                                double lm = 0.0;
+                                FOR_OWN_W(X, q) {
+                                    double e = xmul(cB.a[i][1], ldcg(&yp[q]));
+                                    for (int j = 2; j <= i - 1; ++j) {
+                                        const double aij = cB.a[i][j];
+                                        if (aij == 0.0) continue;
+                                        e = xadd(e, xmul(aij, ldcg(&VSTG(X, j, b)[q])));
+                                    }
+                                    const double yq = ldcg(&y[q]);
+                                    const double yn = xadd(yq, xmul(I.htry, e));
+                                    put_arg(X, argi, b, q, yn);
+                                    if (i == 8) es[q] = e;
+                                    if (i == 7) {
+                                        double v = xmul(cB.e[1], ldcg(&yp[q]));
+                                        v = xadd(v, xmul(cB.e[3], ldcg(&VSTG(X, 3, b)[q])));
+                                        v = xadd(v, xmul(cB.e[4], ldcg(&VSTG(X, 4, b)[q])));
+                                        v = xadd(v, xmul(cB.e[5], ldcg(&VSTG(X, 5, b)[q])));
+                                        v = xadd(v, xmul(cB.e[6], ldcg(&VSTG(X, 6, b)[q])));
+                                        const double wq = fmax(xmul(0.5, xadd(fabs(yq), fabs(yn))), thr);
+                                        lm = fmax(lm, fabs(v) / wq);
+                                    }
+                                }
+                                __syncwarp();
+                                if (i == 7) post_reduce(X, I, b, &lm, 1, true);
+                                I.tstg = xadd(s.t, xmul(cB.c[i], I.htry));
+                                if (s.at_t_end && cB.c[i] == 1.0) I.tstg = s.t_end;
+                            }
+                            if (I.i_stage == 7) {
+                                CO_YIELD(I, L_STEPB);
+                                I.err = xmul(fabs(s.h), I.red[0]);
+                                if (I.err > s.tol) break;
+                            }
+                            Y_RHS(I, L_STAGE, I.tstg, (I.i_stage & 1) ? s.ia1 : s.ia0,
+                                  I.i_stage == 8 ? DST_DERIV + s.d8 : DST_STG + I.i_stage);
+                            s.f_count++;
+                            if (s.phase2 && I.i_stage <= 3 && fabs(I.htry) > I.hmin) {
+                                {
+                                    const int argi = (I.i_stage & 1) ? s.ia1 : s.ia0;
+                                    const double* yn = VPOOL(X, argi, b);
+                                    const double* y = VPOOL(X, s.iy, b);
+                                    const double* yp = VDER(X, s.dyp, b);
+                                    const double* out = VSTG(X, I.i_stage, b);
+                                    double* w = X.F.weights + (size_t)b * X.n3;
+                                    double m4[4] = {0.0, 0.0, 0.0, 0.0};
+                                    FOR_OWN_W(X, q) {
+                                        const double ynq = ldcg(&yn[q]), yq = ldcg(&y[q]);
+                                        const double wq = fmax(ldcg(&w[q]), fabs(ynq));
+                                        w[q] = wq;
+                                        m4[0] = fmax(m4[0], fabs(yq) / wq);
+                                        m4[1] = fmax(m4[1], fabs(ynq) / wq);
+                                        m4[2] = fmax(m4[2], fabs(xsub(ynq, yq)) / wq);
+                                        m4[3] = fmax(m4[3], fabs(xsub(ldcg(&out[q]), ldcg(&yp[q]))) / wq);
+                                    }
+                                    post_reduce(X, I, b, m4, 4, true);
+                                }
+                                CO_YIELD(I, L_STEPA);
+                                {
+                                    double ynrm = I.red[0], ystgnm = I.red[1], argdif = I.red[2];
+                                    const double fdiff = I.red[3];
+                                    const double tdiff = xsub(I.tstg, s.t);
+                                    const double twt = fabs(xsub(s.t_end, s.t));
+                                    ynrm = fmax(ynrm, fabs(s.t) / twt);
+                                    ystgnm = fmax(ystgnm, fabs(I.tstg) / twt);
+                                    argdif = fmax(argdif, fabs(tdiff) / twt);
+                                    bool cutbak = false;
+                                    if (argdif > xmul(X.Q.round_off, fmax(ynrm, ystgnm))) {
+                                        if (xmul(fabs(I.htry), fdiff) > xmul(3.9, argdif)) {
+                                            const double scl = fmax(0.125, fmin(0.5, xmul(3.9, argdif) / xmul(fabs(I.htry), fdiff)));
+                                            I.htry = xmul(scl, I.htry);
+                                            cutbak = true;
+                                        }
+                                    }
+                                    if (cutbak) {
+                                        s.at_t_end = 0;
+                                        if (fabs(I.htry) <= I.hmin) { I.htry = copysign(I.hmin, I.htry); s.phase2 = 0; }
+                                        I.flag = 1;
+                                    }
+                                }
+                                if (I.flag) break;
+                            }
+                        }
+                        if (I.flag) continue;        // phase-2 restart
+                        if (I.i_stage == 7) break;   // early rejection by stepb (err set)
+                        {
+                            const double* y = VPOOL(X, s.iy, b);
+                            const double* yp = VDER(X, s.dyp, b);
+                            const double* yn = VPOOL(X, s.ia0, b);
+                            const double* k8 = VDER(X, s.d8, b);
+                            double* es = X.F.errest + (size_t)b * X.n3;
+                            double* w = X.F.weights + (size_t)b * X.n3;
+                            double lm = 0.0;
+                            FOR_OWN_W(X, q) {
+                                double v = ldcg(&es[q]);
+                                v = xsub(v, xmul(cB.b[1], ldcg(&yp[q])));
+                                for (int i = 2; i <= 7; ++i) {
+                                    if (cB.b[i] == 0.0) continue;
+                                    v = xsub(v, xmul(cB.b[i], ldcg(&VSTG(X, i, b)[q])));
+                                }
+                                v = xsub(v, xmul(cB.b[8], ldcg(&k8[q])));
+                                v = xmul(I.htry, v);
+                                es[q] = v;
+                                const double wq = fmax(xmul(0.5, xadd(fabs(ldcg(&y[q])), fabs(ldcg(&yn[q])))), thr);
+                                w[q] = wq;
+                                lm = fmax(lm, fabs(v) / wq);
+                            }
+                            post_reduce(X, I, b, &lm, 1, true);
+                        }
+                        CO_YIELD(I, L_FINAL);
+                        I.err = I.red[0];
+                        break;
+                    }
+                    s.h = I.htry;
+                    {
+                        double alpha;
+                        if (I.err > s.tol) {
+                            if (s.at_t_start) { I.phase3 = 0; alpha = 0.5; }
+                            else {
+                                s.bad_step_count++;
+                                s.stiff_bad_step_count++;
+                                alpha = I.failed ? 0.5 : fmax(xmul(0.8, pow(s.tol / I.err, 0.2)), 0.5);
+                            }
+                            s.h = xmul(alpha, s.h);
+                            I.failed = 1;
+                            continue;
+                        }
+                        double beta = pow(I.err / s.tol, 0.2);
+                        if (!s.at_t_start) {
+                            const double t1 = pow(I.err, 0.2) / s.h;
+                            const double t2 = pow(s.errold, 0.2) / s.h_old;
+                            if (t1 < xmul(t2, 100.0) && t2 < xmul(t1, 100.0)) beta = xmul(beta, t1 / t2);
+                        }
+                        alpha = 8.0;
+                        if (0.8 < xmul(beta, alpha)) alpha = 0.8 / beta;
+                        if (s.at_t_start) {
+                            s.phase2 = 0;
+                            I.phase3 = I.phase3 && !s.at_t_end && (alpha > 4.0);
+                            if (I.phase3) { s.h = xmul(alpha, s.h); continue; }
+                        }
+                        alpha = fmin(alpha, 2.0);
+                        if (I.failed) alpha = fmin(alpha, 1.0);
+                        alpha = fmax(alpha, 0.5);
+                        s.h_old = s.h;
+                        s.h = xmul(alpha, s.h);
+                        if (s.at_t_start) s.h_average = s.h_old;
+                        else s.h_average = xadd(xmul(0.9, s.h_average), xmul(0.1, s.h_old));
+                        s.at_t_start = 0;
+                        s.errold = I.err;
+                        s.t_old = s.t;
+                        if (s.at_t_end) s.t = s.t_end; else s.t = xadd(s.t, s.h_old);
+                        s.step_count++;
+                        const int oy = s.iy, oyo = s.iyold, oa0 = s.ia0;
+                        s.iyold = oy; s.iy = oa0; s.ia0 = oyo;
+                        const int dp = s.dyp, dpo = s.dypold, d8 = s.d8;
+                        s.dypold = dp; s.dyp = d8; s.d8 = dpo;
+                        if (X.Q.renorm) {
+                            double* v = VPOOL(X, s.iy, b);
+                            const int n = X.P.n;
+                            for (int cell = X.lane; cell < X.nc; cell += 32) {
+                                const int i = X.c0 + cell;
+                                const double x = v[i], y = v[n + i], z = v[2 * n + i];
+                                const double r = sqrt(xadd(xadd(xmul(x, x), xmul(y, y)), xmul(z, z)));
+                                if (r > 0.0) { v[i] = x / r; v[n + i] = y / r; v[2 * n + i] = z / r; }
+                            }
+                            __syncwarp();
+                        }
+                    }
+                    break;
+                }
+            }
+            s.at_t_end = s.t == s.t_end;
+            s.chkeff = s.at_t_end;
+            if (I.ier == 1) { s.intrp_ready = 0; continue; }
+            if (I.ier >= 911) { s.status = I.ier; s.finished = 1; break; }
+            // flag 2..5: return y at the current internal time
+            {
+                const double* y = VPOOL(X, s.iy, b);
+                double* dst = I.dst_slot ? X.F.y_out ? X.F.y_out + ((size_t)b * X.Q.nt + s.ko) * X.n3 : VONE(X, X.F.ystep, b)
+                                         : VONE(X, X.F.ystep, b);
+                copy_own(X, y, dst);
+                I.t_got = s.t;
+                I.flag = I.ier;
+            }
+            break;
+        }
+        if (s.finished) break;
+        s.tlast = I.t_got;
+        if (I.flag == 3) s.n_flag3++;
+        if (I.flag == 4) s.n_flag4++;
+        if (I.flag == 5 || I.flag == 2) s.status = I.flag;
+        if (I.cf & 2) {
+            {
+                const double* dst = I.dst_slot ? X.F.y_out ? X.F.y_out + ((size_t)b * X.Q.nt + s.ko) * X.n3 : VONE(X, X.F.ystep, b)
+                                               : VONE(X, X.F.ystep, b);
+                const double* yl = VONE(X, X.F.ylast, b);
+                double ce = 0.0;
+                FOR_OWN_W(X, q) ce = fmax(ce, fabs(xsub(ldcg(&dst[q]), ldcg(&yl[q]))));
+                post_reduce(X, I, b, &ce, 1, true);
+            }
+            CO_YIELD(I, L_CONV);
+            {
+                const double* dst = I.dst_slot ? X.F.y_out ? X.F.y_out + ((size_t)b * X.Q.nt + s.ko) * X.n3 : VONE(X, X.F.ystep, b)
+                                               : VONE(X, X.F.ystep, b);
+                if (I.red[0] < X.Q.conv_tol) {
+                    if (s.ko < X.Q.nt) {
+                        if (!I.dst_slot && X.F.y_out) copy_own(X, dst, X.F.y_out + ((size_t)b * X.Q.nt + s.ko) * X.n3);
+                        if (X.cb == 0 && X.lane == 0) {
+                            X.F.t_out[(size_t)b * X.Q.nt + s.ko] = I.t_got;
+                            X.F.flags_out[(size_t)b * X.Q.nt + s.ko] = I.flag;
+                        }
+                    }
+                    s.converged_at = s.ko;
+                    s.finished = 1;
+                    s.ci++;
+                    break;
+                }
+                copy_own(X, dst, VONE(X, X.F.ylast, b));
+            }
+        }
+        if (I.dst_slot) {
+            if (X.cb == 0 && X.lane == 0) {
+                X.F.t_out[(size_t)b * X.Q.nt + s.ko] = I.t_got;
+                X.F.flags_out[(size_t)b * X.Q.nt + s.ko] = I.flag;
+            }
+            s.ko++;
+        }
+        s.ci++;
+        if (s.status) { s.finished = 1; break; }
+    }
+    I.req = 3;
+    I.pc = L_DONE;
+    return;
+    case L_DONE:
+        I.req = 3;
+        return;
+    default:
+        break;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// LL epilogue for one instance on the owned cells: sum the S partial demag
+// products and write f to the requested destination.
+// ---------------------------------------------------------------------------
+MT_DEV void epilogue(const BCtx& X, BInst& I, int b)
+{
+    const int n = X.P.n;
+    const TimeScalars ts = inst_scalars(X, b, I.t_rhs);
+    const double* m = VPOOL(X, I.rhs_arg, b);
+    double* out = dst_ptr(X, I.rhs_dst, b);
+    for (int cell = X.lane; cell < X.nc; cell += 32) {
+        const int i = X.c0 + cell;
+        float S[3];
+        for (int a = 0; a < 3; ++a) {
+            float acc = 0.f;
+            for (int sp = 0; sp < X.Q.S; ++sp)
+                acc += ldcg(&X.F.hpart[(((size_t)sp * X.Q.Bp + b) * 3 + a) * X.Q.np + i]);
+            S[a] = acc;
+        }
+        double o[3];
+        cell_rhs(X.P, m, i, S, ts, o);
+        out[i] = o[0]; out[n + i] = o[1]; out[2 * n + i] = o[2];
+    }
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// FP32 SIMT demag tile: H[s][inst][a][cell] for cells of block cb, instances of
+// block ib, sources of split s, from the cell-row FP32 tensor.
+// ---------------------------------------------------------------------------
+constexpr int kSimtJT = 16;
+
+MT_DEV void gemm_tile_simt(const BCtx& X)
+{
+    const int ldk = X.P.ldk, n = X.P.n;
+    float* Ks = reinterpret_cast<float*>(X.smem);        // [6][JT][128]
+    float* Ms = Ks + 6 * kSimtJT * kCellBlock;             // [JT][3][64]
+    const int tid = threadIdx.x;
+    const int tc = tid & 31, ti = tid >> 5;                // 32 cell groups x 16 instance groups
+    const int cbase = X.cb * kCellBlock, ibase = X.ib * kInstBlock;
+    const int j4tot = ldk >> 2;
+    const int js = (int)(((long long)j4tot * X.s) / X.Q.S) * 4;
+    const int je = (int)(((long long)j4tot * (X.s + 1)) / X.Q.S) * 4;
+    float acc[4][4][3];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) acc[q][r][0] = acc[q][r][1] = acc[q][r][2] = 0.f;
+    for (int j0 = js; j0 < je; j0 += kSimtJT) {
+        const int len = min(kSimtJT, je - j0);   // multiple of 4
+        __syncthreads();
+        // K rows: 128 cells x 6 comps x len floats
+        for (int e = tid; e < kCellBlock * 6 * (kSimtJT / 4); e += blockDim.x) {
+            const int cell = e / (6 * (kSimtJT / 4));
+            const int rem = e - cell * 6 * (kSimtJT / 4);
+            const int c = rem / (kSimtJT / 4), j4 = rem - c * (kSimtJT / 4);
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (cbase + cell < n && 4 * j4 < len)
+                v = __ldg(reinterpret_cast<const float4*>(X.P.K + ((size_t)(cbase + cell) * 6 + c) * ldk + j0) + j4);
+            float* d = Ks + (c * kSimtJT + 4 * j4) * kCellBlock + cell;
+            d[0] = v.x; d[kCellBlock] = v.y; d[2 * kCellBlock] = v.z; d[3 * kCellBlock] = v.w;
+        }
+        for (int e = tid; e < kInstBlock * 3 * (kSimtJT / 4); e += blockDim.x) {
+            const int inst = e / (3 * (kSimtJT / 4));
+            const int rem = e - inst * 3 * (kSimtJT / 4);
+            const int bb = rem / (kSimtJT / 4), j4 = rem - bb * (kSimtJT / 4);
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (4 * j4 < len)
+                v = __ldcg(reinterpret_cast<const float4*>(X.F.m32 + ((size_t)(ibase + inst) * 3 + bb) * ldk + j0) + j4);
+            float* d = Ms + ((4 * j4) * 3 + bb) * kInstBlock + inst;
+            d[0] = v.x; d[3 * kInstBlock] = v.y; d[6 * kInstBlock] = v.z; d[9 * kInstBlock] = v.w;
+        }
+        __syncthreads();
+        for (int jj = 0; jj < len; ++jj) {
+            float kv[4][6], mv[4][3];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int c = 0; c < 6; ++c) kv[q][c] = Ks[(c * kSimtJT + jj) * kCellBlock + tc + 32 * q];
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int bb = 0; bb < 3; ++bb) mv[r][bb] = Ms[(jj * 3 + bb) * kInstBlock + ti + 16 * r];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    acc[q][r][0] += kv[q][0] * mv[r][0] + kv[q][1] * mv[r][1] + kv[q][2] * mv[r][2];
+                    acc[q][r][1] += kv[q][1] * mv[r][0] + kv[q][3] * mv[r][1] + kv[q][4] * mv[r][2];
+                    acc[q][r][2] += kv[q][2] * mv[r][0] + kv[q][4] * mv[r][1] + kv[q][5] * mv[r][2];
+                }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const int cell = cbase + tc + 32 * q, inst = ibase + ti + 16 * r;
+                X.F.hpart[(((size_t)X.s * X.Q.Bp + inst) * 3 + a) * X.Q.np + cell] = acc[q][r][a];
+            }
+}
+
+constexpr int kMaxInstPerWarp = 4;
+
+MT_DEV size_t batch_gemm_smem(int prec)
+{
+    return prec == kPrecFP32 ? (size_t)(6 * kSimtJT * kCellBlock + kSimtJT * 3 * kInstBlock) * sizeof(float)
+                             : tc_smem_bytes();
+}
+
+__global__ void __launch_bounds__(kBatchThreads, 1)
+batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMaps maps)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    BCtx X;
+    X.P = P; X.F = F; X.Q = Q;
+    const int t = blockIdx.x;
+    X.s = t % Q.S;
+    X.ib = (t / Q.S) % Q.IB;
+    X.cb = t / (Q.S * Q.IB);
+    X.c0 = X.cb * kCellBlock;
+    X.nc = min(kCellBlock, P.n - X.c0);
+    const int per = kInstBlock / Q.S;
+    X.i0 = X.ib * kInstBlock + X.s * per;
+    X.ni = per;
+    X.n3 = 3 * (size_t)P.n;
+    X.lane = threadIdx.x & 31;
+    X.warp = threadIdx.x >> 5;
+    X.nwarps = blockDim.x >> 5;
+    X.smem = smem_raw;
+    const bool tc = Q.prec != kPrecFP32;
+    TcState tcs;
+    tcs.kb_done = 0; tcs.tiles = 0; tcs.tmem = 0;
+    if (tc) tc_init_impl(X.smem, tcs);
+    // each lane keeps its own (identical) copy of the coroutines of its warp
+    BInst L[kMaxInstPerWarp];
+    int mine = 0;
+    for (int li = X.warp; li < X.ni && mine < kMaxInstPerWarp; li += X.nwarps, ++mine) {
+        const long long* src = reinterpret_cast<const long long*>(&F.inst[(size_t)X.cb * Q.Bp + X.i0 + li]);
+        long long* dst = reinterpret_cast<long long*>(&L[mine]);
+        for (int w = 0; w < (int)(sizeof(BInst) / 8); ++w) dst[w] = __ldcg(src + w);
+        if (L[mine].req == 4) L[mine].req = 0;                 // parked by the previous launch
+        L[mine].budget_mark = L[mine].s.full_f_count + L[mine].s.f_count + Q.evals_budget;
+    }
+    bool ok = true;
+    if (Q.demag_only) {
+        // one product of the operands already in place, then H = -Ms * sum of partials
+        if (!tc) gemm_tile_simt(X);
+        else ok = tc_gemm_tile_impl(X.smem, Q, F, maps, X.cb, X.ib, X.s, Q.prec == kPrecBF16x3, tcs);
+        if (ok && grid_sync(F.gs, 5)) {
+            const int n = P.n;
+            for (int e = threadIdx.x; e < X.ni * 3 * X.nc; e += blockDim.x) {
+                const int li = e / (3 * X.nc), rem = e - li * 3 * X.nc;
+                const int a = rem / X.nc, i = X.c0 + (rem - a * X.nc);
+                const int b = X.i0 + li;
+                if (b >= Q.B) continue;
+                float acc = 0.f;
+                for (int sp = 0; sp < Q.S; ++sp)
+                    acc += __ldcg(&F.hpart[(((size_t)sp * Q.Bp + b) * 3 + a) * Q.np + i]);
+                Q.out_h[(size_t)b * 3 * n + (size_t)a * n + i] = (double)__fmul_rn(-acc, __ldg(&P.Mfact[i]));
+            }
+        }
+        if (tc) tc_finish_impl(X.smem, tcs);
+        return;
+    }
+    for (long long tick = 0; tick < Q.ticks_per_launch && ok; ++tick) {
+        unsigned* ctr = F.counters + 2 * (tick % 3);
+        // P2: resolve reductions, advance
+        int my_active = 0, my_rhs = 0;
+        for (int k = 0; k < mine; ++k) {
+            BInst& I = L[k];
+            const int b = X.i0 + X.warp + k * X.nwarps;
+            if (b >= Q.B) continue;
+            if (I.req == 2) resolve_reduce(X, I, b);
+            if (I.req == 0) advance(X, I, b);
+            if (I.req != 3 && I.req != 4) my_active++;
+            if (I.req == 1) my_rhs++;
+        }
+        asm volatile("fence.proxy.async.global;" ::: "memory");   // operand stores -> TMA reads
+        if (X.lane == 0 && X.cb == 0 && (my_active | my_rhs)) {
+            atomicAdd(&ctr[0], (unsigned)my_active);
+            atomicAdd(&ctr[1], (unsigned)my_rhs);
+        }
+        if (!grid_sync(F.gs, 1)) { ok = false; break; }
+        const unsigned active = __ldcg(&ctr[0]);
+        const unsigned nreq = __ldcg(&ctr[1]);
+        if (t == 0 && threadIdx.x == 0) {
+            unsigned* nxt = F.counters + 2 * ((tick + 1) % 3);
+            nxt[0] = 0; nxt[1] = 0;
+        }
+        if (active == 0) break;
+        if (nreq > 0) {
+            if (!tc) gemm_tile_simt(X);
+            else if (!tc_gemm_tile_impl(X.smem, Q, F, maps, X.cb, X.ib, X.s, Q.prec == kPrecBF16x3, tcs)) ok = false;
+        }
+        if (!grid_sync(F.gs, 2)) { ok = false; break; }
+        if (!ok) break;
+        // P1: epilogue for right-hand-side requests, advance
+        for (int k = 0; k < mine; ++k) {
+            BInst& I = L[k];
+            const int b = X.i0 + X.warp + k * X.nwarps;
+            if (b >= Q.B || I.req != 1) continue;
+            epilogue(X, I, b);
+            I.req = 0;
+            advance(X, I, b);
+        }
+        if (!grid_sync(F.gs, 3)) { ok = false; break; }
+    }
+    if (tc) tc_finish_impl(X.smem, tcs);
+    if (ok && X.lane == 0) {
+        for (int k = 0; k < mine; ++k) {
+            const int li = X.warp + k * X.nwarps;
+            long long* dst = reinterpret_cast<long long*>(&F.inst[(size_t)X.cb * Q.Bp + X.i0 + li]);
+            const long long* src = reinterpret_cast<const long long*>(&L[k]);
+            for (int w = 0; w < (int)(sizeof(BInst) / 8); ++w) dst[w] = src[w];
+        }
+    }
+}
+
+// FP32 cell-row tensor -> BF16 hi/lo [3np][Kd] (rows (a,i), cols (b,j)), zero padded
+__global__ void split_tensor_kernel(const float* __restrict__ K, int n, int ldk, int np, uint16_t* __restrict__ khi,
+                                    uint16_t* __restrict__ klo)
+{
+    const int Kd = 3 * np;
+    const size_t tot = (size_t)Kd * Kd;
+    static const int blk[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+        const int row = (int)(e / Kd), col = (int)(e - (size_t)row * Kd);
+        const int a = row / np, i = row - a * np, bb = col / np, j = col - bb * np;
+        float v = 0.f;
+        if (i < n && j < n) v = K[((size_t)i * 6 + blk[a][bb]) * ldk + j];
+        const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+        khi[e] = __bfloat16_as_ushort(hi);
+        klo[e] = __bfloat16_as_ushort(lo);
+    }
+}
+
+// m (B x 3n FP64) -> GEMM operand of every instance
+__global__ void batch_operand_kernel(const double* __restrict__ m, int B, int n, int ldk, int np, int prec,
+                                     float* __restrict__ m32, uint16_t* __restrict__ mhi, uint16_t* __restrict__ mlo)
+{
+    const size_t tot = (size_t)B * 3 * n;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+        const int b = (int)(e / (3 * (size_t)n));
+        const int q = (int)(e - (size_t)b * 3 * n);
+        const int a = q / n, i = q - a * n;
+        const float f = (float)m[e];
+        if (prec == kPrecFP32) {
+            m32[((size_t)b * 3 + a) * ldk + i] = f;
+        } else {
+            const size_t col = (size_t)b * 3 * np + (size_t)a * np + i;
+            const __nv_bfloat16 hi = __float2bfloat16_rn(f);
+            const __nv_bfloat16 lo = __float2bfloat16_rn(f - __bfloat162float(hi));
+            mhi[col] = __bfloat16_as_ushort(hi);
+            mlo[col] = __bfloat16_as_ushort(lo);
+        }
+    }
+}
+
+}  // namespace
+
+static void bs45b_fill(BS45b& T);
+
+cudaError_t launch_batch_operand(const double* m, int B, int n, int ldk, int np, int prec, float* m32, uint16_t* mhi,
+                                 uint16_t* mlo, cudaStream_t s)
+{
+    batch_operand_kernel<<<592, 256, 0, s>>>(m, B, n, ldk, np, prec, m32, mhi, mlo);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_upload_tables()
+{
+    static BS45b T;
+    bs45b_fill(T);
+    return cudaMemcpyToSymbol(cB, &T, sizeof(T));
+}
+
+int batch_grid(int n, int B, int num_sms, int prec, int* CB, int* IB, int* S)
+{
+    (void)prec;
+    *CB = (n + kCellBlock - 1) / kCellBlock;
+    *IB = (B + kInstBlock - 1) / kInstBlock;
+    const int tiles = (*CB) * (*IB);
+    int s = num_sms / tiles;
+    if (s > 4) s = 4;
+    if (s < 1) s = 1;
+    // the source range of every split is a whole number of 32-wide k-blocks
+    const int Kd = 3 * (*CB) * kCellBlock;
+    while (s > 1 && (Kd % (32 * s)) != 0) --s;
+    *S = s;
+    return tiles * s;
+}
+
+size_t batch_smem_bytes(int n, int ldk, int prec)
+{
+    (void)n; (void)ldk;
+    return prec == kPrecFP32 ? (size_t)(6 * kSimtJT * kCellBlock + kSimtJT * 3 * kInstBlock) * sizeof(float)
+                             : tc_smem_bytes();
+}
+
+cudaError_t launch_batch(const DevProb& P, const BatchBufs& Bf, const BatchParams& Q, int grid, const void* tmaps,
+                         cudaStream_t s)
+{
+    const size_t smem = batch_smem_bytes(P.n, P.ldk, Q.prec);
+    cudaError_t e = cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    DevProb p = P;
+    BatchBufs b = Bf;
+    BatchParams q = Q;
+    TcMaps m;
+    memset(&m, 0, sizeof(m));
+    if (tmaps) memcpy(&m, tmaps, sizeof(m));
+    void* args[] = {&p, &b, &q, &m};
+    return cudaLaunchCooperativeKernel((const void*)batch_kernel, dim3(grid), dim3(kBatchThreads), args, smem, s);
+}
+
+cudaError_t launch_split_tensor(const float* K, int n, int ldk, int np, uint16_t* khi, uint16_t* klo, cudaStream_t s)
+{
+    split_tensor_kernel<<<1184, 256, 0, s>>>(K, n, ldk, np, khi, klo);
+    return cudaGetLastError();
+}
+
+static void bs45b_fill(BS45b& T)
+{
+    memset(&T, 0, sizeof(T));
+    auto& a = T.a;
+    a[2][1] = 1.0 / 6.0;
+    a[3][1] = 2.0 / 27.0; a[3][2] = 4.0 / 27.0;
+    a[4][1] = 183.0 / 1372.0; a[4][2] = -162.0 / 343.0; a[4][3] = 1053.0 / 1372.0;
+    a[5][1] = 68.0 / 297.0; a[5][2] = -4.0 / 11.0; a[5][3] = 42.0 / 143.0; a[5][4] = 1960.0 / 3861.0;
+    a[6][1] = 597.0 / 22528.0; a[6][2] = 81.0 / 352.0; a[6][3] = 63099.0 / 585728.0;
+    a[6][4] = 58653.0 / 366080.0; a[6][5] = 4617.0 / 20480.0;
+    a[7][1] = 174197.0 / 959244.0; a[7][2] = -30942.0 / 79937.0; a[7][3] = 8152137.0 / 19744439.0;
+    a[7][4] = 666106.0 / 1039181.0; a[7][5] = -29421.0 / 29068.0; a[7][6] = 482048.0 / 414219.0;
+    a[8][1] = 587.0 / 8064.0; a[8][3] = 4440339.0 / 15491840.0;
+    a[8][4] = 24353.0 / 124800.0; a[8][5] = 387.0 / 44800.0; a[8][6] = 2152.0 / 5985.0;
+    a[8][7] = 7267.0 / 94080.0;
+    T.b[1] = 2479.0 / 34992.0; T.b[3] = 123.0 / 416.0; T.b[4] = 612941.0 / 3411720.0;
+    T.b[5] = 43.0 / 1440.0; T.b[6] = 2272.0 / 6561.0; T.b[7] = 79937.0 / 1113912.0; T.b[8] = 3293.0 / 556956.0;
+    T.e[1] = -3.0 / 1280.0; T.e[3] = 6561.0 / 632320.0; T.e[4] = -343.0 / 20800.0;
+    T.e[5] = 243.0 / 12800.0; T.e[6] = -1.0 / 95.0;
+    T.c[2] = 1.0 / 6.0; T.c[3] = 2.0 / 9.0; T.c[4] = 3.0 / 7.0; T.c[5] = 2.0 / 3.0; T.c[6] = 3.0 / 4.0;
+    T.c[7] = 1.0; T.c[8] = 1.0; T.c[9] = 1.0 / 2.0; T.c[10] = 5.0 / 6.0; T.c[11] = 1.0 / 9.0;
+    a[9][1] = 455.0 / 6144.0; a[10][1] = -837888343715.0 / 13176988637184.0;
+    a[11][1] = 98719073263.0 / 1551965184000.0;
+    a[10][2] = 30409415.0 / 52955362.0; a[11][2] = 1307.0 / 123552.0;
+    a[9][3] = 10256301.0 / 35409920.0; a[10][3] = -48321525963.0 / 759168069632.0;
+    a[11][3] = 4632066559387.0 / 70181753241600.0;
+    a[9][4] = 2307361.0 / 17971200.0; a[10][4] = 8530738453321.0 / 197654829557760.0;
+    a[11][4] = 7828594302389.0 / 382182512025600.0;
+    a[9][5] = -387.0 / 102400.0; a[10][5] = 1361640523001.0 / 1626788720640.0;
+    a[11][5] = 40763687.0 / 11070259200.0;
+    a[9][6] = 73.0 / 5130.0; a[10][6] = -13143060689.0 / 38604458898.0;
+    a[11][6] = 34872732407.0 / 224610586200.0;
+    a[9][7] = -7267.0 / 215040.0; a[10][7] = 18700221969.0 / 379584034816.0;
+    a[11][7] = -2561897.0 / 30105600.0;
+    a[9][8] = 1.0 / 32.0; a[10][8] = -5831595.0 / 847285792.0; a[11][8] = 1.0 / 10.0;
+    a[10][9] = -5183640.0 / 26477681.0; a[11][9] = -1.0 / 10.0;
+    a[11][10] = -1403317093.0 / 11371610250.0;
+    auto& r = T.r;
+    r[1][6] = -12134338393.0 / 1050809760.0; r[1][5] = -1620741229.0 / 50038560.0;
+    r[1][4] = -2048058893.0 / 59875200.0; r[1][3] = -87098480009.0 / 5254048800.0;
+    r[1][2] = -11513270273.0 / 3502699200.0;
+    r[3][6] = -33197340367.0 / 1218433216.0; r[3][5] = -539868024987.0 / 6092166080.0;
+    r[3][4] = -39991188681.0 / 374902528.0; r[3][3] = -69509738227.0 / 1218433216.0;
+    r[3][2] = -29327744613.0 / 2436866432.0;
+    r[4][6] = -284800997201.0 / 19905339168.0; r[4][5] = -7896875450471.0 / 165877826400.0;
+    r[4][4] = -333945812879.0 / 5671036800.0; r[4][3] = -16209923456237.0 / 497633479200.0;
+    r[4][2] = -2382590741699.0 / 331755652800.0;
+    r[5][6] = -540919.0 / 741312.0; r[5][5] = -103626067.0 / 43243200.0; r[5][4] = -633779.0 / 211200.0;
+    r[5][3] = -32406787.0 / 18532800.0; r[5][2] = -36591193.0 / 86486400.0;
+    r[6][6] = 7157998304.0 / 374350977.0; r[6][5] = 30405842464.0 / 623918295.0;
+    r[6][4] = 183022264.0 / 5332635.0; r[6][3] = -3357024032.0 / 1871754885.0;
+    r[6][2] = -611586736.0 / 89131185.0;
+    r[7][6] = -138073.0 / 9408.0; r[7][5] = -719433.0 / 15680.0; r[7][4] = -1620541.0 / 31360.0;
+    r[7][3] = -385151.0 / 15680.0; r[7][2] = -65403.0 / 15680.0;
+    r[8][6] = 1245.0 / 64.0; r[8][5] = 3991.0 / 64.0; r[8][4] = 4715.0 / 64.0; r[8][3] = 2501.0 / 64.0;
+    r[8][2] = 149.0 / 16.0; r[8][1] = 1.0;
+    r[9][6] = 55.0 / 3.0; r[9][5] = 71.0; r[9][4] = 103.0; r[9][3] = 199.0 / 3.0; r[9][2] = 16.0;
+    r[10][6] = -1774004627.0 / 75810735.0; r[10][5] = -1774004627.0 / 25270245.0;
+    r[10][4] = -26477681.0 / 359975.0; r[10][3] = -11411880511.0 / 379053675.0;
+    r[10][2] = -423642896.0 / 126351225.0;
+    r[11][6] = 35.0; r[11][5] = 105.0; r[11][4] = 117.0; r[11][3] = 59.0; r[11][2] = 12.0;
+}

@@ -19,6 +19,9 @@
 #include "fields.cuh"
 #include "integrate.cuh"
 #include "llg.cuh"
+#include "batch.cuh"
+#include "gemm_tc.cuh"
+#include <cudaTypedefs.h>
 
 namespace {
 
@@ -490,6 +493,379 @@ int mt_integrate(mt_handle* h, const double* t, int nt, const double* m0_dev, do
     stats->status = hs.status;
     stats->converged_at = hs.converged_at;
     if (hs.status != 0) return fail(MT_ERR_SOLVER, "integrator stopped with RKSUITE flag %d", hs.status);
+    return MT_OK;
+}
+
+
+// ---------------------------------------------------------------------------
+// batched instances
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+struct mt_batch {
+    mt_handle* h = nullptr;
+    int B = 0, prec = 0;
+    int CB = 0, IB = 0, S = 0, np = 0, Kd = 0, grid = 0;
+    uint16_t* khi = nullptr;
+    uint16_t* klo = nullptr;
+    double* hext = nullptr;
+    double* alpha0 = nullptr;
+    int nt_hext = 0;
+    bool have_dynamics = false;
+};
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+int get_encoder()
+{
+    if (g_encode) return MT_OK;
+    cudaDriverEntryPointQueryResult q;
+    void* fn = nullptr;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+        return fail(MT_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    return MT_OK;
+}
+
+// 2-D BF16 tensor [outer][inner] (inner contiguous), box {32, box_outer}, 64-byte swizzle
+int make_tmap(CUtensorMap* m, const void* base, uint64_t inner, uint64_t outer, uint32_t box_outer)
+{
+    int rc = get_encoder();
+    if (rc) return rc;
+    cuuint64_t dims[2] = {inner, outer};
+    cuuint64_t strides[1] = {inner * 2};
+    cuuint32_t box[2] = {(cuuint32_t)kTcKB, box_outer};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, es,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(MT_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return MT_OK;
+}
+
+DevProb batch_prob(const mt_batch* bt)
+{
+    DevProb P = make_prob(bt->h);
+    return P;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mt_batch_create(const mt_grid* g, int B, int precision, mt_batch** out)
+{
+    if (!out) return fail(MT_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (B < 1) return fail(MT_ERR_ARG, "B must be >= 1");
+    if (precision < 0 || precision > 2) return fail(MT_ERR_ARG, "unknown precision %d", precision);
+    mt_handle* h = nullptr;
+    int rc = mt_create(g, &h);
+    if (rc) return rc;
+    cudaError_t e = batch_upload_tables();
+    if (e != cudaSuccess) { mt_destroy(h); return fail(MT_ERR_CUDA, "batch tables: %s", cudaGetErrorString(e)); }
+    mt_batch* bt = new mt_batch();
+    bt->h = h;
+    bt->B = B;
+    bt->prec = precision;
+    bt->grid = batch_grid(h->n, B, h->num_sms, precision, &bt->CB, &bt->IB, &bt->S);
+    bt->np = bt->CB * kCellBlock;
+    bt->Kd = 3 * bt->np;
+    *out = bt;
+    return MT_OK;
+}
+
+int mt_batch_destroy(mt_batch* bt)
+{
+    if (!bt) return MT_OK;
+    free_ptr(bt->khi); free_ptr(bt->klo); free_ptr(bt->hext); free_ptr(bt->alpha0);
+    mt_destroy(bt->h);
+    delete bt;
+    return MT_OK;
+}
+
+int mt_batch_set_material(mt_batch* bt, double A0, const double* Ms, const double* K0, const double* u_ea)
+{
+    if (!bt) return fail(MT_ERR_ARG, "null handle");
+    return mt_set_material(bt->h, A0, Ms, K0, u_ea);
+}
+
+int mt_batch_set_dynamics(mt_batch* bt, int solver, double gamma, const double* alpha0, const double* hext, int nt_hext,
+                          int renormalize)
+{
+    if (!bt || !alpha0 || !hext || nt_hext < 1) return fail(MT_ERR_ARG, "bad argument");
+    if (solver != 1 && solver != 2) return fail(MT_ERR_UNSUPPORTED, "solver %d", solver);
+    const int Bp = bt->IB * kInstBlock;
+    std::vector<double> he((size_t)Bp * nt_hext * 4, 0.0), al(Bp, 1.0);
+    memcpy(he.data(), hext, sizeof(double) * (size_t)bt->B * nt_hext * 4);
+    memcpy(al.data(), alpha0, sizeof(double) * bt->B);
+    free_ptr(bt->hext); bt->hext = nullptr;
+    free_ptr(bt->alpha0); bt->alpha0 = nullptr;
+    CUDA_TRY(dalloc(&bt->hext, he.size()));
+    CUDA_TRY(dalloc(&bt->alpha0, al.size()));
+    CUDA_TRY(cudaMemcpy(bt->hext, he.data(), sizeof(double) * he.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(bt->alpha0, al.data(), sizeof(double) * al.size(), cudaMemcpyHostToDevice));
+    bt->nt_hext = nt_hext;
+    // the shared part (solver, gamma) lives in the inner handle; its tables are unused
+    double dummy_tab[8] = {0, 0, 0, 0, 1, 0, 0, 0};
+    int rc = mt_set_dynamics(bt->h, solver, gamma, 1.0, dummy_tab, 1, dummy_tab, 2, 0, renormalize);
+    if (rc) return rc;
+    bt->have_dynamics = true;
+    return MT_OK;
+}
+
+int mt_batch_assemble_demag(mt_batch* bt, void* stream)
+{
+    if (!bt) return fail(MT_ERR_ARG, "null handle");
+    int rc = mt_assemble_demag(bt->h, stream);
+    if (rc) return rc;
+    if (bt->prec != MT_PREC_FP32) {
+        const size_t cnt = (size_t)bt->Kd * bt->Kd;
+        if (!bt->khi) { CUDA_TRY(dalloc(&bt->khi, cnt)); CUDA_TRY(dalloc(&bt->klo, cnt)); }
+        CUDA_TRY(launch_split_tensor(bt->h->K, bt->h->n, bt->h->ldk, bt->np, bt->khi, bt->klo, (cudaStream_t)stream));
+    }
+    return MT_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+struct BatchRun {
+    IntegAlloc A;
+    BatchBufs F;
+    BatchParams Q;
+    TcMaps maps;
+};
+
+int batch_alloc(mt_batch* bt, BatchRun& R, int nt, cudaStream_t s)
+{
+    mt_handle* h = bt->h;
+    const int n = h->n;
+    const int Bp = bt->IB * kInstBlock;
+    const size_t n3 = 3 * (size_t)n;
+    BatchBufs& F = R.F;
+    memset(&F, 0, sizeof(F));
+    CUDA_TRY(R.A.get(&F.pool, 4 * (size_t)Bp * n3));
+    CUDA_TRY(R.A.get(&F.deriv, 3 * (size_t)Bp * n3));
+    CUDA_TRY(R.A.get(&F.stg, 12 * (size_t)Bp * n3));
+    CUDA_TRY(R.A.get(&F.p, 6 * (size_t)Bp * n3));
+    CUDA_TRY(R.A.get(&F.errest, (size_t)Bp * n3));
+    CUDA_TRY(R.A.get(&F.weights, (size_t)Bp * n3));
+    CUDA_TRY(R.A.get(&F.ylast, (size_t)Bp * n3));
+    CUDA_TRY(R.A.get(&F.ystep, (size_t)Bp * n3));
+    CUDA_TRY(cudaMemsetAsync(F.pool, 0, sizeof(double) * 4 * (size_t)Bp * n3, s));
+    if (nt > 0) {
+        CUDA_TRY(R.A.get(&F.t_out, (size_t)Bp * nt));
+        CUDA_TRY(R.A.get(&F.flags_out, (size_t)Bp * nt));
+        CUDA_TRY(cudaMemsetAsync(F.t_out, 0, sizeof(double) * Bp * nt, s));
+        CUDA_TRY(cudaMemsetAsync(F.flags_out, 0, sizeof(int) * Bp * nt, s));
+    }
+    if (bt->prec == MT_PREC_FP32) {
+        CUDA_TRY(R.A.get(&F.m32, (size_t)Bp * 3 * h->ldk));
+        CUDA_TRY(cudaMemsetAsync(F.m32, 0, sizeof(float) * Bp * 3 * (size_t)h->ldk, s));
+    } else {
+        CUDA_TRY(R.A.get(&F.mhi, (size_t)Bp * bt->Kd));
+        CUDA_TRY(R.A.get(&F.mlo, (size_t)Bp * bt->Kd));
+        CUDA_TRY(cudaMemsetAsync(F.mhi, 0, 2 * (size_t)Bp * bt->Kd, s));
+        CUDA_TRY(cudaMemsetAsync(F.mlo, 0, 2 * (size_t)Bp * bt->Kd, s));
+    }
+    CUDA_TRY(R.A.get(&F.hpart, (size_t)bt->S * Bp * 3 * bt->np));
+    CUDA_TRY(R.A.get(&F.partials, (size_t)Bp * kRedSlots * bt->CB));
+    CUDA_TRY(R.A.get(&F.inst, (size_t)bt->CB * Bp));
+    CUDA_TRY(R.A.get(&F.gs, 1));
+    CUDA_TRY(R.A.get(&F.counters, 6));
+    CUDA_TRY(cudaMemsetAsync(F.counters, 0, sizeof(unsigned) * 6, s));
+    F.hext = bt->hext;
+    F.alpha0 = bt->alpha0;
+    BatchParams& Q = R.Q;
+    memset(&Q, 0, sizeof(Q));
+    Q.Bp = Bp; Q.B = bt->B; Q.CB = bt->CB; Q.IB = bt->IB; Q.S = bt->S; Q.np = bt->np; Q.Kd = bt->Kd;
+    Q.nt = nt; Q.nt_hext = bt->nt_hext; Q.prec = bt->prec;
+    Q.khi = bt->khi; Q.klo = bt->klo;
+    Q.renorm = h->renorm;
+    memset(&R.maps, 0, sizeof(R.maps));
+    if (bt->prec != MT_PREC_FP32) {
+        int rc;
+        if ((rc = make_tmap(&R.maps.ahi, bt->khi, bt->Kd, bt->Kd, 128))) return rc;
+        if ((rc = make_tmap(&R.maps.alo, bt->klo, bt->Kd, bt->Kd, 128))) return rc;
+        if ((rc = make_tmap(&R.maps.bhi, F.mhi, bt->Kd, Bp, 64))) return rc;
+        if ((rc = make_tmap(&R.maps.blo, F.mlo, bt->Kd, Bp, 64))) return rc;
+    }
+    return MT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mt_batch_demag_field(mt_batch* bt, const double* m_dev, double* H_dev, void* stream)
+{
+    if (!bt || !m_dev || !H_dev) return fail(MT_ERR_ARG, "bad argument");
+    int rc = check_ready(bt->h, true, false);
+    if (rc) return rc;
+    if (bt->prec != MT_PREC_FP32 && !bt->khi) return fail(MT_ERR_STATE, "call mt_batch_assemble_demag first");
+    cudaStream_t s = (cudaStream_t)stream;
+    BatchRun R;
+    if ((rc = batch_alloc(bt, R, 0, s))) return rc;
+    R.Q.demag_only = 1;
+    R.Q.out_h = H_dev;
+    CUDA_TRY(launch_batch_operand(m_dev, bt->B, bt->h->n, bt->h->ldk, bt->np, bt->prec, R.F.m32, R.F.mhi, R.F.mlo, s));
+    CUDA_TRY(cudaMemsetAsync(R.F.gs, 0, sizeof(GridSync), s));
+    DevProb P = batch_prob(bt);
+    CUDA_TRY(launch_batch(P, R.F, R.Q, bt->grid, bt->prec != MT_PREC_FP32 ? &R.maps : nullptr, s));
+    GridSync gs_h;
+    CUDA_TRY(cudaMemcpyAsync(&gs_h, R.F.gs, sizeof(gs_h), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (gs_h.err || gs_h.abort) return fail(MT_ERR_TIMEOUT, "batch demag: bounded wait gave up (at %d)", gs_h.err_where);
+    return MT_OK;
+}
+
+int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_dev, double tol, double thres,
+                       const double* t_conv, int nt_conv, double conv_tol, double* t_out, double* y_out_dev,
+                       int* flags, mt_stats* stats, void* stream)
+{
+    if (!bt) return fail(MT_ERR_ARG, "null handle");
+    int rc = check_ready(bt->h, true, false);
+    if (rc) return rc;
+    if (!bt->have_dynamics) return fail(MT_ERR_STATE, "call mt_batch_set_dynamics first");
+    if (bt->prec != MT_PREC_FP32 && !bt->khi) return fail(MT_ERR_STATE, "call mt_batch_assemble_demag first");
+    if (!t || nt < 2 || !m0_dev || !t_out || !flags || !stats) return fail(MT_ERR_ARG, "bad argument (nt >= 2 required)");
+    if (nt_conv < 0 || (nt_conv > 0 && !t_conv)) return fail(MT_ERR_ARG, "bad convergence-time list");
+    cudaStream_t s = (cudaStream_t)stream;
+    mt_handle* h = bt->h;
+    const int n = h->n, B = bt->B;
+    const size_t n3 = 3 * (size_t)n;
+    for (int b = 0; b < B; ++b) { memset(&stats[b], 0, sizeof(mt_stats)); stats[b].converged_at = -1; }
+    const double eps = 2.220446049250313e-16;
+    const double round_off = 10.0 * eps, sqrrmc = sqrt(eps), cubrmc = pow(eps, 1.0 / 3.0);
+    const double sqtiny = sqrt(2.2250738585072014e-308);
+    const double toosml = round_off / (1.0 / 18.0);
+    const double t_start = t[0], t_end = t[nt - 1];
+    if (t_start == t_end) return fail(MT_ERR_ARG, "T_START = T_END");
+    if (tol > 0.01 || tol < round_off) return fail(MT_ERR_ARG, "tol %g outside (%g, 0.01)", tol, round_off);
+    if (thres < sqtiny) return fail(MT_ERR_ARG, "threshold %g below %g", thres, sqtiny);
+    const double hmin0 = std::max(sqtiny, toosml * std::max(fabs(t_start), fabs(t_end)));
+    if (fabs(t_end - t_start) < hmin0) return fail(MT_ERR_ARG, "T_END and T_START not distinguishable");
+    std::vector<double> comb;
+    for (int i = 0; i < nt + nt_conv; ++i) {
+        const double v = (i < nt) ? t[i] : t_conv[i - nt];
+        bool dup = (i > 0 && v == 0.0);
+        for (double c : comb) if (c == v) { dup = true; break; }
+        if (i == 0 || !dup) comb.push_back(v);
+    }
+    std::sort(comb.begin(), comb.end());
+    std::vector<int> cflags(comb.size(), 0);
+    for (size_t k = 0; k < comb.size(); ++k) {
+        for (int q = 0; q < nt; ++q) if (t[q] == comb[k]) { cflags[k] |= 1; break; }
+        for (int q = 0; q < nt_conv; ++q) if (t_conv[q] == comb[k]) { cflags[k] |= 2; break; }
+    }
+    BatchRun R;
+    if ((rc = batch_alloc(bt, R, nt, s))) return rc;
+    BatchBufs& F = R.F;
+    BatchParams& Q = R.Q;
+    const int Bp = Q.Bp;
+    double* d_comb = nullptr; int* d_cflags = nullptr;
+    CUDA_TRY(R.A.get(&d_comb, comb.size()));
+    CUDA_TRY(R.A.get(&d_cflags, comb.size()));
+    CUDA_TRY(cudaMemcpyAsync(d_comb, comb.data(), sizeof(double) * comb.size(), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(d_cflags, cflags.data(), sizeof(int) * comb.size(), cudaMemcpyHostToDevice, s));
+    F.y_out = y_out_dev;
+    // y <- m0 (pool slot 0 of every instance), first sample, convergence reference
+    CUDA_TRY(cudaMemcpyAsync(F.pool, m0_dev, sizeof(double) * (size_t)B * n3, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(F.ylast, m0_dev, sizeof(double) * (size_t)B * n3, cudaMemcpyDeviceToDevice, s));
+    if (y_out_dev)
+        for (int b = 0; b < B; ++b)
+            CUDA_TRY(cudaMemcpyAsync(y_out_dev + (size_t)b * nt * n3, m0_dev + (size_t)b * n3, sizeof(double) * n3,
+                                     cudaMemcpyDeviceToDevice, s));
+    std::vector<BInst> init((size_t)bt->CB * Bp);
+    for (int cb = 0; cb < bt->CB; ++cb)
+        for (int b = 0; b < Bp; ++b) {
+            BInst& I = init[(size_t)cb * Bp + b];
+            memset(&I, 0, sizeof(I));
+            RKS& st = I.s;
+            st.t = t_start; st.t_old = t_start; st.t_start = t_start; st.t_end = t_end;
+            st.dir = (t_end - t_start) >= 0 ? 1.0 : -1.0;
+            st.tol = tol;
+            st.h = std::max(fabs(t_end - t_start) / 8.0, hmin0);
+            st.at_t_start = 1; st.phase2 = 1;
+            st.iy = 0; st.iyold = 1; st.ia0 = 2; st.ia1 = 3;
+            st.dyp = 0; st.dypold = 1; st.d8 = 2;
+            st.ci = 1; st.ko = 1;
+            st.converged_at = -1;
+            I.pc = 0;
+            I.req = (b < B) ? 0 : 3;
+        }
+    CUDA_TRY(cudaMemcpyAsync(F.inst, init.data(), sizeof(BInst) * init.size(), cudaMemcpyHostToDevice, s));
+    Q.thres = thres; Q.round_off = round_off; Q.sqrrmc = sqrrmc; Q.cubrmc = cubrmc; Q.sqtiny = sqtiny;
+    Q.toosml = toosml; Q.conv_tol = conv_tol;
+    Q.comb_t = d_comb; Q.comb_flags = d_cflags; Q.ncomb = (int)comb.size();
+    Q.ticks_per_launch = 4000;
+    Q.evals_budget = 1LL << 60;
+    DevProb P = batch_prob(bt);
+    const size_t smem = batch_smem_bytes(n, h->ldk, bt->prec);
+    if (smem > 227 * 1024) return fail(MT_ERR_UNSUPPORTED, "batch shared memory %zu exceeds 227 KB", smem);
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    CUDA_TRY(cudaEventCreate(&ev0));
+    CUDA_TRY(cudaEventCreate(&ev1));
+    struct EvGuard { cudaEvent_t a, b; ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); } } evg{ev0, ev1};
+    double kernel_ms = 0.0;
+    long long launches = 0;
+    std::vector<BInst> hs(Bp);
+    long long last_sig = -1;
+    for (;;) {
+        CUDA_TRY(cudaMemsetAsync(F.gs, 0, sizeof(GridSync), s));
+        CUDA_TRY(cudaMemsetAsync(F.counters, 0, sizeof(unsigned) * 6, s));
+        CUDA_TRY(cudaEventRecord(ev0, s));
+        CUDA_TRY(launch_batch(P, F, Q, bt->grid, bt->prec != MT_PREC_FP32 ? &R.maps : nullptr, s));
+        CUDA_TRY(cudaEventRecord(ev1, s));
+        GridSync gs_h;
+        CUDA_TRY(cudaMemcpyAsync(&gs_h, F.gs, sizeof(gs_h), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaMemcpyAsync(hs.data(), F.inst, sizeof(BInst) * Bp, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        float ms = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, ev0, ev1));
+        kernel_ms += ms;
+        launches++;
+        if (gs_h.err != 0 || gs_h.abort)
+            return fail(MT_ERR_TIMEOUT, "batch integrator: bounded wait gave up (code %d at %d)", gs_h.err, gs_h.err_where);
+        bool all_done = true;
+        long long sig = 0;
+        for (int b = 0; b < B; ++b) {
+            if (hs[b].req != 3) all_done = false;
+            sig += hs[b].s.full_f_count + hs[b].s.f_count + hs[b].s.ci;
+        }
+        if (all_done) break;
+        if (sig == last_sig) return fail(MT_ERR_SOLVER, "batch integrator made no progress");
+        last_sig = sig;
+    }
+    std::vector<int> fl((size_t)Bp * nt);
+    std::vector<double> to((size_t)Bp * nt);
+    CUDA_TRY(cudaMemcpy(to.data(), F.t_out, sizeof(double) * to.size(), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(fl.data(), F.flags_out, sizeof(int) * fl.size(), cudaMemcpyDeviceToHost));
+    int worst = 0;
+    for (int b = 0; b < B; ++b) {
+        memcpy(t_out + (size_t)b * nt, to.data() + (size_t)b * nt, sizeof(double) * nt);
+        memcpy(flags + (size_t)b * nt, fl.data() + (size_t)b * nt, sizeof(int) * nt);
+        t_out[(size_t)b * nt] = t[0];
+        flags[(size_t)b * nt] = 0;
+        const RKS& st = hs[b].s;
+        stats[b].f_evals = st.full_f_count + st.f_count;
+        stats[b].steps = st.step_count;
+        stats[b].bad_steps = st.bad_step_count;
+        stats[b].n_flag3 = st.n_flag3;
+        stats[b].n_flag4 = st.n_flag4;
+        stats[b].n_out = st.ko;
+        stats[b].status = st.status;
+        stats[b].converged_at = st.converged_at;
+        if (st.status) worst = st.status;
+    }
+    stats[0].launches = launches;
+    stats[0].kernel_ms = kernel_ms;
+    if (worst) return fail(MT_ERR_SOLVER, "an instance stopped with RKSUITE flag %d", worst);
     return MT_OK;
 }
 

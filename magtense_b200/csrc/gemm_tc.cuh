@@ -1,0 +1,278 @@
+// tcgen05 (5th-generation tensor core) demag GEMM tile for the batched
+// integrator: H[a][cell][inst] = sum_k Khi/lo[(a, cell), k] * Mhi/lo[inst, k]
+// for the three field components a of 128 receiver cells and 64 instances,
+// over one split of the 3n-long source dimension.
+//
+// Split-BF16: K32 = Khi + Klo and m32 = Mhi + Mlo (each part BF16, the low
+// part the BF16 rounding of the remainder), products accumulated in FP32 in
+// TMEM:  bf16x3 = Khi*Mhi + Khi*Mlo + Klo*Mhi ;  bf16x2 = Khi*Mhi + Klo*Mhi.
+//
+// Per k-block of 32 sources a stage holds A_hi[3], A_lo[3] (3 x 128 x 32 BF16
+// each), B_hi, B_lo (64 x 32 BF16), loaded by TMA (SWIZZLE_64B, no multicast)
+// into a 3-stage shared-memory ring.  Warp 4 (one lane) issues the TMA loads,
+// warp 5 (one lane) issues tcgen05.mma (M=128, N=64, K=16) into three TMEM
+// accumulators (columns 0/64/128) and commits each stage back to its empty
+// barrier; warps 0-3 read the accumulators with tcgen05.ld and store them.
+// Every mbarrier wait is bounded; on a timeout the kernel's abort flag is set.
+#pragma once
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include "common.cuh"
+
+struct TcMaps {
+    CUtensorMap ahi, alo, bhi, blo;
+};
+
+struct TcState {
+    long long kb_done;   // k-blocks consumed so far in this launch (ring position)
+    long long tiles;     // tiles finished so far (accumulator barrier phase)
+    uint32_t tmem;       // TMEM base address of the accumulators
+};
+
+constexpr int kTcStages = 3;
+constexpr int kTcKB = 32;                                    // k elements per stage (64 B rows)
+constexpr int kTcABytes = 128 * kTcKB * 2;                   // one A tile
+constexpr int kTcBBytes = 64 * kTcKB * 2;                    // one B tile
+constexpr int kTcStageBytes = 6 * kTcABytes + 2 * kTcBBytes; // 56 KB
+constexpr int kTcTmemCols = 256;
+
+static inline size_t tc_smem_bytes() { return 1024 + (size_t)kTcStages * kTcStageBytes + 256; }
+
+MT_DEV uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+MT_DEV void mbar_init(uint32_t bar, int count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+MT_DEV void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// bounded wait on the given phase parity; false after the limit
+MT_DEV bool mbar_wait(uint32_t bar, uint32_t parity, GridSync* gs, int where)
+{
+    uint32_t done = 0;
+    const uint64_t t0 = globaltimer_ns();
+    for (long long it = 0; it < 4000000LL; ++it) {
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                     : "=r"(done)
+                     : "r"(bar), "r"(parity)
+                     : "memory");
+        if (done) return true;
+        if ((it & 255) == 255) {
+            if (ld_volatile_i32(&gs->abort)) return false;
+            if (globaltimer_ns() - t0 > 2000000000ULL) break;
+        }
+    }
+    if (atomicCAS(&gs->err, 0, KERR_BARRIER_TIMEOUT) == 0) gs->err_where = where;
+    atomicExch(&gs->abort, 1);
+    return false;
+}
+
+MT_DEV void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(map), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+// shared-memory matrix descriptor: K-major tile of 64-byte rows with the
+// 64-byte swizzle, 8-row groups 512 bytes apart (SBO), version 1 (tcgen05)
+MT_DEV uint64_t sdesc_sw64(uint32_t saddr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;                  // LBO (unused for swizzled K-major)
+    d |= (uint64_t)(512 >> 4) << 32;          // SBO
+    d |= (uint64_t)1 << 46;                   // descriptor version
+    d |= (uint64_t)4 << 61;                   // SWIZZLE_64B
+    return d;
+}
+
+// instruction descriptor: D F32, A/B BF16, both K-major, M = 128, N = 64
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+
+MT_DEV void umma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
+{
+    asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                 " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
+                 "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+                 : "memory");
+}
+
+MT_DEV void umma_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+MT_DEV void tmem_ld32(uint32_t taddr, float (&v)[32])
+{
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+          "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int k = 0; k < 32; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+// shared-memory layout of the GEMM area (1024-aligned base)
+struct TcSmem {
+    uint8_t* stages;     // kTcStages x kTcStageBytes
+    uint64_t* full;      // kTcStages
+    uint64_t* empty;     // kTcStages
+    uint64_t* accum;     // 1
+    uint32_t* tmem_slot; // 1
+};
+
+MT_DEV TcSmem tc_layout(unsigned char* smem)
+{
+    TcSmem L;
+    const uint32_t base = smem_u32(smem);
+    const uint32_t pad = (1024u - (base & 1023u)) & 1023u;
+    L.stages = smem + pad;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(L.stages + (size_t)kTcStages * kTcStageBytes);
+    L.full = bars;
+    L.empty = bars + kTcStages;
+    L.accum = bars + 2 * kTcStages;
+    L.tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kTcStages + 1);
+    return L;
+}
+
+MT_DEV void tc_init_impl(unsigned char* smem, TcState& st)
+{
+    TcSmem L = tc_layout(smem);
+    const int warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < kTcStages; ++k) {
+            mbar_init(smem_u32(&L.full[k]), 1);
+            mbar_init(smem_u32(&L.empty[k]), 1);
+        }
+        mbar_init(smem_u32(L.accum), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(L.tmem_slot)),
+                     "r"(kTcTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    st.tmem = *reinterpret_cast<volatile uint32_t*>(L.tmem_slot);
+    st.kb_done = 0;
+    st.tiles = 0;
+}
+
+MT_DEV void tc_finish_impl(unsigned char* smem, TcState& st)
+{
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if ((threadIdx.x >> 5) == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(st.tmem), "r"(kTcTmemCols) : "memory");
+    (void)smem;
+}
+
+// One GEMM tile (cb, ib, s) of the current tick.  Q/F are BatchParams/BatchBufs.
+// Returns a CTA-uniform ok flag.
+template <typename QT, typename FT>
+MT_DEV bool tc_gemm_tile_impl(unsigned char* smem, const QT& Q, const FT& F, const TcMaps& maps, int cb, int ib, int s,
+                              bool three, TcState& st)
+{
+    TcSmem L = tc_layout(smem);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int kseg = Q.Kd / Q.S;
+    const int k0 = s * kseg;
+    const int nkb = kseg / kTcKB;
+    const uint32_t tx = three ? (uint32_t)kTcStageBytes : (uint32_t)(6 * kTcABytes + kTcBBytes);
+    bool ok = true;
+    if (warp == 4 && lane == 0) {
+        for (int kb = 0; kb < nkb; ++kb) {
+            const long long g = st.kb_done + kb;
+            const int stg = (int)(g % kTcStages);
+            const uint32_t ph = (uint32_t)((g / kTcStages) & 1);
+            if (!mbar_wait(smem_u32(&L.empty[stg]), ph ^ 1u, F.gs, 200)) { ok = false; break; }
+            uint8_t* base = L.stages + (size_t)stg * kTcStageBytes;
+            const uint32_t fb = smem_u32(&L.full[stg]);
+            mbar_expect_tx(fb, tx);
+            const int x = k0 + kb * kTcKB;
+            for (int a = 0; a < 3; ++a) {
+                const int y = a * Q.np + cb * 128;
+                tma_load_2d(smem_u32(base + a * kTcABytes), &maps.ahi, x, y, fb);
+                tma_load_2d(smem_u32(base + (3 + a) * kTcABytes), &maps.alo, x, y, fb);
+            }
+            tma_load_2d(smem_u32(base + 6 * kTcABytes), &maps.bhi, x, ib * 64, fb);
+            if (three) tma_load_2d(smem_u32(base + 6 * kTcABytes + kTcBBytes), &maps.blo, x, ib * 64, fb);
+        }
+        if (!ok) {   // let loads already in flight land before the CTA moves on
+            const long long issued = st.kb_done + nkb;
+            for (long long g = issued - kTcStages; g < issued; ++g) {
+                if (g < 0) continue;
+                mbar_wait(smem_u32(&L.full[g % kTcStages]), (uint32_t)((g / kTcStages) & 1), F.gs, 203);
+            }
+        }
+    } else if (warp == 5 && lane == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        for (int kb = 0; kb < nkb; ++kb) {
+            const long long g = st.kb_done + kb;
+            const int stg = (int)(g % kTcStages);
+            const uint32_t ph = (uint32_t)((g / kTcStages) & 1);
+            if (!mbar_wait(smem_u32(&L.full[stg]), ph, F.gs, 201)) { ok = false; break; }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t base = smem_u32(L.stages + (size_t)stg * kTcStageBytes);
+#pragma unroll
+            for (int kk = 0; kk < kTcKB / 16; ++kk) {
+                const uint32_t koff = kk * 32;
+                const uint64_t bh = sdesc_sw64(base + 6 * kTcABytes + koff);
+                const uint64_t bl = sdesc_sw64(base + 6 * kTcABytes + kTcBBytes + koff);
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    const uint32_t d = st.tmem + a * 64;
+                    const uint64_t ah = sdesc_sw64(base + a * kTcABytes + koff);
+                    const uint64_t al = sdesc_sw64(base + (3 + a) * kTcABytes + koff);
+                    umma(d, ah, bh, (kb > 0 || kk > 0) ? 1u : 0u);
+                    if (three) umma(d, ah, bl, 1u);
+                    umma(d, al, bh, 1u);
+                }
+            }
+            umma_commit(smem_u32(&L.empty[stg]));
+        }
+        if (ok) umma_commit(smem_u32(L.accum));
+    }
+    if (warp < 4) {
+        const uint32_t ph = (uint32_t)(st.tiles & 1);
+        bool w = mbar_wait(smem_u32(L.accum), ph, F.gs, 202);
+        w = __all_sync(0xffffffffu, w);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (w) {
+            const int cell = cb * 128 + warp * 32 + lane;
+#pragma unroll 1
+            for (int a = 0; a < 3; ++a) {
+#pragma unroll 1
+                for (int half = 0; half < 2; ++half) {
+                    float v[32];
+                    tmem_ld32(st.tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(a * 64 + half * 32), v);
+#pragma unroll
+                    for (int k = 0; k < 32; ++k) {
+                        const int inst = ib * 64 + half * 32 + k;
+                        F.hpart[(((size_t)s * Q.Bp + inst) * 3 + a) * Q.np + cell] = v[k];
+                    }
+                }
+            }
+        } else {
+            ok = false;
+        }
+    }
+    st.kb_done += nkb;
+    st.tiles++;
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    return __syncthreads_and(ok ? 1 : 0) != 0;
+}

@@ -172,3 +172,93 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+
+PRECISIONS = {"fp32": 0, "bf16x3": 1, "bf16x2": 2}
+
+
+class BatchSolver:
+    """B instances sharing one uniform grid, material and demag tensor.
+
+    Each instance has its own applied-field table, damping and initial state,
+    and its own RKSUITE 'M' step control; all demag products of one
+    right-hand-side evaluation form one GEMM (``precision``: "fp32" SIMT,
+    "bf16x3" / "bf16x2" split-BF16 on the tcgen05 tensor cores).
+    """
+
+    def __init__(self, res, grid_L, B, *, precision="bf16x3", A0=1.3e-11, Ms=8e5, K0=0.0, u_ea=None, device=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("magtense_b200 needs a CUDA device (no CPU path exists)")
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        nx, ny, nz = (int(v) for v in res)
+        self.res = (nx, ny, nz)
+        self.grid_L = tuple(float(v) for v in grid_L)
+        self.n = nx * ny * nz
+        self.B = int(B)
+        self.precision = precision
+        g = _lib.Grid(nx, ny, nz, *self.grid_L)
+        h = C.c_void_p()
+        with torch.cuda.device(self.device):
+            check(_lib.lib().mt_batch_create(C.byref(g), self.B, PRECISIONS[precision], C.byref(h)), "mt_batch_create")
+        self._h = h
+        n = self.n
+        Ms_ = _np_d(np.broadcast_to(np.asarray(Ms, dtype=np.float64), (n,)))
+        K0_ = _np_d(np.broadcast_to(np.asarray(K0, dtype=np.float64), (n,)))
+        u = np.zeros((n, 3)) if u_ea is None else _np_d(np.asarray(u_ea, dtype=np.float64).reshape(n, 3))
+        check(_lib.lib().mt_batch_set_material(self._h, float(A0), Ms_.ctypes.data_as(_lib.D),
+                                               K0_.ctypes.data_as(_lib.D), u.ctypes.data_as(_lib.D)),
+              "mt_batch_set_material")
+
+    def assemble(self, stream=None):
+        with torch.cuda.device(self.device):
+            check(_lib.lib().mt_batch_assemble_demag(self._h, _stream(stream)), "mt_batch_assemble_demag")
+
+    def set_dynamics(self, *, hext, alpha, solver=2, gamma=0.0, renormalize=False):
+        """hext: (B, nt_hext, 4) rows {t, Hx, Hy, Hz} per instance; alpha: scalar or (B,)."""
+        he = _np_d(hext).reshape(self.B, -1, 4)
+        al = _np_d(np.broadcast_to(np.asarray(alpha, dtype=np.float64), (self.B,)))
+        self._tables = (he, al)
+        check(_lib.lib().mt_batch_set_dynamics(self._h, int(solver), float(gamma), al.ctypes.data_as(_lib.D),
+                                               he.ctypes.data_as(_lib.D), he.shape[1], int(bool(renormalize))),
+              "mt_batch_set_dynamics")
+
+    def demag_field(self, m, stream=None):
+        m = torch.as_tensor(m, dtype=torch.float64, device=self.device).reshape(self.B, 3 * self.n).contiguous()
+        out = torch.empty_like(m)
+        with torch.cuda.device(self.device):
+            check(_lib.lib().mt_batch_demag_field(self._h, _dptr(m), _dptr(out), _stream(stream)),
+                  "mt_batch_demag_field")
+        return out.view(self.B, 3, self.n)
+
+    def integrate(self, t, m0, *, tol=1e-4, thres=1e-6, t_conv=None, conv_tol=1e-4, keep_trajectory=True,
+                  stream=None):
+        """Returns (t_out (B, nt), y_out (B, nt, 3n) cuda FP64 or None, flags (B, nt), stats list)."""
+        t = _np_d(t).reshape(-1)
+        nt = t.shape[0]
+        m0 = torch.as_tensor(m0, dtype=torch.float64, device=self.device).reshape(self.B, 3 * self.n).contiguous()
+        tc = np.zeros(1) if t_conv is None else _np_d(t_conv).reshape(-1)
+        y_out = torch.zeros((self.B, nt, 3 * self.n), dtype=torch.float64, device=self.device) \
+            if keep_trajectory else None
+        t_out = np.zeros((self.B, nt))
+        flags = np.zeros((self.B, nt), dtype=np.int32)
+        st = (_lib.Stats * self.B)()
+        with torch.cuda.device(self.device):
+            rc = _lib.lib().mt_batch_integrate(self._h, t.ctypes.data_as(_lib.D), nt, _dptr(m0), float(tol),
+                                               float(thres), tc.ctypes.data_as(_lib.D), tc.shape[0], float(conv_tol),
+                                               t_out.ctypes.data_as(_lib.D),
+                                               C.c_void_p(0) if y_out is None else _dptr(y_out),
+                                               flags.ctypes.data_as(_lib.I), st, _stream(stream))
+        check(rc, "mt_batch_integrate")
+        return t_out, y_out, flags, [x.as_dict() for x in st]
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _lib.lib().mt_batch_destroy(h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
