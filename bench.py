@@ -1,19 +1,27 @@
 """Benchmark: simulated ns/s of the MagTense micromagnetic hot path on B200.
 
-Workload ("film"): the 80x20x1 std-problem-4 thin film (500x125x3 nm, Ms 8e5,
-A 1.3e-11, K 0), instances that share the geometry, each driven by a seeded
-in-plane field (angle U[0,360) deg, magnitude U[0,50] mT), integrated for
-``--window`` ns at alpha = gamma*0.02 from an s-state (tol 1e-6, output every
-1 ps).  One step = every instance of this rank integrated over the window.
-Synthetic, seeded data stand in for the std-problem-4 dataset workflow.
+Headline workload ("film-batch", the batching configuration): B = 256
+instances of the 80x20x1 std-problem-4 thin film (500x125x3 nm, n = 1600,
+Ms 8e5 A/m, A 1.3e-11 J/m, K 0) sharing one demag tensor, each driven by a
+seeded in-plane field (angle U[0,360) deg, magnitude U[0,50] mT), integrated
+for 1 ns at alpha = gamma*0.02 (gamma = 2.211e5) from an s-state with per-
+instance RKSUITE 'M' step control, tol 1e-6, output every 1 ps.  The demag
+products run as one split-BF16 (bf16x3) tcgen05 GEMM per right-hand-side
+evaluation inside one persistent kernel.  Seeded synthetic inputs stand in
+for the std-problem-4 dataset workflow.  One step = every instance of the
+rank integrated over the window.
+
+Other workloads: "film-plain" (the same film, single-instance FP32 path) and
+"large-plain" (64x64x8 cubes of 5 nm, n = 32768, 25.8 GB FP32 tensor, the
+HBM-bound demag matvec).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload film-plain] [--instances B]
+                  [--workload film-batch|film-plain|large-plain]
 
 Multi-GPU: one process per GPU (torchrun); instances are sharded across ranks
-with no data-path collective ("scaling": "weak"); the step time is the max
-over ranks.  --impl reference times the CPU restatement of the reference
-(oracle/, OpenMP on all host cores) on the same workload, rank 0 only.
+with no data-path collective ("scaling": "weak"); the step time is the max over
+ranks.  --impl reference times the CPU restatement of the reference (oracle/,
+OpenMP on all host cores) on the same workload, rank 0 only.
 """
 from __future__ import annotations
 
@@ -34,8 +42,10 @@ sys.path.insert(0, str(ROOT))
 
 MU0 = 4 * np.pi * 1e-7
 GAMMA = 2.211e5
-RES = (80, 20, 1)
-GRID_L = (500e-9, 125e-9, 3e-9)
+FILM_RES = (80, 20, 1)
+FILM_L = (500e-9, 125e-9, 3e-9)
+LARGE_RES = (64, 64, 8)
+LARGE_L = (320e-9, 320e-9, 40e-9)
 
 
 def parse():
@@ -44,11 +54,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="film-plain", choices=["film-plain"])
-    ap.add_argument("--instances", type=int, default=1, help="instances per rank")
-    ap.add_argument("--window", type=float, default=0.05, help="simulated ns per instance per step")
+    ap.add_argument("--workload", default="film-batch", choices=["film-batch", "film-plain", "large-plain"])
+    ap.add_argument("--instances", type=int, default=256, help="instances per rank (film-batch)")
+    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "bf16x2", "fp32"])
+    ap.add_argument("--window", type=float, default=None, help="simulated ns per instance per step")
     ap.add_argument("--cpu-window", type=float, default=0.3, help="simulated ns of the bounded CPU sample")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
 
 
@@ -56,8 +68,9 @@ def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
-    return 6650.0, 1590.0, "fallback"
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), float(d.get("bf16_tflops_sustained", d["bf16_tflops"])), \
+            "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
 
 
 def instance_fields(seed, count):
@@ -67,9 +80,8 @@ def instance_fields(seed, count):
     return np.stack([mag * np.cos(ang), mag * np.sin(ang), np.zeros(count)], 1)
 
 
-def s_state(n, seed=0):
-    """Seeded start state: (1,1,1)/sqrt3 + N(0, 0.01^2), renormalised (the relaxed
-    state is produced on the GPU before timing)."""
+def start_state(n, seed=0):
+    """Seeded start: (1,1,1)/sqrt3 + N(0, 0.01^2) per component, renormalised."""
     rng = np.random.default_rng(seed)
     m = np.ones((3, n)) / np.sqrt(3) + 0.01 * rng.standard_normal((3, n))
     return (m / np.linalg.norm(m, axis=0)).reshape(-1)
@@ -120,29 +132,27 @@ class Clocks:
 
 
 def dist_setup():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    return int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
 
 
 # --------------------------------------------------------------------------------------------
-def cpu_reference_sample(window_ns, n_inst_seed=0):
-    """Oracle (CPU restatement, OpenMP over all host cores) on a bounded window of the film workload."""
+def cpu_reference_sample(window_ns, workload="film"):
+    """Oracle (CPU restatement, OpenMP over all host cores) on a bounded window of one instance."""
     from oracle import oracle as O
-    n = int(np.prod(RES))
-    h = instance_fields(n_inst_seed, 1)[0]
+    res, L = (FILM_RES, FILM_L) if workload.startswith("film") else (LARGE_RES, LARGE_L)
+    n = int(np.prod(res))
+    h = instance_fields(0, 1)[0]
     win = window_ns * 1e-9
     hext = np.array([[0.0, *h], [win, *h]])
-    P = O.Problem(RES, GRID_L, mode=0, gamma=GAMMA, alpha=GAMMA * 0.02, hext=hext)
-    m0 = s_state(n)
+    P = O.Problem(res, L, mode=0, gamma=GAMMA, alpha=GAMMA * 0.02, hext=hext)
+    m0 = start_state(n)
     nt = max(2, int(round(window_ns / 1e-3)) + 1)
     t0 = time.perf_counter()
     _, _, _, st = P.solve(np.linspace(0, win, nt), m0, tol=1e-6)
     dt = time.perf_counter() - t0
     return {"value": window_ns / dt, "unit": "simulated ns/s", "cores": O.threads(), "kind": "port",
-            "sample": f"{window_ns} ns of the 80x20x1 film dynamics (1 instance, {st['f_evals']} RHS evals, "
-                      f"{dt:.1f} s, oracle FP32-demag mode)"}
+            "sample": f"{window_ns} ns of one 80x20x1 film instance ({st['f_evals']} RHS evals, {dt:.1f} s, "
+                      f"FP32-demag restatement of the reference on the host cores)"}
 
 
 def run_reference(args):
@@ -151,7 +161,7 @@ def run_reference(args):
         return
     vals = []
     for _ in range(args.warmup):
-        cpu_reference_sample(args.cpu_window / 4)
+        cpu_reference_sample(args.cpu_window / 10)
     for _ in range(args.steps):
         vals.append(cpu_reference_sample(args.cpu_window))
     v = statistics.median([x["value"] for x in vals])
@@ -160,15 +170,53 @@ def run_reference(args):
     line = {"metric": "simulated ns/s", "value": v, "unit": "simulated ns/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "film-plain (80x20x1 std-problem-4 film, seeded in-plane fields)",
-                       "window_ns": args.cpu_window, "note": "CPU restatement of the reference (Fortran not "
-                       "buildable here: no Fortran compiler/MKL)"},
+            "config": {"workload": f"{args.workload} (80x20x1 std-problem-4 film instances, seeded in-plane "
+                                   "fields, 1 ns each at alpha_G = 0.02, tol 1e-6)",
+                       "window_ns": args.cpu_window,
+                       "note": "CPU restatement of the reference (the Fortran reference cannot be built here: no "
+                               "Fortran compiler, no MKL); instances are independent, so the per-instance rate is "
+                               "the batch rate on one CPU"},
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "simulated ns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 # --------------------------------------------------------------------------------------------
+def relaxed_state(torch, res, L, relax_ns=0.2):
+    """s-state: seeded start relaxed in zero field at alpha_G = 1 (untimed input preparation)."""
+    from magtense_b200 import Solver
+    n = int(np.prod(res))
+    s = Solver(res, L)
+    s.assemble()
+    s.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 1.0,
+                   hext=np.array([[0, 0, 0, 0], [relax_ns * 1e-9, 0, 0, 0.0]]))
+    _, yr, _, _ = s.integrate(np.linspace(0, relax_ns * 1e-9, 3), torch.as_tensor(start_state(n), device="cuda"),
+                              tol=1e-6)
+    return s, yr[-1].clone()
+
+
+def timed_steps(torch, step_fn, steps, warmup, dist, local):
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > L2
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        step_fn()
+    times, stats = [], []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        for _ in range(steps):
+            flush.fill_(1.0)
+            if dist:
+                dist.barrier()
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            st = step_fn()
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            times.append(ev0.elapsed_time(ev1))
+            stats.append(st)
+    return times, stats, clk.summary(), flush
+
+
 def run_ours(args):
     import torch
     ws, rank, local = dist_setup()
@@ -177,109 +225,191 @@ def run_ours(args):
     if ws > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    from magtense_b200 import Solver
-
-    n = int(np.prod(RES))
-    B = args.instances
-    win = args.window * 1e-9
-    fields = instance_fields(1000 + rank, B)
-    nt = max(2, int(round(args.window / 1e-3)) + 1)
-    t = np.linspace(0, win, nt)
-    s = Solver(RES, GRID_L)
-    s.assemble()
-    # s-state: short zero-field relaxation at alpha_G = 1 from the seeded start (untimed input preparation)
-    s.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 1.0, hext=np.array([[0, 0, 0, 0], [0.2e-9, 0, 0, 0.0]]))
-    _, yr, _, _ = s.integrate(np.linspace(0, 0.2e-9, 3), torch.as_tensor(s_state(n), device="cuda"), tol=1e-6)
-    m_s = yr[-1].clone()
-    m_s_host = m_s.cpu().numpy()
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > L2
-    stream = torch.cuda.current_stream()
-
-    def one_step(e2e=False):
-        stats = []
-        outs = []
-        for b in range(B):
-            hext = np.array([[0.0, *fields[b]], [win, *fields[b]]])
-            s.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.02, hext=hext)
-            if e2e:
-                m0 = torch.from_numpy(m_s_host).pin_memory().to("cuda", non_blocking=True)
-            else:
-                m0 = m_s
-            t_out, y, flags, st = s.integrate(t, m0, tol=1e-6)
-            if e2e:
-                outs.append(y.cpu())
-            stats.append(st)
-        return stats
-
-    for _ in range(args.warmup):
-        one_step()
-    times, stats_all = [], []
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(local) as clk:
-        for _ in range(args.steps):
-            flush.fill_(1.0)
-            if dist:
-                dist.barrier()
-            torch.cuda.synchronize()
-            ev0.record(stream)
-            st = one_step()
-            ev1.record(stream)
-            torch.cuda.synchronize()
-            times.append(ev0.elapsed_time(ev1))
-            stats_all.append(st)
-    # e2e: host m0 in, host trajectory out, through the public API
-    e2e_times = []
-    for _ in range(max(1, args.steps)):
-        flush.fill_(1.0)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        one_step(e2e=True)
-        torch.cuda.synchronize()
-        e2e_times.append((time.perf_counter() - t0) * 1e3)
-    step_ms = max(times)
-    e2e_ms = statistics.median(e2e_times)
-    if dist:
-        tt = torch.tensor([step_ms, e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        step_ms, e2e_ms = float(tt[0]), float(tt[1])
-    flat = [x for st in stats_all for x in st]
-    evals = sum(x["f_evals"] for x in flat)
-    kms = sum(x["kernel_ms"] for x in flat)
-    launches = sum(x["launches"] for x in flat)
-    if rank == 0:
-        hbm, bf16, src = peaks()
-        bytes_per_eval = 24.0 * n * n
-        achieved = bytes_per_eval * evals / (kms / 1e3) / 1e9
-        sim_ns = ws * B * args.window
-        value = sim_ns / (step_ms / 1e3)
-        e2e_val = sim_ns / (e2e_ms / 1e3)
-        line = {
-            "metric": "simulated ns/s", "value": value, "unit": "simulated ns/s", "n_gpus": ws,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "film-plain: 80x20x1 std-problem-4 film (n=1600), plain FP32 demag, "
-                                   "single-instance persistent integrator",
-                       "instances_per_rank": B, "window_ns": args.window, "outputs": nt, "tol": 1e-6,
-                       "parallelism": f"instances sharded over {ws} rank(s)", "l2": "flushed (256 MB write) "
-                       "before every timed step"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None,
-                         "note": f"integrate_kernel: 24*n^2 B of tensor per RHS eval x {evals} evals over "
-                                 f"{kms:.2f} ms device time; peak {src}; the 61 MB tensor is L2-resident"},
-            "e2e": {"value": e2e_val, "unit": "simulated ns/s",
-                    "h2d_bytes_per_step": B * 3 * n * 8,
-                    "d2h_bytes_per_step": B * nt * 3 * n * 8},
-            "gpu_launches": int(launches + 0),
-            "rhs_evals_per_s": evals / (sum(times) / 1e3) * ws,
-            "clocks": clk.summary(),
-        }
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    hbm, bf16, bf16_sus, src = peaks()
+    line = None
+    if args.workload == "film-batch":
+        line = bench_film_batch(torch, args, ws, rank, local, dist, hbm, bf16_sus, src)
+    else:
+        line = bench_plain(torch, args, ws, rank, local, dist, hbm, src)
+    if rank == 0 and line is not None:
         if not args.no_cpu:
-            line["cpu_baseline"] = cpu_reference_sample(args.cpu_window)
+            line["cpu_baseline"] = cpu_reference_sample(args.cpu_window, args.workload)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def max_over_ranks(torch, dist, vals):
+    if not dist:
+        return vals
+    tt = torch.tensor(vals, device="cuda", dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return [float(x) for x in tt]
+
+
+def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
+    from magtense_b200 import BatchSolver, Solver
+    res, L = FILM_RES, FILM_L
+    n = int(np.prod(res))
+    B = args.instances
+    window = 1.0 if args.window is None else args.window
+    win = window * 1e-9
+    nt = int(round(window / 1e-3)) + 1
+    t = np.linspace(0, win, nt)
+    plain, m_s = relaxed_state(torch, res, L)
+    fields = instance_fields(1000 + rank, B)
+    hext = np.zeros((B, 2, 4))
+    hext[:, 1, 0] = win
+    hext[:, :, 1:] = fields[:, None, :]
+    bs = BatchSolver(res, L, B, precision=args.precision)
+    bs.assemble()
+    bs.set_dynamics(hext=hext, alpha=GAMMA * 0.02, gamma=GAMMA)
+    m0 = m_s.unsqueeze(0).expand(B, -1).contiguous()
+    m0_host = m0.cpu().numpy()
+
+    def step():
+        _, y, _, st = bs.integrate(t, m0, tol=1e-6)
+        return st
+
+    times, stats, clocks, flush = timed_steps(torch, step, args.steps, args.warmup, dist, local)
+    # end to end through the public API: host m0 in (pinned), host trajectories out
+    e2e_ms = None
+    if not args.no_e2e:
+        pin_in = torch.from_numpy(m0_host).pin_memory()
+        pin_out = torch.empty((B, nt, 3 * n), dtype=torch.float64).pin_memory()
+        e2e = []
+        for _ in range(max(1, args.steps)):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            dev_in = pin_in.to("cuda", non_blocking=True)
+            _, y, _, _ = bs.integrate(t, dev_in, tol=1e-6)
+            pin_out.copy_(y, non_blocking=True)
+            torch.cuda.synchronize()
+            e2e.append((time.perf_counter() - t0) * 1e3)
+            del y
+        e2e_ms = statistics.median(e2e)
+    # the plain FP32 single-instance path on the same geometry and workload, for the ratio
+    plain_window = min(window, 0.05)
+    plain.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.02,
+                       hext=np.array([[0.0, *fields[0]], [plain_window * 1e-9, *fields[0]]]))
+    tp = np.linspace(0, plain_window * 1e-9, int(round(plain_window / 1e-3)) + 1)
+    plain.integrate(tp, m_s, tol=1e-6)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    _, _, _, pst = plain.integrate(tp, m_s, tol=1e-6)
+    torch.cuda.synchronize()
+    plain_rate = plain_window / (time.perf_counter() - t0)
+    step_ms = max(times)
+    step_ms, e2e_red = max_over_ranks(torch, dist, [step_ms, e2e_ms or 0.0])
+    if rank != 0:
+        return None
+    flat = [x for st in stats for x in st]
+    evals = sum(x["f_evals"] for x in flat)
+    kms = sum(st[0]["kernel_ms"] for st in stats)
+    launches = sum(st[0]["launches"] for st in stats)
+    flops = 18.0 * n * n * evals
+    achieved = flops / (kms / 1e3) / 1e12
+    sim_ns = ws * B * window
+    value = sim_ns / (step_ms / 1e3)
+    line = {
+        "metric": "simulated ns/s", "value": value, "unit": "simulated ns/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
+        "config": {"workload": f"film-batch: {B} instances/rank of the 80x20x1 std-problem-4 film (n=1600), "
+                               f"{window} ns each at alpha_G=0.02, seeded in-plane fields, per-instance RKSUITE 'M' "
+                               f"(tol 1e-6, output every 1 ps), {args.precision} tcgen05 demag GEMM",
+                   "instances_per_rank": B, "window_ns": window, "outputs": nt,
+                   "parallelism": f"instances sharded over {ws} rank(s)",
+                   "l2": "flushed (256 MB write) before every timed step"},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
+                     "frac": achieved / peak_tf, "traffic": None,
+                     "note": f"batch_kernel: 18*n^2 useful flops per instance RHS evaluation x {evals} evaluations "
+                             f"over {kms:.1f} ms of device time; peak = sustained cuBLAS bf16 ({src})"},
+        "plain_fp32_same_geometry": {"value": plain_rate, "unit": "simulated ns/s",
+                                     "note": f"single-instance FP32 path, {plain_window} ns window"},
+        "batched_over_plain": value / ws / plain_rate,
+        "gpu_launches": int(launches),
+        "rhs_evals_per_s": evals / (sum(times) / 1e3) * ws,
+        "clocks": clocks,
+    }
+    if e2e_ms is not None:
+        line["e2e"] = {"value": sim_ns / (e2e_red / 1e3), "unit": "simulated ns/s",
+                       "h2d_bytes_per_step": B * 3 * n * 8, "d2h_bytes_per_step": B * nt * 3 * n * 8}
+    return line
+
+
+def bench_plain(torch, args, ws, rank, local, dist, hbm, src):
+    from magtense_b200 import Solver
+    large = args.workload == "large-plain"
+    res, L = (LARGE_RES, LARGE_L) if large else (FILM_RES, FILM_L)
+    n = int(np.prod(res))
+    window = (0.002 if large else 0.05) if args.window is None else args.window
+    win = window * 1e-9
+    nt = max(2, int(round(window / 1e-3)) + 1)
+    t = np.linspace(0, win, nt)
+    if large:
+        rng = np.random.default_rng(1)
+        axis = rng.standard_normal(3)
+        axis /= np.linalg.norm(axis)
+        s = Solver(res, L, K0=5e3, u_ea=np.tile(axis, (n, 1)))
+        s.assemble()
+        m = rng.standard_normal((3, n))
+        m_s = torch.as_tensor((m / np.linalg.norm(m, axis=0)).reshape(-1), device="cuda")
+        h = np.array([10e-3 / MU0, 0.0, 0.0])
+        s.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.1, hext=np.array([[0.0, *h], [win, *h]]))
+    else:
+        s, m_s = relaxed_state(torch, res, L)
+        h = instance_fields(1000 + rank, 1)[0]
+        s.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.02, hext=np.array([[0.0, *h], [win, *h]]))
+
+    def step():
+        _, _, _, st = s.integrate(t, m_s, tol=1e-6)
+        return [st]
+
+    times, stats, clocks, flush = timed_steps(torch, step, args.steps, args.warmup, dist, local)
+    m_host = m_s.cpu().numpy()
+    e2e = []
+    for _ in range(max(1, args.steps)):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m0 = torch.from_numpy(m_host).pin_memory().to("cuda", non_blocking=True)
+        _, y, _, _ = s.integrate(t, m0, tol=1e-6)
+        y.cpu()
+        torch.cuda.synchronize()
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    step_ms, e2e_ms = max_over_ranks(torch, dist, [max(times), statistics.median(e2e)])
+    if rank != 0:
+        return None
+    flat = [x for st in stats for x in st]
+    evals = sum(x["f_evals"] for x in flat)
+    kms = sum(x["kernel_ms"] for x in flat)
+    launches = sum(x["launches"] for x in flat)
+    achieved = 24.0 * n * n * evals / (kms / 1e3) / 1e9
+    sim_ns = ws * window
+    return {
+        "metric": "simulated ns/s", "value": sim_ns / (step_ms / 1e3), "unit": "simulated ns/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": ("large-plain: 64x64x8 cubes of 5 nm (n=32768, 25.8 GB FP32 tensor), K=5e3 J/m^3 "
+                                "along a seeded axis, 10 mT field, alpha_G=0.1" if large else
+                                "film-plain: 80x20x1 std-problem-4 film (n=1600), single instance") +
+                               ", plain FP32 demag, persistent single-instance integrator, tol 1e-6",
+                   "window_ns": window, "outputs": nt, "parallelism": f"one instance per rank, {ws} rank(s)",
+                   "l2": "flushed (256 MB write) before every timed step"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None,
+                     "note": f"integrate_kernel: 24*n^2 tensor bytes per RHS evaluation x {evals} evaluations over "
+                             f"{kms:.2f} ms of device time; peak {src} HBM copy"},
+        "e2e": {"value": sim_ns / (e2e_ms / 1e3), "unit": "simulated ns/s", "h2d_bytes_per_step": 3 * n * 8,
+                "d2h_bytes_per_step": nt * 3 * n * 8},
+        "gpu_launches": int(launches),
+        "rhs_evals_per_s": evals / (sum(times) / 1e3) * ws,
+        "clocks": clocks,
+    }
 
 
 def main():

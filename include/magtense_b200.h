@@ -134,6 +134,8 @@ typedef struct mt_batch mt_batch;
 #define MT_PREC_FP32 0     /* FP32 SIMT product, same arithmetic as the single-instance path */
 #define MT_PREC_BF16X3 1   /* tcgen05, K and m split into BF16 hi+lo, 3 products, FP32 accumulate */
 #define MT_PREC_BF16X2 2   /* tcgen05, K split hi+lo, m in BF16, 2 products, FP32 accumulate */
+#define MT_PREC_FP16X3S 3  /* tcgen05, rows of K scaled by powers of two, K and m split into FP16 hi+lo,
+                              3 products, FP32 accumulate (about FP32 accuracy) */
 
 int mt_batch_create(const mt_grid* grid, int B, int precision, mt_batch** out);
 int mt_batch_destroy(mt_batch* b);

@@ -64,6 +64,22 @@ MT_DEV double* dst_ptr(const BCtx& X, int id, int b)
     return VSTG(X, id, b);
 }
 
+// hi/lo split of one FP32 value into the 16-bit operand format of the precision
+MT_DEV void split_store(float f, int prec, uint16_t* hi_out, uint16_t* lo_out)
+{
+    if (prec == kPrecFP16x3S) {
+        const __half hi = __float2half_rn(f);
+        const __half lo = __float2half_rn(f - __half2float(hi));
+        *hi_out = __half_as_ushort(hi);
+        *lo_out = __half_as_ushort(lo);
+    } else {
+        const __nv_bfloat16 hi = __float2bfloat16_rn(f);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(f - __bfloat162float(hi));
+        *hi_out = __bfloat16_as_ushort(hi);
+        *lo_out = __bfloat16_as_ushort(lo);
+    }
+}
+
 // own elements of one instance, lane-strided: component a, cell i, index q = a*n + i
 #define FOR_OWN_W(X, q)                                                                       \
     for (int _e = (X).lane; _e < 3 * (X).nc; _e += 32)                                        \
@@ -81,10 +97,7 @@ MT_DEV void put_arg(const BCtx& X, int argi, int b, int q, double v)
         X.F.m32[((size_t)b * 3 + a) * X.P.ldk + i] = f;
     } else {
         const size_t col = (size_t)b * X.Q.Kd + (size_t)a * X.Q.np + i;
-        const __nv_bfloat16 hi = __float2bfloat16_rn(f);
-        const __nv_bfloat16 lo = __float2bfloat16_rn(f - __bfloat162float(hi));
-        X.F.mhi[col] = __bfloat16_as_ushort(hi);
-        X.F.mlo[col] = __bfloat16_as_ushort(lo);
+        split_store(f, X.Q.prec, X.F.mhi + col, X.F.mlo + col);
     }
 }
 
@@ -844,6 +857,23 @@ MT_DEV void epilogue(const BCtx& X, BInst& I, int b)
     __syncwarp();
 }
 
+MT_DEV void epilogue_cell(const BCtx& X, int b, double t_rhs, int arg, int dst, int i)
+{
+    const int n = X.P.n;
+    const TimeScalars ts = inst_scalars(X, b, t_rhs);
+    const double* m = VPOOL(X, arg, b);
+    double* out = dst_ptr(X, dst, b);
+    float S[3];
+    for (int a = 0; a < 3; ++a) {
+        float acc = 0.f;
+        for (int sp = 0; sp < X.Q.S; ++sp) acc += ldcg(&X.F.hpart[(((size_t)sp * X.Q.Bp + b) * 3 + a) * X.Q.np + i]);
+        S[a] = acc;
+    }
+    double o[3];
+    cell_rhs(X.P, m, i, S, ts, o);
+    out[i] = o[0]; out[n + i] = o[1]; out[2 * n + i] = o[2];
+}
+
 // ---------------------------------------------------------------------------
 // FP32 SIMT demag tile: H[s][inst][a][cell] for cells of block cb, instances of
 // block ib, sources of split s, from the cell-row FP32 tensor.
@@ -857,7 +887,9 @@ MT_DEV void gemm_tile_simt(const BCtx& X)
     float* Ms = Ks + 6 * kSimtJT * kCellBlock;             // [JT][3][64]
     const int tid = threadIdx.x;
     const int tc = tid & 31, ti = tid >> 5;                // 32 cell groups x 16 instance groups
-    const int cbase = X.cb * kCellBlock, ibase = X.ib * kInstBlock;
+    const int cbase = X.cb * kCellBlock;
+    for (int half = 0; half < kInstBlock / 64; ++half) {
+    const int ibase = X.ib * kInstBlock + half * 64;
     const int j4tot = ldk >> 2;
     const int js = (int)(((long long)j4tot * X.s) / X.Q.S) * 4;
     const int je = (int)(((long long)j4tot * (X.s + 1)) / X.Q.S) * 4;
@@ -880,15 +912,15 @@ MT_DEV void gemm_tile_simt(const BCtx& X)
             float* d = Ks + (c * kSimtJT + 4 * j4) * kCellBlock + cell;
             d[0] = v.x; d[kCellBlock] = v.y; d[2 * kCellBlock] = v.z; d[3 * kCellBlock] = v.w;
         }
-        for (int e = tid; e < kInstBlock * 3 * (kSimtJT / 4); e += blockDim.x) {
+        for (int e = tid; e < 64 * 3 * (kSimtJT / 4); e += blockDim.x) {
             const int inst = e / (3 * (kSimtJT / 4));
             const int rem = e - inst * 3 * (kSimtJT / 4);
             const int bb = rem / (kSimtJT / 4), j4 = rem - bb * (kSimtJT / 4);
             float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
             if (4 * j4 < len)
                 v = __ldcg(reinterpret_cast<const float4*>(X.F.m32 + ((size_t)(ibase + inst) * 3 + bb) * ldk + j0) + j4);
-            float* d = Ms + ((4 * j4) * 3 + bb) * kInstBlock + inst;
-            d[0] = v.x; d[3 * kInstBlock] = v.y; d[6 * kInstBlock] = v.z; d[9 * kInstBlock] = v.w;
+            float* d = Ms + ((4 * j4) * 3 + bb) * 64 + inst;
+            d[0] = v.x; d[3 * 64] = v.y; d[6 * 64] = v.z; d[9 * 64] = v.w;
         }
         __syncthreads();
         for (int jj = 0; jj < len; ++jj) {
@@ -900,7 +932,7 @@ MT_DEV void gemm_tile_simt(const BCtx& X)
 #pragma unroll
             for (int r = 0; r < 4; ++r)
 #pragma unroll
-                for (int bb = 0; bb < 3; ++bb) mv[r][bb] = Ms[(jj * 3 + bb) * kInstBlock + ti + 16 * r];
+                for (int bb = 0; bb < 3; ++bb) mv[r][bb] = Ms[(jj * 3 + bb) * 64 + ti + 16 * r];
 #pragma unroll
             for (int q = 0; q < 4; ++q)
 #pragma unroll
@@ -920,13 +952,15 @@ MT_DEV void gemm_tile_simt(const BCtx& X)
                 const int cell = cbase + tc + 32 * q, inst = ibase + ti + 16 * r;
                 X.F.hpart[(((size_t)X.s * X.Q.Bp + inst) * 3 + a) * X.Q.np + cell] = acc[q][r][a];
             }
+    __syncthreads();
+    }
 }
 
-constexpr int kMaxInstPerWarp = 4;
+constexpr int kMaxInstPerWarp = 8;
 
 MT_DEV size_t batch_gemm_smem(int prec)
 {
-    return prec == kPrecFP32 ? (size_t)(6 * kSimtJT * kCellBlock + kSimtJT * 3 * kInstBlock) * sizeof(float)
+    return prec == kPrecFP32 ? (size_t)(6 * kSimtJT * kCellBlock + kSimtJT * 3 * 64) * sizeof(float)
                              : tc_smem_bytes();
 }
 
@@ -951,6 +985,8 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
     X.nwarps = blockDim.x >> 5;
     X.smem = smem_raw;
     const bool tc = Q.prec != kPrecFP32;
+    struct ReqDesc { double t; int on, arg, dst, pad; };
+    __shared__ ReqDesc s_req[kInstBlock];
     TcState tcs;
     tcs.kb_done = 0; tcs.tiles = 0; tcs.tmem = 0;
     if (tc) tc_init_impl(X.smem, tcs);
@@ -968,7 +1004,8 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
     if (Q.demag_only) {
         // one product of the operands already in place, then H = -Ms * sum of partials
         if (!tc) gemm_tile_simt(X);
-        else ok = tc_gemm_tile_impl(X.smem, Q, F, maps, X.cb, X.ib, X.s, Q.prec == kPrecBF16x3, tcs);
+        else ok = tc_gemm_tile_impl(X.smem, Q, F, maps, X.cb, X.ib, X.s, Q.prec != kPrecBF16x2,
+                                    Q.prec == kPrecFP16x3S, Q.prec == kPrecFP16x3S ? Q.row_inv : nullptr, tcs);
         if (ok && grid_sync(F.gs, 5)) {
             const int n = P.n;
             for (int e = threadIdx.x; e < X.ni * 3 * X.nc; e += blockDim.x) {
@@ -985,8 +1022,21 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
         if (tc) tc_finish_impl(X.smem, tcs);
         return;
     }
+    const bool prof = F.prof != nullptr && threadIdx.x == 0;
+    unsigned long long acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint64_t tp = prof ? globaltimer_ns() : 0;
+#define PROF_MARK(k)                                       \
+    do {                                                   \
+        if (prof) {                                        \
+            const uint64_t _n = globaltimer_ns();          \
+            acc[k] += _n - tp;                             \
+            tp = _n;                                       \
+        }                                                  \
+    } while (0)
+    long long ticks_run = 0;
     for (long long tick = 0; tick < Q.ticks_per_launch && ok; ++tick) {
         unsigned* ctr = F.counters + 2 * (tick % 3);
+        ticks_run++;
         // P2: resolve reductions, advance
         int my_active = 0, my_rhs = 0;
         for (int k = 0; k < mine; ++k) {
@@ -1002,32 +1052,76 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
         if (X.lane == 0 && X.cb == 0 && (my_active | my_rhs)) {
             atomicAdd(&ctr[0], (unsigned)my_active);
             atomicAdd(&ctr[1], (unsigned)my_rhs);
+            if (my_rhs) atomicAdd(&F.ibreq[(tick % 3) * Q.IB + X.ib], (unsigned)my_rhs);
         }
+        __syncthreads();
+        PROF_MARK(0);
         if (!grid_sync(F.gs, 1)) { ok = false; break; }
+        PROF_MARK(1);
         const unsigned active = __ldcg(&ctr[0]);
-        const unsigned nreq = __ldcg(&ctr[1]);
+        const unsigned nreq = __ldcg(&F.ibreq[(tick % 3) * Q.IB + X.ib]);   // requests in this tile's instances
         if (t == 0 && threadIdx.x == 0) {
             unsigned* nxt = F.counters + 2 * ((tick + 1) % 3);
             nxt[0] = 0; nxt[1] = 0;
+            for (int k = 0; k < Q.IB; ++k) F.ibreq[((tick + 1) % 3) * Q.IB + k] = 0;
         }
         if (active == 0) break;
         if (nreq > 0) {
             if (!tc) gemm_tile_simt(X);
-            else if (!tc_gemm_tile_impl(X.smem, Q, F, maps, X.cb, X.ib, X.s, Q.prec == kPrecBF16x3, tcs)) ok = false;
+            else if (!tc_gemm_tile_impl(X.smem, Q, F, maps, X.cb, X.ib, X.s, Q.prec != kPrecBF16x2,
+                                        Q.prec == kPrecFP16x3S, Q.prec == kPrecFP16x3S ? Q.row_inv : nullptr, tcs))
+                ok = false;
         }
+        __syncthreads();
+        PROF_MARK(2);
         if (!grid_sync(F.gs, 2)) { ok = false; break; }
+        PROF_MARK(3);
         if (!ok) break;
-        // P1: epilogue for right-hand-side requests, advance
+        // P1: LL epilogue of every requesting instance on the owned cells, spread
+        // over all threads, then each warp advances its instances
+        for (int k = 0; k < mine; ++k) {
+            const BInst& I = L[k];
+            if (X.lane == 0) {
+                const int li = X.warp + k * X.nwarps;
+                s_req[li].on = (X.i0 + li < Q.B && I.req == 1) ? 1 : 0;
+                s_req[li].arg = I.rhs_arg;
+                s_req[li].dst = I.rhs_dst;
+                s_req[li].t = I.t_rhs;
+            }
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < X.ni * X.nc; e += blockDim.x) {
+            const int li = e / X.nc, cell = e - li * X.nc;
+            if (!s_req[li].on) continue;
+            epilogue_cell(X, X.i0 + li, s_req[li].t, s_req[li].arg, s_req[li].dst, X.c0 + cell);
+        }
+        __syncthreads();
         for (int k = 0; k < mine; ++k) {
             BInst& I = L[k];
             const int b = X.i0 + X.warp + k * X.nwarps;
             if (b >= Q.B || I.req != 1) continue;
-            epilogue(X, I, b);
             I.req = 0;
             advance(X, I, b);
         }
+        __syncthreads();
+        PROF_MARK(4);
         if (!grid_sync(F.gs, 3)) { ok = false; break; }
+        PROF_MARK(5);
     }
+    if (prof) {
+        if (t == 0) {
+            for (int k = 0; k < 6; ++k) atomicAdd(&F.prof[k], acc[k]);
+            atomicAdd(&F.prof[7], (unsigned long long)ticks_run);
+        }
+        // busiest CTA per work phase (P2, GEMM, P1): value and CTA index
+        const int work[3] = {0, 2, 4};
+        for (int k = 0; k < 3; ++k) {
+            const unsigned long long v = acc[work[k]];
+            const unsigned long long old = atomicMax(&F.prof[8 + k], v);
+            if (v > old) F.prof[12 + k] = (unsigned long long)t;
+        }
+    }
+#undef PROF_MARK
     if (tc) tc_finish_impl(X.smem, tcs);
     if (ok && X.lane == 0) {
         for (int k = 0; k < mine; ++k) {
@@ -1039,8 +1133,35 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
     }
 }
 
-// FP32 cell-row tensor -> BF16 hi/lo [3np][Kd] (rows (a,i), cols (b,j)), zero padded
-__global__ void split_tensor_kernel(const float* __restrict__ K, int n, int ldk, int np, uint16_t* __restrict__ khi,
+// power-of-two row scale for the fp16s tensor: largest |K| of row r into [2^13, 2^14)
+__global__ void row_scale_kernel(const float* __restrict__ K, int n, int ldk, int np, float* __restrict__ row_inv)
+{
+    const int row = blockIdx.x;          // (a, i) row of the 3np x 3np matrix
+    const int a = row / np, i = row - a * np;
+    static const int blk[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    float mx = 0.f;
+    if (i < n)
+        for (int bb = 0; bb < 3; ++bb)
+            for (int j = threadIdx.x; j < n; j += blockDim.x)
+                mx = fmaxf(mx, fabsf(K[((size_t)i * 6 + blk[a][bb]) * ldk + j]));
+    __shared__ float red[32];
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float m = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, red[w]);
+        int e = 0;
+        if (m > 0.f) { frexpf(m, &e); }          // m = f * 2^e, f in [0.5, 1)
+        const int shift = (m > 0.f) ? 14 - e : 0;  // m * 2^shift in [2^13, 2^14)
+        row_inv[row] = ldexpf(1.0f, -shift);
+    }
+}
+
+// FP32 cell-row tensor -> 16-bit hi/lo [3np][Kd] (rows (a,i), cols (b,j)), zero padded;
+// fp16s rows are multiplied by 1/row_inv first
+__global__ void split_tensor_kernel(const float* __restrict__ K, int n, int ldk, int np, int prec,
+                                    const float* __restrict__ row_inv, uint16_t* __restrict__ khi,
                                     uint16_t* __restrict__ klo)
 {
     const int Kd = 3 * np;
@@ -1051,10 +1172,8 @@ __global__ void split_tensor_kernel(const float* __restrict__ K, int n, int ldk,
         const int a = row / np, i = row - a * np, bb = col / np, j = col - bb * np;
         float v = 0.f;
         if (i < n && j < n) v = K[((size_t)i * 6 + blk[a][bb]) * ldk + j];
-        const __nv_bfloat16 hi = __float2bfloat16_rn(v);
-        const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
-        khi[e] = __bfloat16_as_ushort(hi);
-        klo[e] = __bfloat16_as_ushort(lo);
+        if (prec == kPrecFP16x3S) v = v / row_inv[row];   // exact: power of two
+        split_store(v, prec, khi + e, klo + e);
     }
 }
 
@@ -1072,10 +1191,7 @@ __global__ void batch_operand_kernel(const double* __restrict__ m, int B, int n,
             m32[((size_t)b * 3 + a) * ldk + i] = f;
         } else {
             const size_t col = (size_t)b * 3 * np + (size_t)a * np + i;
-            const __nv_bfloat16 hi = __float2bfloat16_rn(f);
-            const __nv_bfloat16 lo = __float2bfloat16_rn(f - __bfloat162float(hi));
-            mhi[col] = __bfloat16_as_ushort(hi);
-            mlo[col] = __bfloat16_as_ushort(lo);
+            split_store(f, prec, mhi + col, mlo + col);
         }
     }
 }
@@ -1117,29 +1233,54 @@ int batch_grid(int n, int B, int num_sms, int prec, int* CB, int* IB, int* S)
 size_t batch_smem_bytes(int n, int ldk, int prec)
 {
     (void)n; (void)ldk;
-    return prec == kPrecFP32 ? (size_t)(6 * kSimtJT * kCellBlock + kSimtJT * 3 * kInstBlock) * sizeof(float)
+    return prec == kPrecFP32 ? (size_t)(6 * kSimtJT * kCellBlock + kSimtJT * 3 * 64) * sizeof(float)
                              : tc_smem_bytes();
 }
 
 cudaError_t launch_batch(const DevProb& P, const BatchBufs& Bf, const BatchParams& Q, int grid, const void* tmaps,
-                         cudaStream_t s)
+                         cudaStream_t s, const void* l2_base, size_t l2_bytes, float l2_hit)
 {
     const size_t smem = batch_smem_bytes(P.n, P.ldk, Q.prec);
     cudaError_t e = cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    DevProb p = P;
-    BatchBufs b = Bf;
-    BatchParams q = Q;
     TcMaps m;
     memset(&m, 0, sizeof(m));
     if (tmaps) memcpy(&m, tmaps, sizeof(m));
-    void* args[] = {&p, &b, &q, &m};
-    return cudaLaunchCooperativeKernel((const void*)batch_kernel, dim3(grid), dim3(kBatchThreads), args, smem, s);
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kBatchThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[2];
+    memset(attr, 0, sizeof(attr));
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    int na = 1;
+    if (l2_base && l2_bytes) {
+        // keep the split tensor resident in L2 across ticks (the per-instance state streams past it)
+        attr[1].id = cudaLaunchAttributeAccessPolicyWindow;
+        attr[1].val.accessPolicyWindow.base_ptr = const_cast<void*>(l2_base);
+        attr[1].val.accessPolicyWindow.num_bytes = l2_bytes;
+        attr[1].val.accessPolicyWindow.hitRatio = l2_hit;
+        attr[1].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        attr[1].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        na = 2;
+    }
+    cfg.attrs = attr;
+    cfg.numAttrs = na;
+    return cudaLaunchKernelEx(&cfg, batch_kernel, P, Bf, Q, m);
 }
 
-cudaError_t launch_split_tensor(const float* K, int n, int ldk, int np, uint16_t* khi, uint16_t* klo, cudaStream_t s)
+cudaError_t launch_split_tensor(const float* K, int n, int ldk, int np, int prec, uint16_t* khi, uint16_t* klo,
+                                float* row_inv, cudaStream_t s)
 {
-    split_tensor_kernel<<<1184, 256, 0, s>>>(K, n, ldk, np, khi, klo);
+    if (prec == kPrecFP16x3S) {
+        row_scale_kernel<<<3 * np, 256, 0, s>>>(K, n, ldk, np, row_inv);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    split_tensor_kernel<<<1184, 256, 0, s>>>(K, n, ldk, np, prec, row_inv, khi, klo);
     return cudaGetLastError();
 }
 

@@ -8,10 +8,10 @@
 
 constexpr int kBatchThreads = 512;
 constexpr int kCellBlock = 128;   // receiver cells per tile (tcgen05 M = 128)
-constexpr int kInstBlock = 64;    // instances per tile (tcgen05 N = 64)
+constexpr int kInstBlock = 128;   // instances per tile (tcgen05 N = 128)
 constexpr int kRedSlots = 4;      // values per reduction
 
-enum BatchPrecision { kPrecFP32 = 0, kPrecBF16x3 = 1, kPrecBF16x2 = 2 };
+enum BatchPrecision { kPrecFP32 = 0, kPrecBF16x3 = 1, kPrecBF16x2 = 2, kPrecFP16x3S = 3 };
 
 // Per-instance coroutine state: RKSUITE scalars plus the resume point and the
 // locals that live across a yield.  One private copy per owning CTA.
@@ -55,6 +55,8 @@ struct BatchBufs {
     BInst* inst;       // [CB][Bp] private coroutine copies
     GridSync* gs;
     unsigned* counters;  // [3][2]: active instances, right-hand-side requests
+    unsigned* ibreq;     // [3][IB]: right-hand-side requests per instance block
+    unsigned long long* prof;  // [8] phase times (ns) seen by CTA 0, or nullptr
     // per-instance inputs
     const double* hext;    // [Bp][nt_hext][4]
     const double* alpha0;  // [Bp]
@@ -74,13 +76,15 @@ struct BatchParams {
     // tcgen05 operands
     const uint16_t* khi;      // [3np][Kd] BF16 tensor (rows (a,i), cols (b,j))
     const uint16_t* klo;
+    const float* row_inv;     // [3np] 1/s_r of the fp16s tensor rows
 };
 
 cudaError_t batch_upload_tables();
 int batch_grid(int n, int B, int num_sms, int prec, int* CB, int* IB, int* S);
 size_t batch_smem_bytes(int n, int ldk, int prec);
 cudaError_t launch_batch(const DevProb& P, const BatchBufs& Bf, const BatchParams& Q, int grid, const void* tmaps,
-                         cudaStream_t s);
-cudaError_t launch_split_tensor(const float* K, int n, int ldk, int np, uint16_t* khi, uint16_t* klo, cudaStream_t s);
+                         cudaStream_t s, const void* l2_base = nullptr, size_t l2_bytes = 0, float l2_hit = 0.f);
+cudaError_t launch_split_tensor(const float* K, int n, int ldk, int np, int prec, uint16_t* khi, uint16_t* klo,
+                                float* row_inv, cudaStream_t s);
 cudaError_t launch_batch_operand(const double* m, int B, int n, int ldk, int np, int prec, float* m32, uint16_t* mhi,
                                  uint16_t* mlo, cudaStream_t s);

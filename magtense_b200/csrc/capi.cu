@@ -508,6 +508,7 @@ struct mt_batch {
     int CB = 0, IB = 0, S = 0, np = 0, Kd = 0, grid = 0;
     uint16_t* khi = nullptr;
     uint16_t* klo = nullptr;
+    float* row_inv = nullptr;
     double* hext = nullptr;
     double* alpha0 = nullptr;
     int nt_hext = 0;
@@ -561,7 +562,7 @@ int mt_batch_create(const mt_grid* g, int B, int precision, mt_batch** out)
     if (!out) return fail(MT_ERR_ARG, "null argument");
     *out = nullptr;
     if (B < 1) return fail(MT_ERR_ARG, "B must be >= 1");
-    if (precision < 0 || precision > 2) return fail(MT_ERR_ARG, "unknown precision %d", precision);
+    if (precision < 0 || precision > 3) return fail(MT_ERR_ARG, "unknown precision %d", precision);
     mt_handle* h = nullptr;
     int rc = mt_create(g, &h);
     if (rc) return rc;
@@ -581,7 +582,7 @@ int mt_batch_create(const mt_grid* g, int B, int precision, mt_batch** out)
 int mt_batch_destroy(mt_batch* bt)
 {
     if (!bt) return MT_OK;
-    free_ptr(bt->khi); free_ptr(bt->klo); free_ptr(bt->hext); free_ptr(bt->alpha0);
+    free_ptr(bt->khi); free_ptr(bt->row_inv); free_ptr(bt->hext); free_ptr(bt->alpha0);
     mt_destroy(bt->h);
     delete bt;
     return MT_OK;
@@ -624,8 +625,13 @@ int mt_batch_assemble_demag(mt_batch* bt, void* stream)
     if (rc) return rc;
     if (bt->prec != MT_PREC_FP32) {
         const size_t cnt = (size_t)bt->Kd * bt->Kd;
-        if (!bt->khi) { CUDA_TRY(dalloc(&bt->khi, cnt)); CUDA_TRY(dalloc(&bt->klo, cnt)); }
-        CUDA_TRY(launch_split_tensor(bt->h->K, bt->h->n, bt->h->ldk, bt->np, bt->khi, bt->klo, (cudaStream_t)stream));
+        if (!bt->khi) {
+            CUDA_TRY(dalloc(&bt->khi, 2 * cnt));   // hi and lo contiguous: one L2 persistence window
+            bt->klo = bt->khi + cnt;
+            CUDA_TRY(dalloc(&bt->row_inv, (size_t)bt->Kd));
+        }
+        CUDA_TRY(launch_split_tensor(bt->h->K, bt->h->n, bt->h->ldk, bt->np, bt->prec, bt->khi, bt->klo, bt->row_inv,
+                                     (cudaStream_t)stream));
     }
     return MT_OK;
 }
@@ -679,21 +685,27 @@ int batch_alloc(mt_batch* bt, BatchRun& R, int nt, cudaStream_t s)
     CUDA_TRY(R.A.get(&F.gs, 1));
     CUDA_TRY(R.A.get(&F.counters, 6));
     CUDA_TRY(cudaMemsetAsync(F.counters, 0, sizeof(unsigned) * 6, s));
+    CUDA_TRY(R.A.get(&F.ibreq, 3 * (size_t)bt->IB));
+    CUDA_TRY(cudaMemsetAsync(F.ibreq, 0, sizeof(unsigned) * 3 * bt->IB, s));
+    if (getenv("MT_BATCH_PROFILE")) {
+        CUDA_TRY(R.A.get(&F.prof, 16));
+        CUDA_TRY(cudaMemsetAsync(F.prof, 0, sizeof(unsigned long long) * 16, s));
+    }
     F.hext = bt->hext;
     F.alpha0 = bt->alpha0;
     BatchParams& Q = R.Q;
     memset(&Q, 0, sizeof(Q));
     Q.Bp = Bp; Q.B = bt->B; Q.CB = bt->CB; Q.IB = bt->IB; Q.S = bt->S; Q.np = bt->np; Q.Kd = bt->Kd;
     Q.nt = nt; Q.nt_hext = bt->nt_hext; Q.prec = bt->prec;
-    Q.khi = bt->khi; Q.klo = bt->klo;
+    Q.khi = bt->khi; Q.klo = bt->klo; Q.row_inv = bt->row_inv;
     Q.renorm = h->renorm;
     memset(&R.maps, 0, sizeof(R.maps));
     if (bt->prec != MT_PREC_FP32) {
         int rc;
         if ((rc = make_tmap(&R.maps.ahi, bt->khi, bt->Kd, bt->Kd, 128))) return rc;
         if ((rc = make_tmap(&R.maps.alo, bt->klo, bt->Kd, bt->Kd, 128))) return rc;
-        if ((rc = make_tmap(&R.maps.bhi, F.mhi, bt->Kd, Bp, 64))) return rc;
-        if ((rc = make_tmap(&R.maps.blo, F.mlo, bt->Kd, Bp, 64))) return rc;
+        if ((rc = make_tmap(&R.maps.bhi, F.mhi, bt->Kd, Bp, kTcN))) return rc;
+        if ((rc = make_tmap(&R.maps.blo, F.mlo, bt->Kd, Bp, kTcN))) return rc;
     }
     return MT_OK;
 }
@@ -815,12 +827,38 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
     double kernel_ms = 0.0;
     long long launches = 0;
     std::vector<BInst> hs(Bp);
+    // L2 residency of the split tensor (process-local limit, restored on return)
+    size_t l2_bytes = 0;
+    float l2_hit = 0.f;
+    size_t prev_limit = 0;
+    bool limit_set = false;
+    if (bt->prec != MT_PREC_FP32 && !getenv("MT_NO_L2_PERSIST")) {
+        int max_persist = 0, max_win = 0;
+        cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, h->device);
+        cudaDeviceGetAttribute(&max_win, cudaDevAttrMaxAccessPolicyWindowSize, h->device);
+        const size_t want = 2 * (size_t)bt->Kd * bt->Kd * sizeof(uint16_t);
+        if (max_persist > 0 && max_win > 0 && cudaDeviceGetLimit(&prev_limit, cudaLimitPersistingL2CacheSize) == cudaSuccess) {
+            const size_t lim = std::min(want, (size_t)max_persist);
+            if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, lim) == cudaSuccess) {
+                limit_set = true;
+                l2_bytes = std::min(want, (size_t)max_win);
+                l2_hit = (float)std::min(1.0, (double)lim / (double)l2_bytes);
+            }
+        }
+        cudaGetLastError();
+    }
+    struct L2Guard {
+        bool on; size_t prev;
+        ~L2Guard() { if (on) { cudaCtxResetPersistingL2Cache(); cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, prev); } }
+    } l2g{limit_set, prev_limit};
     long long last_sig = -1;
     for (;;) {
         CUDA_TRY(cudaMemsetAsync(F.gs, 0, sizeof(GridSync), s));
         CUDA_TRY(cudaMemsetAsync(F.counters, 0, sizeof(unsigned) * 6, s));
+        CUDA_TRY(cudaMemsetAsync(F.ibreq, 0, sizeof(unsigned) * 3 * bt->IB, s));
         CUDA_TRY(cudaEventRecord(ev0, s));
-        CUDA_TRY(launch_batch(P, F, Q, bt->grid, bt->prec != MT_PREC_FP32 ? &R.maps : nullptr, s));
+        CUDA_TRY(launch_batch(P, F, Q, bt->grid, bt->prec != MT_PREC_FP32 ? &R.maps : nullptr, s,
+                              l2_bytes ? bt->khi : nullptr, l2_bytes, l2_hit));
         CUDA_TRY(cudaEventRecord(ev1, s));
         GridSync gs_h;
         CUDA_TRY(cudaMemcpyAsync(&gs_h, F.gs, sizeof(gs_h), cudaMemcpyDeviceToHost, s));
@@ -865,6 +903,15 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
     }
     stats[0].launches = launches;
     stats[0].kernel_ms = kernel_ms;
+    if (F.prof) {
+        unsigned long long pr[16];
+        CUDA_TRY(cudaMemcpy(pr, F.prof, sizeof(pr), cudaMemcpyDeviceToHost));
+        const double tk = pr[7] ? (double)pr[7] : 1.0;
+        fprintf(stderr, "[batch profile] ticks %llu  per tick (us) at CTA 0: P2 %.2f B1 %.2f GEMM %.2f Bh %.2f P1 %.2f B2 %.2f"
+                "  busiest CTA: P2 %.2f (cta %llu) GEMM %.2f (cta %llu) P1 %.2f (cta %llu)\n",
+                pr[7], pr[0] / tk / 1e3, pr[1] / tk / 1e3, pr[2] / tk / 1e3, pr[3] / tk / 1e3, pr[4] / tk / 1e3,
+                pr[5] / tk / 1e3, pr[8] / tk / 1e3, pr[12], pr[9] / tk / 1e3, pr[13], pr[10] / tk / 1e3, pr[14]);
+    }
     if (worst) return fail(MT_ERR_SOLVER, "an instance stopped with RKSUITE flag %d", worst);
     return MT_OK;
 }

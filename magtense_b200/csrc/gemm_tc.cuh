@@ -1,22 +1,29 @@
 // tcgen05 (5th-generation tensor core) demag GEMM tile for the batched
 // integrator: H[a][cell][inst] = sum_k Khi/lo[(a, cell), k] * Mhi/lo[inst, k]
-// for the three field components a of 128 receiver cells and 64 instances,
+// for the three field components a of 128 receiver cells and 128 instances,
 // over one split of the 3n-long source dimension.
 //
 // Split-BF16: K32 = Khi + Klo and m32 = Mhi + Mlo (each part BF16, the low
 // part the BF16 rounding of the remainder), products accumulated in FP32 in
 // TMEM:  bf16x3 = Khi*Mhi + Khi*Mlo + Klo*Mhi ;  bf16x2 = Khi*Mhi + Klo*Mhi.
+// Split-FP16 with row scaling (fp16s): every tensor row r is multiplied by a
+// power of two s_r that puts its largest entry in [2^13, 2^14), then split
+// into FP16 hi+lo (22 significant bits); m splits into FP16 hi+lo; the three
+// products are accumulated in FP32 and the epilogue multiplies row r by 1/s_r
+// (exact).  Small entries of a row fall into the FP16 subnormal range, where
+// the absolute error stays below 2^-24 / s_r.
 //
 // Per k-block of 32 sources a stage holds A_hi[3], A_lo[3] (3 x 128 x 32 BF16
-// each), B_hi, B_lo (64 x 32 BF16), loaded by TMA (SWIZZLE_64B, no multicast)
+// each), B_hi, B_lo (128 x 32 BF16), loaded by TMA (SWIZZLE_64B, no multicast)
 // into a 3-stage shared-memory ring.  Warp 4 (one lane) issues the TMA loads,
-// warp 5 (one lane) issues tcgen05.mma (M=128, N=64, K=16) into three TMEM
-// accumulators (columns 0/64/128) and commits each stage back to its empty
+// warp 5 (one lane) issues tcgen05.mma (M=128, N=128, K=16) into three TMEM
+// accumulators (columns 0/128/256) and commits each stage back to its empty
 // barrier; warps 0-3 read the accumulators with tcgen05.ld and store them.
 // Every mbarrier wait is bounded; on a timeout the kernel's abort flag is set.
 #pragma once
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include "common.cuh"
 
 struct TcMaps {
@@ -30,11 +37,12 @@ struct TcState {
 };
 
 constexpr int kTcStages = 3;
+constexpr int kTcN = 128;                                    // instances per tile (MMA N)
 constexpr int kTcKB = 32;                                    // k elements per stage (64 B rows)
 constexpr int kTcABytes = 128 * kTcKB * 2;                   // one A tile
-constexpr int kTcBBytes = 64 * kTcKB * 2;                    // one B tile
-constexpr int kTcStageBytes = 6 * kTcABytes + 2 * kTcBBytes; // 56 KB
-constexpr int kTcTmemCols = 256;
+constexpr int kTcBBytes = kTcN * kTcKB * 2;                  // one B tile
+constexpr int kTcStageBytes = 6 * kTcABytes + 2 * kTcBBytes; // 64 KB
+constexpr int kTcTmemCols = 512;                             // three N-column accumulators
 
 static inline size_t tc_smem_bytes() { return 1024 + (size_t)kTcStages * kTcStageBytes + 256; }
 
@@ -90,14 +98,15 @@ MT_DEV uint64_t sdesc_sw64(uint32_t saddr)
     return d;
 }
 
-// instruction descriptor: D F32, A/B BF16, both K-major, M = 128, N = 64
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+// instruction descriptors: D F32, A/B BF16 (or F16), both K-major, M = 128, N = kTcN
+constexpr uint32_t kIdescBF16 = (1u << 4) | (1u << 7) | (1u << 10) | (((uint32_t)kTcN >> 3) << 17) | ((128u >> 4) << 24);
+constexpr uint32_t kIdescF16 = (1u << 4) | (0u << 7) | (0u << 10) | (((uint32_t)kTcN >> 3) << 17) | ((128u >> 4) << 24);
 
-MT_DEV void umma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
+MT_DEV void umma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate)
 {
     asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
                  " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
-                 "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate)
+                 "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
                  : "memory");
 }
 
@@ -185,7 +194,7 @@ MT_DEV void tc_finish_impl(unsigned char* smem, TcState& st)
 // Returns a CTA-uniform ok flag.
 template <typename QT, typename FT>
 MT_DEV bool tc_gemm_tile_impl(unsigned char* smem, const QT& Q, const FT& F, const TcMaps& maps, int cb, int ib, int s,
-                              bool three, TcState& st)
+                              bool three, bool f16, const float* row_inv, TcState& st)
 {
     TcSmem L = tc_layout(smem);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -209,8 +218,8 @@ MT_DEV bool tc_gemm_tile_impl(unsigned char* smem, const QT& Q, const FT& F, con
                 tma_load_2d(smem_u32(base + a * kTcABytes), &maps.ahi, x, y, fb);
                 tma_load_2d(smem_u32(base + (3 + a) * kTcABytes), &maps.alo, x, y, fb);
             }
-            tma_load_2d(smem_u32(base + 6 * kTcABytes), &maps.bhi, x, ib * 64, fb);
-            if (three) tma_load_2d(smem_u32(base + 6 * kTcABytes + kTcBBytes), &maps.blo, x, ib * 64, fb);
+            tma_load_2d(smem_u32(base + 6 * kTcABytes), &maps.bhi, x, ib * kTcN, fb);
+            if (three) tma_load_2d(smem_u32(base + 6 * kTcABytes + kTcBBytes), &maps.blo, x, ib * kTcN, fb);
         }
         if (!ok) {   // let loads already in flight land before the CTA moves on
             const long long issued = st.kb_done + nkb;
@@ -221,6 +230,7 @@ MT_DEV bool tc_gemm_tile_impl(unsigned char* smem, const QT& Q, const FT& F, con
         }
     } else if (warp == 5 && lane == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t idesc = f16 ? kIdescF16 : kIdescBF16;
         for (int kb = 0; kb < nkb; ++kb) {
             const long long g = st.kb_done + kb;
             const int stg = (int)(g % kTcStages);
@@ -235,12 +245,12 @@ MT_DEV bool tc_gemm_tile_impl(unsigned char* smem, const QT& Q, const FT& F, con
                 const uint64_t bl = sdesc_sw64(base + 6 * kTcABytes + kTcBBytes + koff);
 #pragma unroll
                 for (int a = 0; a < 3; ++a) {
-                    const uint32_t d = st.tmem + a * 64;
+                    const uint32_t d = st.tmem + a * kTcN;
                     const uint64_t ah = sdesc_sw64(base + a * kTcABytes + koff);
                     const uint64_t al = sdesc_sw64(base + (3 + a) * kTcABytes + koff);
-                    umma(d, ah, bh, (kb > 0 || kk > 0) ? 1u : 0u);
-                    if (three) umma(d, ah, bl, 1u);
-                    umma(d, al, bh, 1u);
+                    umma(d, ah, bh, idesc, (kb > 0 || kk > 0) ? 1u : 0u);
+                    if (three) umma(d, ah, bl, idesc, 1u);
+                    umma(d, al, bh, idesc, 1u);
                 }
             }
             umma_commit(smem_u32(&L.empty[stg]));
@@ -256,14 +266,15 @@ MT_DEV bool tc_gemm_tile_impl(unsigned char* smem, const QT& Q, const FT& F, con
             const int cell = cb * 128 + warp * 32 + lane;
 #pragma unroll 1
             for (int a = 0; a < 3; ++a) {
+                const float sc = row_inv ? __ldg(&row_inv[a * Q.np + cell]) : 1.0f;
 #pragma unroll 1
-                for (int half = 0; half < 2; ++half) {
+                for (int half = 0; half < kTcN / 32; ++half) {
                     float v[32];
-                    tmem_ld32(st.tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(a * 64 + half * 32), v);
+                    tmem_ld32(st.tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(a * kTcN + half * 32), v);
 #pragma unroll
                     for (int k = 0; k < 32; ++k) {
-                        const int inst = ib * 64 + half * 32 + k;
-                        F.hpart[(((size_t)s * Q.Bp + inst) * 3 + a) * Q.np + cell] = v[k];
+                        const int inst = ib * kTcN + half * 32 + k;
+                        F.hpart[(((size_t)s * Q.Bp + inst) * 3 + a) * Q.np + cell] = v[k] * sc;
                     }
                 }
             }

@@ -174,7 +174,7 @@ class Solver:
             pass
 
 
-PRECISIONS = {"fp32": 0, "bf16x3": 1, "bf16x2": 2}
+PRECISIONS = {"fp32": 0, "bf16x3": 1, "bf16x2": 2, "fp16s": 3}
 
 
 class BatchSolver:

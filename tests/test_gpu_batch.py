@@ -74,7 +74,7 @@ def test_batch_fp32_many_blocks(torch_cuda, oracle):
                         window=0.02e-9, nt=5, atol=1e-5, check_ids=[0, 37, 69])
 
 
-@pytest.mark.parametrize("precision,rtol", [("bf16x3", 3e-5), ("bf16x2", 5e-3)])
+@pytest.mark.parametrize("precision,rtol", [("bf16x3", 3e-5), ("bf16x2", 5e-3), ("fp16s", 1e-5)])
 def test_batch_demag_split_bf16_accuracy(torch_cuda, oracle, precision, rtol):
     from magtense_b200 import BatchSolver
     res, L = [24, 8, 2], [120e-9, 40e-9, 10e-9]
@@ -109,3 +109,9 @@ def test_batch_bf16x3_trajectories(torch_cuda, oracle):
     worst, stats = run_batch_vs_oracle(torch_cuda, oracle, [20, 5, 1], [125e-9, 31.25e-9, 3e-9], B=6,
                                        precision="bf16x3", window=0.1e-9, nt=21, atol=1e-4)
     print("bf16x3 worst |dm| vs oracle", worst)
+
+
+def test_batch_fp16s_trajectories(torch_cuda, oracle):
+    worst, stats = run_batch_vs_oracle(torch_cuda, oracle, [20, 5, 1], [125e-9, 31.25e-9, 3e-9], B=6,
+                                       precision="fp16s", window=0.1e-9, nt=21, atol=2e-5)
+    print("fp16s worst |dm| vs oracle", worst)
