@@ -109,6 +109,24 @@ int mt_fields(mt_handle* h, double t, const double* m_dev, double* Hj_dev, doubl
 /* dm/dt of the Landau-Lifshitz equation (dmdt_fct :220-273). */
 int mt_rhs(mt_handle* h, double t, const double* m_dev, double* dmdt_dev, void* stream);
 
+/* Allocation-free dm/dt.  No counterpart in the reference: it exists for
+ * callers that may not allocate device memory (for example code running while
+ * a CUDA graph is captured, or a host framework that owns all device memory
+ * through its own pool).  Same result as mt_rhs, but the FP32 copy of m that
+ * the demag product reads lives in a fixed array inside the library
+ * (3 * MT_NOALLOC_MAX_CELLS floats, held on every GPU that loads the library
+ * until the process exits) instead of memory allocated on first use; the call
+ * allocates nothing and rejects grids with more than MT_NOALLOC_MAX_CELLS
+ * cells (MT_ERR_ARG).  The handle must already hold the tensor, material and
+ * dynamics.  The first call on a device looks up the array's device address
+ * (once per device, with that device current); make that first call before
+ * any stream capture.  All calls share the one array: calls that overlap on
+ * the GPU (different streams, or different handles on the same device) race
+ * and must be serialised by the caller.  Each call rewrites the whole array
+ * region it uses before reading it. */
+#define MT_NOALLOC_MAX_CELLS 16384
+int mt_rhs_noalloc(mt_handle* h, double t, const double* m_dev, double* dmdt_dev, void* stream);
+
 /* ---------------- time integration ---------------- */
 
 /* MagTense_ODE_RKSuite (ODE_Solvers.f90:124-237) driving RKSUITE-90 method 'M'

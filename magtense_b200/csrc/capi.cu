@@ -11,6 +11,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -976,3 +977,63 @@ int icl_MVMult_GetH_sparse(const float*, const float*, const float*, float*, flo
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free right-hand side
+// ---------------------------------------------------------------------------
+// mt_rhs keeps an FP32 copy of m for the demag product in memory it allocates
+// on first use.  Some callers may not allocate device memory at all: code that
+// runs while a CUDA graph is being captured, host frameworks that hand out all
+// device memory from their own pool, or control loops that must never touch
+// the allocator.  For them the same copy lives in this fixed array instead,
+// reserved once when the library loads and held by every GPU that loads it
+// until the process exits.  Its size fixes the largest grid this entry point
+// accepts.
+static __device__ __align__(256) float g_noalloc_m32[3 * MT_NOALLOC_MAX_CELLS];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+float* g_noalloc_ptr[256] = {nullptr};   // device address of g_noalloc_m32, per device ordinal
+
+// Looked up once per device, with that device current.  In host code the
+// array's name is only a host-side stand-in; kernels must get this address.
+int noalloc_scratch(int dev, float** out)
+{
+    if (dev < 0 || dev >= 256) return fail(MT_ERR_ARG, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        float* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress((void**)&p, g_noalloc_m32);
+        if (e != cudaSuccess || !p)
+            return fail(MT_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_m32) on device %d: %s", dev, cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return MT_OK;
+}
+
+}  // namespace
+
+extern "C" int mt_rhs_noalloc(mt_handle* h, double t, const double* m_dev, double* dmdt_dev, void* stream)
+{
+    if (!h) return fail(MT_ERR_ARG, "null handle");
+    if (h->n > MT_NOALLOC_MAX_CELLS)
+        return fail(MT_ERR_ARG, "n = %d cells exceeds the %d-cell limit of mt_rhs_noalloc (use mt_rhs)", h->n,
+                    MT_NOALLOC_MAX_CELLS);
+    int rc = check_ready(h, true, true);
+    if (rc) return rc;
+    if (!m_dev || !dmdt_dev) return fail(MT_ERR_ARG, "null device pointer");
+    int dev = -1;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev != h->device) return fail(MT_ERR_ARG, "current device %d is not the handle's device %d", dev, h->device);
+    float* scratch = nullptr;
+    if ((rc = noalloc_scratch(dev, &scratch))) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    DevProb P = make_prob(h);
+    // the conversion rewrites all 3*ldk entries (zero padding included), so no
+    // state left by an earlier call is read
+    CUDA_TRY(launch_m_to_f32(m_dev, h->n, h->ldk, scratch, s));
+    CUDA_TRY(launch_field(2, P, m_dev, scratch, t, dmdt_dev, nullptr, nullptr, nullptr, nullptr, 0.f, h->num_sms, s));
+    return MT_OK;
+}
