@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--cpu-window", type=float, default=0.3, help="simulated ns of the bounded CPU sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--res", type=int, nargs=3, default=None,
+                    help="large-plain: override the grid (cubes of 5 nm), e.g. a small case for profiling")
     return ap.parse_args()
 
 
@@ -345,6 +347,9 @@ def bench_plain(torch, args, ws, rank, local, dist, hbm, src):
     from magtense_b200 import Solver
     large = args.workload == "large-plain"
     res, L = (LARGE_RES, LARGE_L) if large else (FILM_RES, FILM_L)
+    if large and args.res:
+        res = tuple(args.res)
+        L = tuple(5e-9 * v for v in res)
     n = int(np.prod(res))
     window = (0.002 if large else 0.05) if args.window is None else args.window
     win = window * 1e-9
@@ -394,7 +399,8 @@ def bench_plain(torch, args, ws, rank, local, dist, hbm, src):
         "metric": "simulated ns/s", "value": sim_ns / (step_ms / 1e3), "unit": "simulated ns/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": ("large-plain: 64x64x8 cubes of 5 nm (n=32768, 25.8 GB FP32 tensor), K=5e3 J/m^3 "
+        "config": {"workload": (f"large-plain: {res[0]}x{res[1]}x{res[2]} cubes of 5 nm (n={n}, "
+                                f"{24 * n * n / 1e9:.2f} GB FP32 tensor), K=5e3 J/m^3 "
                                 "along a seeded axis, 10 mT field, alpha_G=0.1" if large else
                                 "film-plain: 80x20x1 std-problem-4 film (n=1600), single instance") +
                                ", plain FP32 demag, persistent single-instance integrator, tol 1e-6",
