@@ -49,6 +49,13 @@ struct BCtx {
     unsigned char* smem;
     BInst* sinst;           // shared-memory copies of the owned coroutines
     long long tick;
+    // int8 backend, set every tick: active instance tiles, Stream-K units and the
+    // CTAs covering this CTA's tiles (3 components x 2 instance tiles from jb0)
+    int nact;
+    long long U;
+    const int* act_pos;     // [2 IB] position of a 64-instance tile in the active list, -1 if idle
+    int jb0;
+    const SkCover* cov;     // [3][2]
 };
 
 // per-instance vector addressing
@@ -86,6 +93,32 @@ MT_DEV void split_store(float f, int prec, uint16_t* hi_out, uint16_t* lo_out)
         if ([[maybe_unused]] const int _a = _e / (X).nc, _i = (X).c0 + (_e - _a * (X).nc),   \
                       q = _a * (X).P.n + _i; true)
 
+// int8 limbs of one source value: mq = rint(v 2^30) = m0 2^24 + m1 2^16 + m2 2^8 + m3
+// (signed digits, m3 lowest).  |v| must stay below 1.96 so that m0 fits; a value
+// outside records KERR_RANGE and stops the launch.
+constexpr double kI8MScale = 1073741824.0;   // 2^30
+constexpr double kI8MMax = 1.96;
+
+MT_DEV void i8_store_m(double v, int8_t* dst, size_t limb_stride, GridSync* gs)
+{
+    if (!(fabs(v) <= kI8MMax)) {
+        if (atomicCAS(&gs->err, 0, KERR_RANGE) == 0) gs->err_where = 300;
+        atomicExch(&gs->abort, 1);
+        v = 0.0;
+    }
+    long long x = __double2ll_rn(v * kI8MScale);
+    int8_t d[4];
+#pragma unroll
+    for (int l = 3; l >= 1; --l) {
+        const int dl = (int)(signed char)(x & 0xff);
+        d[l] = (int8_t)dl;
+        x = (x - dl) >> 8;
+    }
+    d[0] = (int8_t)x;
+#pragma unroll
+    for (int l = 0; l < 4; ++l) dst[(size_t)l * limb_stride] = d[l];
+}
+
 // write the stage argument (FP64) and the GEMM operand copy for one element
 MT_DEV void put_arg(const BCtx& X, int argi, int b, int q, double v)
 {
@@ -93,7 +126,9 @@ MT_DEV void put_arg(const BCtx& X, int argi, int b, int q, double v)
     const int n = X.P.n;
     const int a = q / n, i = q - a * n;
     const float f = (float)v;
-    if (X.Q.prec == kPrecFP32) {
+    if (X.Q.prec == kPrecI8) {
+        i8_store_m(v, X.F.mlimb + (size_t)b * X.Q.Kd + (size_t)a * X.Q.np + i, (size_t)X.Q.Bp * X.Q.Kd, X.F.gs);
+    } else if (X.Q.prec == kPrecFP32) {
         X.F.m32[((size_t)b * 3 + a) * X.P.ldk + i] = f;
     } else {
         const size_t col = (size_t)b * X.Q.Kd + (size_t)a * X.Q.np + i;
@@ -304,7 +339,7 @@ MT_DEV void advance(BCtx& X, BInst& I, int b)
                     s.phase2 = 1;
                     s.h = fabs(s.h);
                     const double ypnorm = fmax(0.0, I.red[0] < 0.0 ? -1.0 : I.red[0]);
-                    const double tau = pow(s.tol, 0.2);
+                    const double tau = root5(s.tol);
                     if (xmul(s.h, ypnorm) > tau) s.h = tau / ypnorm;
                     I.hmin = fmax(X.Q.sqtiny, xmul(X.Q.toosml, fmax(fabs(s.t_start), fabs(s.t_end))));
                     s.h = xmul(s.dir, fmax(s.h, I.hmin));
@@ -711,16 +746,16 @@ MT_DEV void advance(BCtx& X, BInst& I, int b)
                             else {
                                 s.bad_step_count++;
                                 s.stiff_bad_step_count++;
-                                alpha = I.failed ? 0.5 : fmax(xmul(0.8, pow(s.tol / I.err, 0.2)), 0.5);
+                                alpha = I.failed ? 0.5 : fmax(xmul(0.8, root5(s.tol / I.err)), 0.5);
                             }
                             s.h = xmul(alpha, s.h);
                             I.failed = 1;
                             continue;
                         }
-                        double beta = pow(I.err / s.tol, 0.2);
+                        double beta = root5(I.err / s.tol);
                         if (!s.at_t_start) {
-                            const double t1 = pow(I.err, 0.2) / s.h;
-                            const double t2 = pow(s.errold, 0.2) / s.h_old;
+                            const double t1 = root5(I.err) / s.h;
+                            const double t2 = root5(s.errold) / s.h_old;
                             if (t1 < xmul(t2, 100.0) && t2 < xmul(t1, 100.0)) beta = xmul(beta, t1 / t2);
                         }
                         alpha = 8.0;
@@ -835,26 +870,31 @@ MT_DEV void advance(BCtx& X, BInst& I, int b)
 // LL epilogue for one instance on the owned cells: sum the S partial demag
 // products and write f to the requested destination.
 // ---------------------------------------------------------------------------
-MT_DEV void epilogue(const BCtx& X, BInst& I, int b)
+// exact demag field of cell i, instance b (int8 backend): -Ms_i 2^(-30-e_r) H_int
+MT_DEV void i8_cell_field(const BCtx& X, int b, int i, double hm[3])
 {
-    const int n = X.P.n;
-    const TimeScalars ts = inst_scalars(X, b, I.t_rhs);
-    const double* m = VPOOL(X, I.rhs_arg, b);
-    double* out = dst_ptr(X, I.rhs_dst, b);
-    for (int cell = X.lane; cell < X.nc; cell += 32) {
-        const int i = X.c0 + cell;
-        float S[3];
-        for (int a = 0; a < 3; ++a) {
-            float acc = 0.f;
-            for (int sp = 0; sp < X.Q.S; ++sp)
-                acc += ldcg(&X.F.hpart[(((size_t)sp * X.Q.Bp + b) * 3 + a) * X.Q.np + i]);
-            S[a] = acc;
-        }
-        double o[3];
-        cell_rhs(X.P, m, i, S, ts, o);
-        out[i] = o[0]; out[n + i] = o[1]; out[2 * n + i] = o[2];
+    const double ms = (double)__ldg(&X.P.Mfact[i]);
+    const int jl = b / kI8N - X.jb0;
+    for (int a = 0; a < 3; ++a) {
+        const int r = a * X.Q.np + i;
+        const long long h = i8_tile_sum(X.F.part, X.Q.maxseg, X.cov[a * 2 + jl], r & 127, b % kI8N);
+        hm[a] = xmul(-ms, xmul((double)h, __ldg(&X.Q.row_scale[r])));
     }
-    __syncwarp();
+}
+
+// covers of this CTA's tiles for the current active list (threads 0..5)
+MT_DEV void i8_fill_cover(BCtx& X, SkCover* cov)
+{
+    const int k = threadIdx.x;
+    if (k < 6 && X.nc > 0) {
+        const int a = k / 2, jb = X.jb0 + (k & 1);
+        SkCover cv = {0, -1, 0};
+        if (jb < 2 * X.Q.IB && X.act_pos[jb] >= 0) {
+            const long long t = (long long)X.act_pos[jb] * X.Q.RB + (a * X.Q.np + X.c0) / 128;
+            cv = sk_cover(t, X.Q.nks, X.U);
+        }
+        cov[k] = cv;
+    }
 }
 
 MT_DEV void epilogue_cell(const BCtx& X, int b, double t_rhs, int arg, int dst, int i)
@@ -863,6 +903,13 @@ MT_DEV void epilogue_cell(const BCtx& X, int b, double t_rhs, int arg, int dst, 
     const TimeScalars ts = inst_scalars(X, b, t_rhs);
     const double* m = VPOOL(X, arg, b);
     double* out = dst_ptr(X, dst, b);
+    if (X.Q.prec == kPrecI8) {
+        double hm[3], o[3];
+        i8_cell_field(X, b, i, hm);
+        cell_rhs_h(X.P, m, i, hm, ts, o);
+        out[i] = o[0]; out[n + i] = o[1]; out[2 * n + i] = o[2];
+        return;
+    }
     float S[3];
     for (int a = 0; a < 3; ++a) {
         float acc = 0.f;
@@ -937,9 +984,17 @@ MT_DEV void gemm_tile_simt(const BCtx& X)
             for (int q = 0; q < 4; ++q)
 #pragma unroll
                 for (int r = 0; r < 4; ++r) {
-                    acc[q][r][0] += kv[q][0] * mv[r][0] + kv[q][1] * mv[r][1] + kv[q][2] * mv[r][2];
-                    acc[q][r][1] += kv[q][1] * mv[r][0] + kv[q][3] * mv[r][1] + kv[q][4] * mv[r][2];
-                    acc[q][r][2] += kv[q][2] * mv[r][0] + kv[q][4] * mv[r][1] + kv[q][5] * mv[r][2];
+                    // explicit FMAs: this file is compiled without contraction (the FP64
+                    // coroutine arithmetic must round every operation like the oracle)
+                    acc[q][r][0] = __fmaf_rn(kv[q][0], mv[r][0], acc[q][r][0]);
+                    acc[q][r][0] = __fmaf_rn(kv[q][1], mv[r][1], acc[q][r][0]);
+                    acc[q][r][0] = __fmaf_rn(kv[q][2], mv[r][2], acc[q][r][0]);
+                    acc[q][r][1] = __fmaf_rn(kv[q][1], mv[r][0], acc[q][r][1]);
+                    acc[q][r][1] = __fmaf_rn(kv[q][3], mv[r][1], acc[q][r][1]);
+                    acc[q][r][1] = __fmaf_rn(kv[q][4], mv[r][2], acc[q][r][1]);
+                    acc[q][r][2] = __fmaf_rn(kv[q][2], mv[r][0], acc[q][r][2]);
+                    acc[q][r][2] = __fmaf_rn(kv[q][4], mv[r][1], acc[q][r][2]);
+                    acc[q][r][2] = __fmaf_rn(kv[q][5], mv[r][2], acc[q][r][2]);
                 }
         }
     }
@@ -958,11 +1013,6 @@ MT_DEV void gemm_tile_simt(const BCtx& X)
 
 constexpr int kMaxInstPerWarp = 8;
 
-MT_DEV size_t batch_gemm_smem(int prec)
-{
-    return prec == kPrecFP32 ? (size_t)(6 * kSimtJT * kCellBlock + kSimtJT * 3 * 64) * sizeof(float)
-                             : tc_smem_bytes();
-}
 
 __global__ void __launch_bounds__(kBatchThreads, 1)
 batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMaps maps)
@@ -974,22 +1024,32 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
     X.s = t % Q.S;
     X.ib = (t / Q.S) % Q.IB;
     X.cb = t / (Q.S * Q.IB);
-    X.c0 = X.cb * kCellBlock;
-    X.nc = min(kCellBlock, P.n - X.c0);
+    const bool owner = X.cb < Q.CB;    // CTAs past CB x IB x S only take GEMM work (int8 backend)
+    X.c0 = owner ? X.cb * kCellBlock : 0;
+    X.nc = owner ? min(kCellBlock, P.n - X.c0) : 0;
     const int per = kInstBlock / Q.S;
     X.i0 = X.ib * kInstBlock + X.s * per;
-    X.ni = per;
+    X.ni = owner ? per : 0;
+    X.nact = 0;
+    X.U = 0;
+    __shared__ int s_act[2 * kMaxIB], s_actpos[2 * kMaxIB], s_nact;
+    __shared__ SkCover s_cov[6];
+    X.act_pos = s_actpos;
+    X.jb0 = X.i0 / kI8N;
+    X.cov = s_cov;
     X.n3 = 3 * (size_t)P.n;
     X.lane = threadIdx.x & 31;
     X.warp = threadIdx.x >> 5;
     X.nwarps = blockDim.x >> 5;
     X.smem = smem_raw;
-    const bool tc = Q.prec != kPrecFP32;
+    const bool i8 = Q.prec == kPrecI8;
+    const bool tc = Q.prec != kPrecFP32 && !i8;
     struct ReqDesc { double t; int on, arg, dst, pad; };
     __shared__ ReqDesc s_req[kInstBlock];
     TcState tcs;
     tcs.kb_done = 0; tcs.tiles = 0; tcs.tmem = 0;
     if (tc) tc_init_impl(X.smem, tcs);
+    if (i8) tc_i8_init(X.smem, tcs);
     // each lane keeps its own (identical) copy of the coroutines of its warp
     BInst L[kMaxInstPerWarp];
     int mine = 0;
@@ -1003,9 +1063,20 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
     bool ok = true;
     if (Q.demag_only) {
         // one product of the operands already in place, then H = -Ms * sum of partials
-        if (!tc) gemm_tile_simt(X);
-        else ok = tc_gemm_tile_impl(X.smem, Q, F, maps, X.cb, X.ib, X.s, Q.prec != kPrecBF16x2,
-                                    Q.prec == kPrecFP16x3S, Q.prec == kPrecFP16x3S ? Q.row_inv : nullptr, tcs);
+        if (i8) {
+            const int JB = Q.Bp / kI8N;
+            for (int k = threadIdx.x; k < JB; k += blockDim.x) { s_act[k] = k; s_actpos[k] = k; }
+            __syncthreads();
+            X.nact = JB;
+            X.U = (long long)JB * Q.RB * Q.nks;
+            i8_fill_cover(X, s_cov);
+            ok = tc_i8_streamk(X.smem, F, F.part, Q.maxseg, maps, X.nact, s_act, Q.RB, Q.nks, tcs);
+        } else if (!tc) {
+            gemm_tile_simt(X);
+        } else {
+            ok = tc_gemm_tile_impl(X.smem, Q, F, maps, X.cb, X.ib, X.s, Q.prec != kPrecBF16x2,
+                                   Q.prec == kPrecFP16x3S, Q.prec == kPrecFP16x3S ? Q.row_inv : nullptr, tcs);
+        }
         if (ok && grid_sync(F.gs, 5)) {
             const int n = P.n;
             for (int e = threadIdx.x; e < X.ni * 3 * X.nc; e += blockDim.x) {
@@ -1013,13 +1084,21 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
                 const int a = rem / X.nc, i = X.c0 + (rem - a * X.nc);
                 const int b = X.i0 + li;
                 if (b >= Q.B) continue;
-                float acc = 0.f;
-                for (int sp = 0; sp < Q.S; ++sp)
-                    acc += __ldcg(&F.hpart[(((size_t)sp * Q.Bp + b) * 3 + a) * Q.np + i]);
-                Q.out_h[(size_t)b * 3 * n + (size_t)a * n + i] = (double)__fmul_rn(-acc, __ldg(&P.Mfact[i]));
+                double h;
+                if (i8) {
+                    const int r = a * Q.np + i;
+                    const long long v = i8_tile_sum(F.part, Q.maxseg, s_cov[a * 2 + b / kI8N - X.jb0], r & 127, b % kI8N);
+                    h = xmul(-(double)__ldg(&P.Mfact[i]), xmul((double)v, __ldg(&Q.row_scale[r])));
+                } else {
+                    float acc = 0.f;
+                    for (int sp = 0; sp < Q.S; ++sp)
+                        acc += __ldcg(&F.hpart[(((size_t)sp * Q.Bp + b) * 3 + a) * Q.np + i]);
+                    h = (double)__fmul_rn(-acc, __ldg(&P.Mfact[i]));
+                }
+                Q.out_h[(size_t)b * 3 * n + (size_t)a * n + i] = h;
             }
         }
-        if (tc) tc_finish_impl(X.smem, tcs);
+        if (tc || i8) tc_finish_impl(X.smem, tcs);
         return;
     }
     const bool prof = F.prof != nullptr && threadIdx.x == 0;
@@ -1066,7 +1145,24 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
             for (int k = 0; k < Q.IB; ++k) F.ibreq[((tick + 1) % 3) * Q.IB + k] = 0;
         }
         if (active == 0) break;
-        if (nreq > 0) {
+        if (i8) {
+            // 64-instance tiles of the blocks with requests, in order; every CTA builds the same list
+            if (threadIdx.x == 0) {
+                int na = 0;
+                for (int k = 0; k < 2 * Q.IB; ++k) {
+                    const bool on = __ldcg(&F.ibreq[(tick % 3) * Q.IB + k / 2]) > 0;
+                    s_actpos[k] = on ? na : -1;
+                    if (on) s_act[na++] = k;
+                }
+                s_nact = na;
+            }
+            __syncthreads();
+            X.nact = s_nact;
+            X.U = (long long)X.nact * Q.RB * Q.nks;
+            i8_fill_cover(X, s_cov);   // read in P1, after the barriers that follow the GEMM
+            if (X.nact > 0 && !tc_i8_streamk(X.smem, F, F.part, Q.maxseg, maps, X.nact, s_act, Q.RB, Q.nks, tcs))
+                ok = false;
+        } else if (nreq > 0) {
             if (!tc) gemm_tile_simt(X);
             else if (!tc_gemm_tile_impl(X.smem, Q, F, maps, X.cb, X.ib, X.s, Q.prec != kPrecBF16x2,
                                         Q.prec == kPrecFP16x3S, Q.prec == kPrecFP16x3S ? Q.row_inv : nullptr, tcs))
@@ -1122,7 +1218,7 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
         }
     }
 #undef PROF_MARK
-    if (tc) tc_finish_impl(X.smem, tcs);
+    if (tc || i8) tc_finish_impl(X.smem, tcs);
     if (ok && X.lane == 0) {
         for (int k = 0; k < mine; ++k) {
             const int li = X.warp + k * X.nwarps;
@@ -1177,9 +1273,62 @@ __global__ void split_tensor_kernel(const float* __restrict__ K, int n, int ldk,
     }
 }
 
+// int8 tensor rows: 2^e_r puts the largest |K| of row r into [2^21, 2^22);
+// row_scale[r] = 2^(-30 - e_r) converts the exact limb sum back (0 for empty rows)
+__global__ void i8_row_kernel(const float* __restrict__ K, int n, int ldk, int np, int* __restrict__ row_exp,
+                              double* __restrict__ row_scale)
+{
+    const int row = blockIdx.x;
+    const int a = row / np, i = row - a * np;
+    static const int blk[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    float mx = 0.f;
+    if (i < n)
+        for (int bb = 0; bb < 3; ++bb)
+            for (int j = threadIdx.x; j < n; j += blockDim.x)
+                mx = fmaxf(mx, fabsf(K[((size_t)i * 6 + blk[a][bb]) * ldk + j]));
+    __shared__ float red[32];
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float m = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, red[w]);
+        int e = 0;
+        if (m > 0.f) frexpf(m, &e);                // m = f 2^e, f in [0.5, 1)
+        const int ex = (m > 0.f) ? 22 - e : 0;     // m 2^ex in [2^21, 2^22)
+        row_exp[row] = ex;
+        row_scale[row] = (m > 0.f) ? ldexp(1.0, -30 - ex) : 0.0;
+    }
+}
+
+// FP32 cell-row tensor -> three int8 limbs [3][3np][Kd] of Kq = rint(K 2^e_r),
+// Kq = k0 2^16 + k1 2^8 + k2 (signed digits, k2 lowest), zero padded
+__global__ void i8_limb_kernel(const float* __restrict__ K, int n, int ldk, int np, const int* __restrict__ row_exp,
+                               int8_t* __restrict__ klimb)
+{
+    const int Kd = 3 * np;
+    const size_t tot = (size_t)Kd * Kd;
+    static const int blk[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
+        const int row = (int)(e / Kd), col = (int)(e - (size_t)row * Kd);
+        const int a = row / np, i = row - a * np, bb = col / np, j = col - bb * np;
+        float v = 0.f;
+        if (i < n && j < n) v = K[((size_t)i * 6 + blk[a][bb]) * ldk + j];
+        long long x = __double2ll_rn(ldexp((double)v, row_exp[row]));
+        const int k2 = (int)(signed char)(x & 0xff);
+        x = (x - k2) >> 8;
+        const int k1 = (int)(signed char)(x & 0xff);
+        x = (x - k1) >> 8;
+        klimb[e] = (int8_t)x;
+        klimb[tot + e] = (int8_t)k1;
+        klimb[2 * tot + e] = (int8_t)k2;
+    }
+}
+
 // m (B x 3n FP64) -> GEMM operand of every instance
 __global__ void batch_operand_kernel(const double* __restrict__ m, int B, int n, int ldk, int np, int prec,
-                                     float* __restrict__ m32, uint16_t* __restrict__ mhi, uint16_t* __restrict__ mlo)
+                                     float* __restrict__ m32, uint16_t* __restrict__ mhi, uint16_t* __restrict__ mlo,
+                                     int8_t* __restrict__ mlimb, int Bp, GridSync* gs)
 {
     const size_t tot = (size_t)B * 3 * n;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < tot; e += (size_t)gridDim.x * blockDim.x) {
@@ -1187,7 +1336,9 @@ __global__ void batch_operand_kernel(const double* __restrict__ m, int B, int n,
         const int q = (int)(e - (size_t)b * 3 * n);
         const int a = q / n, i = q - a * n;
         const float f = (float)m[e];
-        if (prec == kPrecFP32) {
+        if (prec == kPrecI8) {
+            i8_store_m(m[e], mlimb + (size_t)b * 3 * np + (size_t)a * np + i, (size_t)Bp * 3 * np, gs);
+        } else if (prec == kPrecFP32) {
             m32[((size_t)b * 3 + a) * ldk + i] = f;
         } else {
             const size_t col = (size_t)b * 3 * np + (size_t)a * np + i;
@@ -1201,10 +1352,35 @@ __global__ void batch_operand_kernel(const double* __restrict__ m, int B, int n,
 static void bs45b_fill(BS45b& T);
 
 cudaError_t launch_batch_operand(const double* m, int B, int n, int ldk, int np, int prec, float* m32, uint16_t* mhi,
-                                 uint16_t* mlo, cudaStream_t s)
+                                 uint16_t* mlo, int8_t* mlimb, int Bp, GridSync* gs, cudaStream_t s)
 {
-    batch_operand_kernel<<<592, 256, 0, s>>>(m, B, n, ldk, np, prec, m32, mhi, mlo);
+    batch_operand_kernel<<<592, 256, 0, s>>>(m, B, n, ldk, np, prec, m32, mhi, mlo, mlimb, Bp, gs);
     return cudaGetLastError();
+}
+
+cudaError_t launch_limb_tensor(const float* K, int n, int ldk, int np, int8_t* klimb, double* row_scale,
+                               cudaStream_t s)
+{
+    int* row_exp = nullptr;
+    cudaError_t e = cudaMallocAsync(&row_exp, sizeof(int) * 3 * (size_t)np, s);
+    if (e != cudaSuccess) return e;
+    i8_row_kernel<<<3 * np, 256, 0, s>>>(K, n, ldk, np, row_exp, row_scale);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        i8_limb_kernel<<<1184, 256, 0, s>>>(K, n, ldk, np, row_exp, klimb);
+        e = cudaGetLastError();
+    }
+    cudaError_t e2 = cudaFreeAsync(row_exp, s);
+    return e != cudaSuccess ? e : e2;
+}
+
+// slots per CTA: the longest Stream-K range (all instance tiles active) spans
+// at most ceil(len / nks) + 1 tiles
+int batch_i8_maxseg(int RB, int nks, int JB, int G)
+{
+    const long long U = (long long)RB * nks * JB;
+    const long long len = (U + G - 1) / G;
+    return (int)((len + nks - 1) / nks) + 1;
 }
 
 cudaError_t batch_upload_tables()
@@ -1216,7 +1392,6 @@ cudaError_t batch_upload_tables()
 
 int batch_grid(int n, int B, int num_sms, int prec, int* CB, int* IB, int* S)
 {
-    (void)prec;
     *CB = (n + kCellBlock - 1) / kCellBlock;
     *IB = (B + kInstBlock - 1) / kInstBlock;
     const int tiles = (*CB) * (*IB);
@@ -1227,12 +1402,15 @@ int batch_grid(int n, int B, int num_sms, int prec, int* CB, int* IB, int* S)
     const int Kd = 3 * (*CB) * kCellBlock;
     while (s > 1 && (Kd % (32 * s)) != 0) --s;
     *S = s;
+    // int8: the coroutine owners as above, the Stream-K GEMM on every SM
+    if (prec == kPrecI8 && tiles * s < num_sms) return num_sms;
     return tiles * s;
 }
 
 size_t batch_smem_bytes(int n, int ldk, int prec)
 {
     (void)n; (void)ldk;
+    if (prec == kPrecI8) return tc_i8_smem_bytes();
     return prec == kPrecFP32 ? (size_t)(6 * kSimtJT * kCellBlock + kSimtJT * 3 * 64) * sizeof(float)
                              : tc_smem_bytes();
 }

@@ -11,7 +11,8 @@ constexpr int kCellBlock = 128;   // receiver cells per tile (tcgen05 M = 128)
 constexpr int kInstBlock = 128;   // instances per tile (tcgen05 N = 128)
 constexpr int kRedSlots = 4;      // values per reduction
 
-enum BatchPrecision { kPrecFP32 = 0, kPrecBF16x3 = 1, kPrecBF16x2 = 2, kPrecFP16x3S = 3 };
+enum BatchPrecision { kPrecFP32 = 0, kPrecBF16x3 = 1, kPrecBF16x2 = 2, kPrecFP16x3S = 3, kPrecI8 = 4 };
+constexpr int kMaxIB = 64;        // instance blocks (B <= 8192)
 
 // Per-instance coroutine state: RKSUITE scalars plus the resume point and the
 // locals that live across a yield.  One private copy per owning CTA.
@@ -50,7 +51,9 @@ struct BatchBufs {
     float* m32;        // [Bp][3][ldk] FP32 argument (fp32 backend)
     uint16_t* mhi;     // [Bp][Kd] BF16 argument, K-major (tcgen05 backends)
     uint16_t* mlo;
+    int8_t* mlimb;     // [4][Bp][Kd] int8 limbs of the argument (int8 backend)
     float* hpart;      // [S][Bp][3][np] partial demag sums
+    long long* part;   // [G][maxseg][64][128] exact int64 segment sums (int8 backend)
     double* partials;  // [Bp][kRedSlots][CB] reduction partials
     BInst* inst;       // [CB][Bp] private coroutine copies
     GridSync* gs;
@@ -77,6 +80,9 @@ struct BatchParams {
     const uint16_t* khi;      // [3np][Kd] BF16 tensor (rows (a,i), cols (b,j))
     const uint16_t* klo;
     const float* row_inv;     // [3np] 1/s_r of the fp16s tensor rows
+    // int8 backend: Stream-K geometry and the per-row scale 2^(-30 - e_r)
+    int RB, nks, maxseg;
+    const double* row_scale;  // [3np]
 };
 
 cudaError_t batch_upload_tables();
@@ -87,4 +93,7 @@ cudaError_t launch_batch(const DevProb& P, const BatchBufs& Bf, const BatchParam
 cudaError_t launch_split_tensor(const float* K, int n, int ldk, int np, int prec, uint16_t* khi, uint16_t* klo,
                                 float* row_inv, cudaStream_t s);
 cudaError_t launch_batch_operand(const double* m, int B, int n, int ldk, int np, int prec, float* m32, uint16_t* mhi,
-                                 uint16_t* mlo, cudaStream_t s);
+                                 uint16_t* mlo, int8_t* mlimb, int Bp, GridSync* gs, cudaStream_t s);
+cudaError_t launch_limb_tensor(const float* K, int n, int ldk, int np, int8_t* klimb, double* row_scale,
+                               cudaStream_t s);
+int batch_i8_maxseg(int RB, int nks, int JB, int G);

@@ -510,6 +510,8 @@ struct mt_batch {
     uint16_t* khi = nullptr;
     uint16_t* klo = nullptr;
     float* row_inv = nullptr;
+    int8_t* klimb = nullptr;      // int8 backend: [3][3np][Kd]
+    double* row_scale = nullptr;  // [3np]
     double* hext = nullptr;
     double* alpha0 = nullptr;
     int nt_hext = 0;
@@ -548,6 +550,22 @@ int make_tmap(CUtensorMap* m, const void* base, uint64_t inner, uint64_t outer, 
     return MT_OK;
 }
 
+// 3-D int8 tensor [limbs][outer][inner] (inner contiguous), box {64, box_outer, 1}, 64-byte swizzle
+int make_tmap_i8(CUtensorMap* m, const void* base, uint64_t inner, uint64_t outer, uint64_t limbs, uint32_t box_outer)
+{
+    int rc = get_encoder();
+    if (rc) return rc;
+    cuuint64_t dims[3] = {inner, outer, limbs};
+    cuuint64_t strides[2] = {inner, inner * outer};
+    cuuint32_t box[3] = {(cuuint32_t)kI8KB, box_outer, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, es,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(MT_ERR_CUDA, "cuTensorMapEncodeTiled (int8) failed (%d)", (int)r);
+    return MT_OK;
+}
+
 DevProb batch_prob(const mt_batch* bt)
 {
     DevProb P = make_prob(bt->h);
@@ -563,7 +581,7 @@ int mt_batch_create(const mt_grid* g, int B, int precision, mt_batch** out)
     if (!out) return fail(MT_ERR_ARG, "null argument");
     *out = nullptr;
     if (B < 1) return fail(MT_ERR_ARG, "B must be >= 1");
-    if (precision < 0 || precision > 3) return fail(MT_ERR_ARG, "unknown precision %d", precision);
+    if (precision < 0 || precision > 4) return fail(MT_ERR_ARG, "unknown precision %d", precision);
     mt_handle* h = nullptr;
     int rc = mt_create(g, &h);
     if (rc) return rc;
@@ -576,6 +594,11 @@ int mt_batch_create(const mt_grid* g, int B, int precision, mt_batch** out)
     bt->grid = batch_grid(h->n, B, h->num_sms, precision, &bt->CB, &bt->IB, &bt->S);
     bt->np = bt->CB * kCellBlock;
     bt->Kd = 3 * bt->np;
+    if (precision == MT_PREC_INT8 && bt->Kd > 43000) {
+        // D_s sums up to three limb products of magnitude <= 2^14 over the k range in int32
+        mt_batch_destroy(bt);
+        return fail(MT_ERR_UNSUPPORTED, "int8 precision supports up to 14336 cells");
+    }
     *out = bt;
     return MT_OK;
 }
@@ -584,6 +607,7 @@ int mt_batch_destroy(mt_batch* bt)
 {
     if (!bt) return MT_OK;
     free_ptr(bt->khi); free_ptr(bt->row_inv); free_ptr(bt->hext); free_ptr(bt->alpha0);
+    free_ptr(bt->klimb); free_ptr(bt->row_scale);
     mt_destroy(bt->h);
     delete bt;
     return MT_OK;
@@ -624,7 +648,15 @@ int mt_batch_assemble_demag(mt_batch* bt, void* stream)
     if (!bt) return fail(MT_ERR_ARG, "null handle");
     int rc = mt_assemble_demag(bt->h, stream);
     if (rc) return rc;
-    if (bt->prec != MT_PREC_FP32) {
+    if (bt->prec == MT_PREC_INT8) {
+        const size_t cnt = (size_t)bt->Kd * bt->Kd;
+        if (!bt->klimb) {
+            CUDA_TRY(dalloc(&bt->klimb, 3 * cnt));
+            CUDA_TRY(dalloc(&bt->row_scale, (size_t)bt->Kd));
+        }
+        CUDA_TRY(launch_limb_tensor(bt->h->K, bt->h->n, bt->h->ldk, bt->np, bt->klimb, bt->row_scale,
+                                    (cudaStream_t)stream));
+    } else if (bt->prec != MT_PREC_FP32) {
         const size_t cnt = (size_t)bt->Kd * bt->Kd;
         if (!bt->khi) {
             CUDA_TRY(dalloc(&bt->khi, 2 * cnt));   // hi and lo contiguous: one L2 persistence window
@@ -674,13 +706,21 @@ int batch_alloc(mt_batch* bt, BatchRun& R, int nt, cudaStream_t s)
     if (bt->prec == MT_PREC_FP32) {
         CUDA_TRY(R.A.get(&F.m32, (size_t)Bp * 3 * h->ldk));
         CUDA_TRY(cudaMemsetAsync(F.m32, 0, sizeof(float) * Bp * 3 * (size_t)h->ldk, s));
+    } else if (bt->prec == MT_PREC_INT8) {
+        CUDA_TRY(R.A.get(&F.mlimb, 4 * (size_t)Bp * bt->Kd));
+        CUDA_TRY(cudaMemsetAsync(F.mlimb, 0, 4 * (size_t)Bp * bt->Kd, s));
     } else {
         CUDA_TRY(R.A.get(&F.mhi, (size_t)Bp * bt->Kd));
         CUDA_TRY(R.A.get(&F.mlo, (size_t)Bp * bt->Kd));
         CUDA_TRY(cudaMemsetAsync(F.mhi, 0, 2 * (size_t)Bp * bt->Kd, s));
         CUDA_TRY(cudaMemsetAsync(F.mlo, 0, 2 * (size_t)Bp * bt->Kd, s));
     }
-    CUDA_TRY(R.A.get(&F.hpart, (size_t)bt->S * Bp * 3 * bt->np));
+    const int RB = bt->Kd / 128, nks = bt->Kd / kI8KB;
+    const int maxseg = bt->prec == MT_PREC_INT8 ? batch_i8_maxseg(RB, nks, Bp / kI8N, bt->grid) : 0;
+    if (bt->prec == MT_PREC_INT8)
+        CUDA_TRY(R.A.get(&F.part, (size_t)bt->grid * maxseg * kI8SlotElems));
+    else
+        CUDA_TRY(R.A.get(&F.hpart, (size_t)bt->S * Bp * 3 * bt->np));
     CUDA_TRY(R.A.get(&F.partials, (size_t)Bp * kRedSlots * bt->CB));
     CUDA_TRY(R.A.get(&F.inst, (size_t)bt->CB * Bp));
     CUDA_TRY(R.A.get(&F.gs, 1));
@@ -699,9 +739,14 @@ int batch_alloc(mt_batch* bt, BatchRun& R, int nt, cudaStream_t s)
     Q.Bp = Bp; Q.B = bt->B; Q.CB = bt->CB; Q.IB = bt->IB; Q.S = bt->S; Q.np = bt->np; Q.Kd = bt->Kd;
     Q.nt = nt; Q.nt_hext = bt->nt_hext; Q.prec = bt->prec;
     Q.khi = bt->khi; Q.klo = bt->klo; Q.row_inv = bt->row_inv;
+    Q.RB = RB; Q.nks = nks; Q.maxseg = maxseg; Q.row_scale = bt->row_scale;
     Q.renorm = h->renorm;
     memset(&R.maps, 0, sizeof(R.maps));
-    if (bt->prec != MT_PREC_FP32) {
+    if (bt->prec == MT_PREC_INT8) {
+        int rc;
+        if ((rc = make_tmap_i8(&R.maps.ahi, bt->klimb, bt->Kd, bt->Kd, 3, 128))) return rc;
+        if ((rc = make_tmap_i8(&R.maps.bhi, F.mlimb, bt->Kd, Bp, 4, kI8N))) return rc;
+    } else if (bt->prec != MT_PREC_FP32) {
         int rc;
         if ((rc = make_tmap(&R.maps.ahi, bt->khi, bt->Kd, bt->Kd, 128))) return rc;
         if ((rc = make_tmap(&R.maps.alo, bt->klo, bt->Kd, bt->Kd, 128))) return rc;
@@ -720,19 +765,21 @@ int mt_batch_demag_field(mt_batch* bt, const double* m_dev, double* H_dev, void*
     if (!bt || !m_dev || !H_dev) return fail(MT_ERR_ARG, "bad argument");
     int rc = check_ready(bt->h, true, false);
     if (rc) return rc;
-    if (bt->prec != MT_PREC_FP32 && !bt->khi) return fail(MT_ERR_STATE, "call mt_batch_assemble_demag first");
+    if (bt->prec != MT_PREC_FP32 && !bt->khi && !bt->klimb) return fail(MT_ERR_STATE, "call mt_batch_assemble_demag first");
     cudaStream_t s = (cudaStream_t)stream;
     BatchRun R;
     if ((rc = batch_alloc(bt, R, 0, s))) return rc;
     R.Q.demag_only = 1;
     R.Q.out_h = H_dev;
-    CUDA_TRY(launch_batch_operand(m_dev, bt->B, bt->h->n, bt->h->ldk, bt->np, bt->prec, R.F.m32, R.F.mhi, R.F.mlo, s));
     CUDA_TRY(cudaMemsetAsync(R.F.gs, 0, sizeof(GridSync), s));
+    CUDA_TRY(launch_batch_operand(m_dev, bt->B, bt->h->n, bt->h->ldk, bt->np, bt->prec, R.F.m32, R.F.mhi, R.F.mlo,
+                                  R.F.mlimb, R.Q.Bp, R.F.gs, s));
     DevProb P = batch_prob(bt);
     CUDA_TRY(launch_batch(P, R.F, R.Q, bt->grid, bt->prec != MT_PREC_FP32 ? &R.maps : nullptr, s));
     GridSync gs_h;
     CUDA_TRY(cudaMemcpyAsync(&gs_h, R.F.gs, sizeof(gs_h), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
+    if (gs_h.err == KERR_RANGE) return fail(MT_ERR_ARG, "int8 precision: a component of m is outside (-1.96, 1.96)");
     if (gs_h.err || gs_h.abort) return fail(MT_ERR_TIMEOUT, "batch demag: bounded wait gave up (at %d)", gs_h.err_where);
     return MT_OK;
 }
@@ -745,7 +792,7 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
     int rc = check_ready(bt->h, true, false);
     if (rc) return rc;
     if (!bt->have_dynamics) return fail(MT_ERR_STATE, "call mt_batch_set_dynamics first");
-    if (bt->prec != MT_PREC_FP32 && !bt->khi) return fail(MT_ERR_STATE, "call mt_batch_assemble_demag first");
+    if (bt->prec != MT_PREC_FP32 && !bt->khi && !bt->klimb) return fail(MT_ERR_STATE, "call mt_batch_assemble_demag first");
     if (!t || nt < 2 || !m0_dev || !t_out || !flags || !stats) return fail(MT_ERR_ARG, "bad argument (nt >= 2 required)");
     if (nt_conv < 0 || (nt_conv > 0 && !t_conv)) return fail(MT_ERR_ARG, "bad convergence-time list");
     cudaStream_t s = (cudaStream_t)stream;
@@ -837,7 +884,7 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
         int max_persist = 0, max_win = 0;
         cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, h->device);
         cudaDeviceGetAttribute(&max_win, cudaDevAttrMaxAccessPolicyWindowSize, h->device);
-        const size_t want = 2 * (size_t)bt->Kd * bt->Kd * sizeof(uint16_t);
+        const size_t want = (bt->prec == MT_PREC_INT8 ? 3 : 4) * (size_t)bt->Kd * bt->Kd;
         if (max_persist > 0 && max_win > 0 && cudaDeviceGetLimit(&prev_limit, cudaLimitPersistingL2CacheSize) == cudaSuccess) {
             const size_t lim = std::min(want, (size_t)max_persist);
             if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, lim) == cudaSuccess) {
@@ -859,7 +906,9 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
         CUDA_TRY(cudaMemsetAsync(F.ibreq, 0, sizeof(unsigned) * 3 * bt->IB, s));
         CUDA_TRY(cudaEventRecord(ev0, s));
         CUDA_TRY(launch_batch(P, F, Q, bt->grid, bt->prec != MT_PREC_FP32 ? &R.maps : nullptr, s,
-                              l2_bytes ? bt->khi : nullptr, l2_bytes, l2_hit));
+                              l2_bytes ? (bt->prec == MT_PREC_INT8 ? (const void*)bt->klimb : (const void*)bt->khi)
+                                       : nullptr,
+                              l2_bytes, l2_hit));
         CUDA_TRY(cudaEventRecord(ev1, s));
         GridSync gs_h;
         CUDA_TRY(cudaMemcpyAsync(&gs_h, F.gs, sizeof(gs_h), cudaMemcpyDeviceToHost, s));
@@ -869,6 +918,8 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
         CUDA_TRY(cudaEventElapsedTime(&ms, ev0, ev1));
         kernel_ms += ms;
         launches++;
+        if (gs_h.err == KERR_RANGE)
+            return fail(MT_ERR_ARG, "int8 precision: a component of m left (-1.96, 1.96)");
         if (gs_h.err != 0 || gs_h.abort)
             return fail(MT_ERR_TIMEOUT, "batch integrator: bounded wait gave up (code %d at %d)", gs_h.err, gs_h.err_where);
         bool all_done = true;

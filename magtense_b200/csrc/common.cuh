@@ -7,7 +7,7 @@
 #define MT_DEV __device__ __forceinline__
 
 // Error codes recorded by kernels in GridSync::err (host maps them to MT_ERR_*).
-enum { KERR_NONE = 0, KERR_BARRIER_TIMEOUT = 1, KERR_BAD_CONFIG = 2 };
+enum { KERR_NONE = 0, KERR_BARRIER_TIMEOUT = 1, KERR_BAD_CONFIG = 2, KERR_RANGE = 3 };
 
 // Grid-wide barrier state for the persistent cooperative kernels.  count is
 // reset to 0 by the host before every launch.
@@ -120,6 +120,28 @@ MT_DEV double block_reduce(double v, double* scratch)
 MT_DEV double xmul(double a, double b) { return __dmul_rn(a, b); }
 MT_DEV double xadd(double a, double b) { return __dadd_rn(a, b); }
 MT_DEV double xsub(double a, double b) { return __dsub_rn(a, b); }
+
+// x^(1/5) for the RKSUITE step-size control, from IEEE operations only (so the
+// host oracle, which runs the same iteration, rounds identically): x = f 2^e,
+// e = 5 q + r, y = f 2^r in [0.5, 16), twelve Newton steps z <- z + (y / z^4 - z) / 5
+// from z = 1 (y < 2) or 1.5, then 2^q z.  Agrees with pow(x, 0.2) to a few ulp
+// (pow's exponent 0.2 is itself 1/5 + 1.1e-17).
+MT_DEV double root5(double x)
+{
+    if (!(x > 0.0)) return 0.0;
+    if (isinf(x)) return x;
+    int e = 0;
+    const double f = frexp(x, &e);
+    const int q = (e >= 0) ? e / 5 : -((-e + 4) / 5);
+    const double y = ldexp(f, e - 5 * q);
+    double z = (y < 2.0) ? 1.0 : 1.5;
+    for (int k = 0; k < 12; ++k) {
+        const double z2 = __dmul_rn(z, z);
+        const double z4 = __dmul_rn(z2, z2);
+        z = __dadd_rn(z, __ddiv_rn(__dsub_rn(__ddiv_rn(y, z4), z), 5.0));
+    }
+    return ldexp(z, q);
+}
 
 MT_DEV double ldcg(const double* p) { return __ldcg(p); }
 MT_DEV float ldcg(const float* p) { return __ldcg(p); }

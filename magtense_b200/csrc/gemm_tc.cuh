@@ -287,3 +287,280 @@ MT_DEV bool tc_gemm_tile_impl(unsigned char* smem, const QT& Q, const FT& F, con
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     return __syncthreads_and(ok ? 1 : 0) != 0;
 }
+
+// ---------------------------------------------------------------------------
+// Exact fixed-point demag product on the integer tensor pipe (kind::i8).
+//
+// Tensor row r (component a, cell i; 3np rows) is scaled by 2^e_r so that its
+// largest entry lies in [2^21, 2^22) and rounded to an integer Kq (|Kq| < 2^22),
+// written as three signed 8-bit limbs Kq = k0 2^16 + k1 2^8 + k2.  Every source
+// value m_j (|m_j| < 1.96) is rounded to mq = rint(m_j 2^30) and written as four
+// limbs mq = m0 2^24 + m1 2^16 + m2 2^8 + m3.  All twelve limb products are
+// accumulated exactly in int32 TMEM accumulators grouped by s = a + b (D_s,
+// columns 64 s .. 64 s + 63) and combined in int64 as
+// H = sum_s 2^(8 (5 - s)) D_s = sum_j Kq_rj mq_j, exactly: the sum over sources
+// carries no rounding, does not depend on the order or split of the k range,
+// and the field 2^(-30 - e_r) H is the same bit pattern on every run.
+//
+// Work split (Stream-K): tile = 128 tensor rows x 64 instances, unit = one
+// 64-wide k step of a tile; the units of all active tiles are split into
+// contiguous non-empty ranges, one per CTA, so every SM gets the same number of
+// MMAs.  A CTA's range covers pieces ("segments") of one or more tiles; each
+// segment's exact int64 partial goes to its own slot [CTA][segment][inst][row],
+// and the reader sums the slots of the CTAs that cover the tile.
+// ---------------------------------------------------------------------------
+constexpr int kI8Stages = 4;
+constexpr int kI8KB = 64;                                    // int8 sources per stage (64-byte rows)
+constexpr int kI8N = 64;                                     // instances per tile (MMA N)
+constexpr int kI8ATile = 128 * kI8KB;                        // one 128-row K limb tile, 8 KB
+constexpr int kI8BTile = kI8N * kI8KB;                       // one 64-row m limb tile, 4 KB
+constexpr int kI8KLimbs = 3, kI8MLimbs = 4, kI8Acc = 6;
+constexpr int kI8StageBytes = kI8KLimbs * kI8ATile + kI8MLimbs * kI8BTile;   // 40 KB
+constexpr int kI8SlotElems = kI8N * 128;                     // int64 per segment slot
+// D S32 (2 at bit 4), A and B signed 8-bit (1 at bits 7 and 10), N = 64, M = 128
+constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | (((uint32_t)kI8N >> 3) << 17) | ((128u >> 4) << 24);
+
+static inline size_t tc_i8_smem_bytes() { return 1024 + (size_t)kI8Stages * kI8StageBytes + 256; }
+
+struct I8Smem {
+    uint8_t* stages;
+    uint64_t* full;      // kI8Stages
+    uint64_t* empty;     // kI8Stages
+    uint64_t* accum;     // segment accumulators complete
+    uint64_t* tfree;     // segment accumulators drained (4 epilogue warps)
+    uint32_t* tmem_slot;
+};
+
+MT_DEV I8Smem i8_layout(unsigned char* smem)
+{
+    I8Smem L;
+    const uint32_t base = smem_u32(smem);
+    const uint32_t pad = (1024u - (base & 1023u)) & 1023u;
+    L.stages = smem + pad;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(L.stages + (size_t)kI8Stages * kI8StageBytes);
+    L.full = bars;
+    L.empty = bars + kI8Stages;
+    L.accum = bars + 2 * kI8Stages;
+    L.tfree = bars + 2 * kI8Stages + 1;
+    L.tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kI8Stages + 2);
+    return L;
+}
+
+MT_DEV void tc_i8_init(unsigned char* smem, TcState& st)
+{
+    I8Smem L = i8_layout(smem);
+    const int warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < kI8Stages; ++k) {
+            mbar_init(smem_u32(&L.full[k]), 1);
+            mbar_init(smem_u32(&L.empty[k]), 1);
+        }
+        mbar_init(smem_u32(L.accum), 1);
+        mbar_init(smem_u32(L.tfree), 4);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(L.tmem_slot)),
+                     "r"(kTcTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    st.tmem = *reinterpret_cast<volatile uint32_t*>(L.tmem_slot);
+    st.kb_done = 0;
+    st.tiles = 0;
+}
+
+MT_DEV void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(bar)
+        : "memory");
+}
+
+MT_DEV void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
+{
+    asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                 " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
+                 "l"(adesc), "l"(bdesc), "r"(kIdescI8), "r"(accumulate)
+                 : "memory");
+}
+
+MT_DEV void tmem_ld32_i(uint32_t taddr, int (&v)[32])
+{
+    float f[32];
+    tmem_ld32(taddr, f);
+#pragma unroll
+    for (int k = 0; k < 32; ++k) v[k] = __float_as_int(f[k]);
+}
+
+MT_DEV void mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Stream-K over U units on G = min(gridDim.x, U) CTAs (every range non-empty):
+// CTA c owns units [sk_start(c), sk_start(c + 1))
+MT_DEV long long sk_ctas(long long U) { return U < (long long)gridDim.x ? U : (long long)gridDim.x; }
+MT_DEV long long sk_start(long long c, long long U, long long G) { return c * U / G; }
+
+// The CTAs whose ranges touch tile t (units [t nks, (t+1) nks)) are first..last;
+// the tile is the jf-th segment of CTA first and the first segment (slot 0) of
+// every later one, because their ranges start inside it.
+struct SkCover { int first, last, jf; };
+
+MT_DEV SkCover sk_cover(long long t, long long nks, long long U)
+{
+    const long long G = sk_ctas(U);
+    const long long x0 = t * nks, x1 = (t + 1) * nks;
+    long long f = ((x0 + 1) * G + U - 1) / U - 1;
+    long long l = (x1 * G + U - 1) / U - 1;
+    if (f > G - 1) f = G - 1;
+    if (l > G - 1) l = G - 1;
+    if (f < 0) f = 0;
+    SkCover cv;
+    cv.first = (int)f;
+    cv.last = (int)l;
+    cv.jf = (int)(t - sk_start(f, U, G) / nks);
+    return cv;
+}
+
+// The Stream-K share of this CTA in one tick: nact active instance tiles
+// (act_jb[0..nact), 64 instances each), RB row blocks, nks k steps per tile.
+// part: int64 slots [gridDim.x][maxseg][64][128].  Returns a CTA-uniform ok flag.
+template <typename FT>
+MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int maxseg, const TcMaps& maps,
+                          int nact, const int* act_jb, int RB, int nks, TcState& st)
+{
+    I8Smem L = i8_layout(smem);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long U = (long long)nact * RB * nks;
+    const long long G = sk_ctas(U), c = blockIdx.x;
+    bool ok = true;
+    if (c >= G) return __syncthreads_and(1) != 0;
+    const long long u0 = sk_start(c, U, G), u1 = sk_start(c + 1, U, G);
+    if (warp == 4 && lane == 0) {
+        long long g = st.kb_done;
+        for (long long u = u0; u < u1 && ok;) {
+            const int t = (int)(u / nks), ks0 = (int)(u - (long long)t * nks);
+            const long long ue = min(u1, (long long)(t + 1) * nks);
+            const int rb = t % RB, jb = act_jb[t / RB];
+            for (int ks = ks0; ks < ks0 + (int)(ue - u); ++ks, ++g) {
+                const int stg = (int)(g % kI8Stages);
+                const uint32_t ph = (uint32_t)((g / kI8Stages) & 1);
+                if (!mbar_wait(smem_u32(&L.empty[stg]), ph ^ 1u, F.gs, 210)) { ok = false; break; }
+                uint8_t* base = L.stages + (size_t)stg * kI8StageBytes;
+                const uint32_t fb = smem_u32(&L.full[stg]);
+                mbar_expect_tx(fb, (uint32_t)kI8StageBytes);
+                const int x = ks * kI8KB;
+                for (int a = 0; a < kI8KLimbs; ++a)
+                    tma_load_3d(smem_u32(base + a * kI8ATile), &maps.ahi, x, rb * 128, a, fb);
+                for (int b = 0; b < kI8MLimbs; ++b)
+                    tma_load_3d(smem_u32(base + kI8KLimbs * kI8ATile + b * kI8BTile), &maps.bhi, x, jb * kI8N, b, fb);
+            }
+            u = ue;
+        }
+        if (!ok) {   // let loads already in flight land before the CTA moves on
+            for (long long q = g - kI8Stages; q < g; ++q) {
+                if (q < st.kb_done) continue;
+                mbar_wait(smem_u32(&L.full[q % kI8Stages]), (uint32_t)((q / kI8Stages) & 1), F.gs, 213);
+            }
+        }
+    } else if (warp == 5 && lane == 0) {
+        long long g = st.kb_done, seg = st.tiles;
+        for (long long u = u0; u < u1 && ok; ++seg) {
+            const int t = (int)(u / nks), ks0 = (int)(u - (long long)t * nks);
+            const long long ue = min(u1, (long long)(t + 1) * nks);
+            // the accumulators of the previous segment must be drained first
+            if (seg > 0 && !mbar_wait(smem_u32(L.tfree), (uint32_t)((seg - 1) & 1), F.gs, 214)) { ok = false; break; }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            for (int ks = ks0; ks < ks0 + (int)(ue - u); ++ks, ++g) {
+                const int stg = (int)(g % kI8Stages);
+                const uint32_t ph = (uint32_t)((g / kI8Stages) & 1);
+                if (!mbar_wait(smem_u32(&L.full[stg]), ph, F.gs, 211)) { ok = false; break; }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t base = smem_u32(L.stages + (size_t)stg * kI8StageBytes);
+#pragma unroll
+                for (int kk = 0; kk < kI8KB / 32; ++kk) {
+#pragma unroll
+                    for (int a = 0; a < kI8KLimbs; ++a) {
+                        const uint64_t ad = sdesc_sw64(base + a * kI8ATile + kk * 32);
+#pragma unroll
+                        for (int b = 0; b < kI8MLimbs; ++b) {
+                            const uint64_t bd = sdesc_sw64(base + kI8KLimbs * kI8ATile + b * kI8BTile + kk * 32);
+                            // the first product into each accumulator of the segment overwrites it:
+                            // (0,b) opens s = 0..3, (1,3) opens s = 4, (2,3) opens s = 5
+                            const bool first = ks == ks0 && kk == 0 && (a == 0 || b == kI8MLimbs - 1);
+                            umma_i8(st.tmem + (uint32_t)((a + b) * kI8N), ad, bd, first ? 0u : 1u);
+                        }
+                    }
+                }
+                umma_commit(smem_u32(&L.empty[stg]));
+            }
+            if (ok) umma_commit(smem_u32(L.accum));
+            u = ue;
+        }
+    }
+    if (warp < 4) {
+        long long seg = st.tiles;
+        const long long tfirst = u0 / nks;
+        for (long long u = u0; u < u1; ++seg) {
+            const int t = (int)(u / nks);
+            const long long ue = min(u1, (long long)(t + 1) * nks);
+            bool w = ok && mbar_wait(smem_u32(L.accum), (uint32_t)(seg & 1), F.gs, 212);
+            w = __all_sync(0xffffffffu, w);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (!w) { ok = false; break; }
+            const int row = warp * 32 + lane;
+            long long* slot = part + ((size_t)c * maxseg + (size_t)(t - tfirst)) * kI8SlotElems;
+#pragma unroll 1
+            for (int grp = 0; grp < kI8N / 32; ++grp) {
+                long long h[32];
+                int d[32];
+                const uint32_t ta = st.tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(grp * 32);
+                tmem_ld32_i(ta, d);
+#pragma unroll
+                for (int k = 0; k < 32; ++k) h[k] = (long long)d[k];
+#pragma unroll 1
+                for (int s = 1; s < kI8Acc; ++s) {
+                    tmem_ld32_i(ta + (uint32_t)(s * kI8N), d);
+#pragma unroll
+                    for (int k = 0; k < 32; ++k) h[k] = h[k] * 256 + (long long)d[k];
+                }
+#pragma unroll
+                for (int k = 0; k < 32; ++k) slot[(size_t)(grp * 32 + k) * 128 + row] = h[k];
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(L.tfree));
+            u = ue;
+        }
+    }
+    // every role walked the same segment list
+    {
+        long long nseg = 0, nk = 0;
+        for (long long u = u0; u < u1; ++nseg) {
+            const int t = (int)(u / nks);
+            const long long ue = min(u1, (long long)(t + 1) * nks);
+            nk += ue - u;
+            u = ue;
+        }
+        st.kb_done += nk;
+        st.tiles += nseg;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    return __syncthreads_and(ok ? 1 : 0) != 0;
+}
+
+// exact int64 demag sum of row lr of a tile for instance lj: the slots of the
+// CTAs cv.first..cv.last that cover the tile
+MT_DEV long long i8_tile_sum(const long long* part, int maxseg, const SkCover& cv, int lr, int lj)
+{
+    const size_t off = (size_t)lj * 128 + (size_t)lr;
+    long long acc = __ldcg(&part[((size_t)cv.first * maxseg + (size_t)cv.jf) * kI8SlotElems + off]);
+    for (int c = cv.first + 1; c <= cv.last; ++c) acc += __ldcg(&part[(size_t)c * maxseg * kI8SlotElems + off]);
+    return acc;
+}

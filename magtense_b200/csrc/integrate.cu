@@ -436,7 +436,7 @@ MT_DEV int rk_step_integrate(Ctx& X, RKS& s)
         s.phase2 = 1;
         s.h = fabs(s.h);
         const double ypnorm = fmax(0.0, v1[0] < 0.0 ? -1.0 : v1[0]);
-        const double tau = pow(s.tol, 0.2);
+        const double tau = root5(s.tol);
         if (xmul(s.h, ypnorm) > tau) s.h = tau / ypnorm;
         hmin = fmax(X.Q.sqtiny, xmul(X.Q.toosml, fmax(fabs(s.t_start), fabs(s.t_end))));
         s.h = xmul(s.dir, fmax(s.h, hmin));
@@ -475,16 +475,16 @@ MT_DEV int rk_step_integrate(Ctx& X, RKS& s)
                 s.bad_step_count++;
                 s.stiff_bad_step_count++;
                 if (failed) alpha = 0.5;
-                else alpha = fmax(xmul(0.8, pow(s.tol / err, 0.2)), 0.5);
+                else alpha = fmax(xmul(0.8, root5(s.tol / err)), 0.5);
             }
             s.h = xmul(alpha, s.h);
             failed = 1;
             continue;
         }
-        double beta = pow(err / s.tol, 0.2);
+        double beta = root5(err / s.tol);
         if (!s.at_t_start) {
-            const double t1 = pow(err, 0.2) / s.h;
-            const double t2 = pow(s.errold, 0.2) / s.h_old;
+            const double t1 = root5(err) / s.h;
+            const double t2 = root5(s.errold) / s.h_old;
             if (t1 < xmul(t2, 100.0) && t2 < xmul(t1, 100.0)) beta = xmul(beta, t1 / t2);
         }
         alpha = 8.0;

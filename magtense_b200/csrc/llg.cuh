@@ -106,8 +106,7 @@ MT_DEV double lap_cell_dev(const DevProb& P, const double* v, int i)
 // S = sum_j K m (FP32, this cell's three rows).
 struct CellFields { double hj[3], hh[3], hk[3], hm[3]; };
 
-MT_DEV CellFields cell_fields(const DevProb& P, const double* m, int i, const float S[3],
-                              const TimeScalars& ts)
+MT_DEV CellFields cell_fields_local(const DevProb& P, const double* m, int i, const TimeScalars& ts)
 {
     const int n = P.n;
     CellFields F;
@@ -122,17 +121,23 @@ MT_DEV CellFields cell_fields(const DevProb& P, const double* m, int i, const fl
     F.hk[0] = xmul(k2, xadd(xadd(xmul(axx, mx), xmul(axy, my)), xmul(axz, mz)));
     F.hk[1] = xmul(k2, xadd(xadd(xmul(axy, mx), xmul(ayy, my)), xmul(ayz, mz)));
     F.hk[2] = xmul(k2, xadd(xadd(xmul(axz, mx), xmul(ayz, my)), xmul(azz, mz)));
+    return F;
+}
+
+MT_DEV CellFields cell_fields(const DevProb& P, const double* m, int i, const float S[3],
+                              const TimeScalars& ts)
+{
+    CellFields F = cell_fields_local(P, m, i, ts);
     const float ms = __ldg(&P.Mfact[i]);
     for (int a = 0; a < 3; ++a) F.hm[a] = (double)__fmul_rn(-S[a], ms);
     return F;
 }
 
 // dm/dt for one cell (dmdt_fct :251-271).
-MT_DEV void cell_rhs(const DevProb& P, const double* m, int i, const float S[3], const TimeScalars& ts,
-                     double out[3])
+MT_DEV void cell_rhs_from(const DevProb& P, const double* m, int i, const CellFields& F, const TimeScalars& ts,
+                          double out[3])
 {
     const int n = P.n;
-    CellFields F = cell_fields(P, m, i, S, ts);
     const double mx = ldcg(&m[i]), my = ldcg(&m[n + i]), mz = ldcg(&m[2 * n + i]);
     double he[3];
     for (int a = 0; a < 3; ++a) he[a] = xadd(xadd(xadd(F.hh[a], F.hj[a]), F.hm[a]), F.hk[a]);
@@ -146,6 +151,21 @@ MT_DEV void cell_rhs(const DevProb& P, const double* m, int i, const float S[3],
     out[0] = xsub(xmul(g, cx), xmul(ts.alpha, h2x));
     out[1] = xsub(xmul(g, cy), xmul(ts.alpha, h2y));
     out[2] = xsub(xmul(g, cz), xmul(ts.alpha, h2z));
+}
+
+MT_DEV void cell_rhs(const DevProb& P, const double* m, int i, const float S[3], const TimeScalars& ts,
+                     double out[3])
+{
+    cell_rhs_from(P, m, i, cell_fields(P, m, i, S, ts), ts, out);
+}
+
+// the same with the demagnetisation field given in FP64 (exact fixed-point product)
+MT_DEV void cell_rhs_h(const DevProb& P, const double* m, int i, const double hm[3], const TimeScalars& ts,
+                       double out[3])
+{
+    CellFields F = cell_fields_local(P, m, i, ts);
+    F.hm[0] = hm[0]; F.hm[1] = hm[1]; F.hm[2] = hm[2];
+    cell_rhs_from(P, m, i, F, ts, out);
 }
 
 // ------------------------------------------------------------------------

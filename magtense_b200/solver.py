@@ -174,7 +174,7 @@ class Solver:
             pass
 
 
-PRECISIONS = {"fp32": 0, "bf16x3": 1, "bf16x2": 2, "fp16s": 3}
+PRECISIONS = {"fp32": 0, "bf16x3": 1, "bf16x2": 2, "fp16s": 3, "int8": 4}
 
 
 class BatchSolver:
@@ -182,8 +182,15 @@ class BatchSolver:
 
     Each instance has its own applied-field table, damping and initial state,
     and its own RKSUITE 'M' step control; all demag products of one
-    right-hand-side evaluation form one GEMM (``precision``: "fp32" SIMT,
-    "bf16x3" / "bf16x2" split-BF16 on the tcgen05 tensor cores).
+    right-hand-side evaluation form one GEMM.  ``precision``:
+
+    - "fp32": FP32 SIMT, the reference's arithmetic;
+    - "bf16x3" / "bf16x2": split-BF16 on the tcgen05 tensor cores, FP32 accumulate;
+    - "fp16s": row-scaled split-FP16 on the tensor cores, FP32 accumulate;
+    - "int8": exact fixed-point product on the integer tensor pipe (tensor rows
+      as 24-bit fixed point, m as rint(m 2^30), twelve int8 limb products summed
+      exactly).  It has no rounding noise, so the step-size control sees the
+      dynamics instead of FP32 rounding; needs |m| < 1.96.
     """
 
     def __init__(self, res, grid_L, B, *, precision="bf16x3", A0=1.3e-11, Ms=8e5, K0=0.0, u_ea=None, device=None):

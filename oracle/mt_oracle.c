@@ -28,9 +28,13 @@
  *   output driver  MagTense_ODE_RKSuite  source/NumericalIntegration/NumericalIntegration/ODE_Solvers.f90:124-237
  *                  simple_unique/simple_sort SpecialFunctions.f90:13-65
  *
- * Two precisions: mode 0 ("ref") keeps the reference's FP32 demag tensor and
+ * Three precisions: mode 0 ("ref") keeps the reference's FP32 demag tensor and
  * FP32 demag product; mode 1 ("fp64") keeps the tensor and the product in
- * FP64 and serves the error statements against FP64.
+ * FP64 and serves the error statements against FP64; mode 2 ("int8") is the
+ * exact fixed-point product of the GPU's int8 backend, restated from its
+ * definition (rows of the FP32 tensor as 24-bit fixed point in three int8
+ * limbs, m as rint(m 2^30) in four limbs, all twelve limb products summed
+ * exactly), so the GPU must reproduce it bit for bit.
  *
  * Summation order of the FP32 demag product follows the reference BLAS SGEMV
  * column sweep (y(i) += (-x(j))*A(i,j), j = 1..n, one block after the other);
@@ -235,6 +239,28 @@ void or_assemble(int nx, int ny, int nz, double Lx, double Ly, double Lz,
     free(pts);
 }
 
+/* x^(1/5) for the step-size control (RKSuitef90.f90 uses (tol/err)**expon
+ * with expon = 1/5).  libm pow differs between the host and the device in the
+ * last bits, so both sides use this fixed iteration of IEEE operations:
+ * x = f 2^e, e = 5 q + r, y = f 2^r in [0.5, 16), twelve Newton steps
+ * z <- z + (y / z^4 - z) / 5 from z = 1 (y < 2) or 1.5, result 2^q z. */
+static double or_root5(double x)
+{
+    if (!(x > 0.0)) return 0.0;
+    if (isinf(x)) return x;
+    int e = 0;
+    const double f = frexp(x, &e);
+    const int q = (e >= 0) ? e / 5 : -((-e + 4) / 5);
+    const double y = ldexp(f, e - 5 * q);
+    double z = (y < 2.0) ? 1.0 : 1.5;
+    for (int k = 0; k < 12; ++k) {
+        const double z2 = z * z;
+        const double z4 = z2 * z2;
+        z = z + (y / z4 - z) / 5.0;
+    }
+    return ldexp(z, q);
+}
+
 /* ------------------------------------------------------------------ */
 /* problem and right-hand side                                         */
 /* ------------------------------------------------------------------ */
@@ -255,6 +281,11 @@ typedef struct {
     int renorm;                       /* per-cell |m| renormalisation after accepted steps */
     float* ms;                        /* FP32 copy of m for the demag product */
     long nrhs;
+    /* mode 2: limbs [3][3n][3n] of the fixed-point tensor rows, 2^(-30-e_r) per row */
+    signed char* klimb;
+    double* row_scale;
+    int* mlimb;                       /* [4][3n] limbs of the current m */
+    int range_err;                    /* a component of m outside (-1.96, 1.96) was seen */
 } or_problem;
 
 or_problem* or_problem_create(int nx, int ny, int nz, double Lx, double Ly, double Lz,
@@ -310,7 +341,89 @@ void or_problem_destroy(or_problem* p)
 {
     if (!p) return;
     free(p->alpha_tab); free(p->hext); free(p->Jfact); free(p->Kfact); free(p->Mfact);
-    free(p->A6); free(p->ms); free(p);
+    free(p->A6); free(p->ms); free(p->klimb); free(p->row_scale); free(p->mlimb); free(p);
+}
+int or_problem_range_err(const or_problem* p) { return p->range_err; }
+
+/* mode 2 tensor limbs from the FP32 tensor: row r = (a, i), column (b, j).
+ * 2^e_r puts the row's largest |K| in [2^21, 2^22); Kq = rint(K 2^e_r) =
+ * k0 2^16 + k1 2^8 + k2 with signed 8-bit digits (k2 the lowest);
+ * row_scale = 2^(-30 - e_r). */
+static void or_i8_build(or_problem* p)
+{
+    const int n = p->n, n3 = 3 * n;
+    static const int blk[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    const size_t tot = (size_t)n3 * n3;
+    p->klimb = (signed char*)malloc(3 * tot);
+    p->row_scale = (double*)malloc(sizeof(double) * n3);
+    p->mlimb = (int*)malloc(sizeof(int) * 4 * (size_t)n3);
+#pragma omp parallel for schedule(static)
+    for (int r = 0; r < n3; ++r) {
+        const int a = r / n, i = r - a * n;
+        float mx = 0.0f;
+        for (int b = 0; b < 3; ++b)
+            for (int j = 0; j < n; ++j) {
+                float v = fabsf(p->K32[((size_t)blk[a][b] * n + i) * (size_t)n + j]);
+                if (v > mx) mx = v;
+            }
+        int e = 0;
+        if (mx > 0.0f) frexpf(mx, &e);
+        const int ex = (mx > 0.0f) ? 22 - e : 0;
+        p->row_scale[r] = (mx > 0.0f) ? ldexp(1.0, -30 - ex) : 0.0;
+        for (int b = 0; b < 3; ++b)
+            for (int j = 0; j < n; ++j) {
+                const float v = p->K32[((size_t)blk[a][b] * n + i) * (size_t)n + j];
+                long long x = llrint(ldexp((double)v, ex));
+                const int k2 = (int)(signed char)(x & 0xff);
+                x = (x - k2) >> 8;
+                const int k1 = (int)(signed char)(x & 0xff);
+                x = (x - k1) >> 8;
+                const size_t e2 = (size_t)r * n3 + (size_t)b * n + j;
+                p->klimb[e2] = (signed char)x;
+                p->klimb[tot + e2] = (signed char)k1;
+                p->klimb[2 * tot + e2] = (signed char)k2;
+            }
+    }
+}
+
+/* mode 2 demag field: Hm = -Ms_i * 2^(-30-e_r) * H_int with the exact
+ * H_int = sum_j Kq_rj mq_j = sum_s 2^(8(5-s)) D_s, D_s = sum_j sum_{a+b=s} k_a m_b
+ * (all twelve limb products), converted to double once */
+static void or_i8_demag(or_problem* p, const double* m, double* Hm)
+{
+    const int n = p->n, n3 = 3 * n;
+    const size_t tot = (size_t)n3 * n3;
+    if (!p->klimb) or_i8_build(p);
+    int* ml = p->mlimb;
+    for (int j = 0; j < n3; ++j) {
+        double v = m[j];
+        if (!(fabs(v) <= 1.96)) { p->range_err = 1; v = 0.0; }
+        long long x = llrint(v * 1073741824.0);
+        int d[4];
+        for (int l = 3; l >= 1; --l) {
+            const int dl = (int)(signed char)(x & 0xff);
+            d[l] = dl;
+            x = (x - dl) >> 8;
+        }
+        d[0] = (int)x;
+        for (int l = 0; l < 4; ++l) ml[(size_t)l * n3 + j] = d[l];
+    }
+#pragma omp parallel for schedule(static)
+    for (int r = 0; r < n3; ++r) {
+        int D[6] = {0, 0, 0, 0, 0, 0};
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 4; ++b) {
+                const signed char* kr = p->klimb + (size_t)a * tot + (size_t)r * n3;
+                const int* mr = ml + (size_t)b * n3;
+                int acc = 0;
+                for (int j = 0; j < n3; ++j) acc += (int)kr[j] * mr[j];
+                D[a + b] += acc;
+            }
+        long long h = (long long)D[0];
+        for (int s2 = 1; s2 < 6; ++s2) h = h * 256 + (long long)D[s2];
+        const int i = r % n;
+        Hm[r] = (-(double)p->Mfact[i]) * ((double)h * p->row_scale[r]);
+    }
 }
 
 /* locate + interp1_MagTense (util.f90:39-85).  Outside the table the value is 0;
@@ -399,7 +512,9 @@ void or_fields(or_problem* p, double t, const double* m, double* Hj, double* Hh,
         Hk[2 * n + i] = k2 * ((A[2 * n + i] * mx[i] + A[4 * n + i] * my[i]) + A[5 * n + i] * mz[i]);
     }
     /* demag */
-    if (p->mode == 0) {
+    if (p->mode == 2) {
+        or_i8_demag(p, m, Hm);
+    } else if (p->mode == 0) {
         float* ms = p->ms;
         for (int i = 0; i < 3 * n; ++i) ms[i] = (float)m[i];
         const float* K = p->K32;
@@ -887,7 +1002,7 @@ static int rk_step_integrate(or_rk* R)
             any = 1;
         }
         ypnorm = fmax(0.0, any ? mx : -DBL_MAX);
-        double tau = pow(R->tol, R->expon);
+        double tau = or_root5(R->tol);
         if (R->h * ypnorm > tau) R->h = tau / ypnorm;
         hmin = fmax(R->sqtiny, R->toosml * fmax(fabs(R->t_start), fabs(R->t_end)));
         R->h = R->dir * fmax(R->h, hmin);
@@ -929,15 +1044,15 @@ static int rk_step_integrate(or_rk* R)
                 R->bad_step_count++;
                 R->stiff_bad_step_count++;
                 if (failed) alpha = R->rs1;
-                else { alpha = R->safety * pow(R->tol / err, R->expon); alpha = fmax(alpha, R->rs1); }
+                else { alpha = R->safety * or_root5(R->tol / err); alpha = fmax(alpha, R->rs1); }
             }
             R->h = alpha * R->h; failed = 1;
             continue;
         }
-        double beta = pow(err / R->tol, R->expon);
+        double beta = or_root5(err / R->tol);
         if (!R->at_t_start) {
-            double t1 = pow(err, R->expon) / R->h;
-            double t2 = pow(R->errold, R->expon) / R->h_old;
+            double t1 = or_root5(err) / R->h;
+            double t2 = or_root5(R->errold) / R->h_old;
             if (t1 < t2 * 100.0 && t2 < t1 * 100.0) beta = beta * (t1 / t2);
         }
         alpha = R->rs3;

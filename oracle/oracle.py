@@ -67,6 +67,8 @@ def lib():
         L.or_problem_nrhs.argtypes = [C.c_void_p]
         L.or_problem_nrhs.restype = C.c_long
         L.or_problem_destroy.argtypes = [C.c_void_p]
+        L.or_problem_range_err.argtypes = [C.c_void_p]
+        L.or_problem_range_err.restype = C.c_int
         L.or_fields.argtypes = [C.c_void_p, C.c_double, D, D, D, D, D]
         L.or_rhs.argtypes = [C.c_void_p, C.c_double, D, D]
         L.or_interp1.argtypes = [D, C.c_int, C.c_int, C.c_int, C.c_double]
@@ -146,6 +148,8 @@ class Problem:
 
     mode 0 ("ref"): FP32 tensor and FP32 demag product, as the reference.
     mode 1 ("fp64"): FP64 tensor and FP64 product.
+    mode 2 ("int8"): the exact fixed-point product of the int8 backend, from
+    the FP32 tensor (24-bit rows, m as rint(m 2^30), twelve limb products).
     """
 
     def __init__(self, res, L, *, solver=2, mode=0, A0=1.3e-11, Ms=8e5, K0=0.0, u_ea=None,
@@ -165,7 +169,7 @@ class Problem:
         self.Ms = Ms
         self.h = lib().or_problem_create(nx, ny, nz, *self.L, solver, mode, float(A0), _d(Ms), _d(K0), _d(u),
                                          float(gamma), float(alpha), _d(at), at.shape[0], _d(he), he.shape[0])
-        if mode == 0 and K32 is None:
+        if mode in (0, 2) and K32 is None:
             K32, _ = assemble(res, L, fp32=True)
         if mode == 1 and K64 is None:
             _, K64 = assemble(res, L, fp32=False, fp64=True)
@@ -188,6 +192,11 @@ class Problem:
 
     def set_alpha0(self, a):
         lib().or_problem_set_alpha0(self.h, float(a))
+
+    @property
+    def range_err(self):
+        """mode 2: a component of m outside (-1.96, 1.96) was met"""
+        return bool(lib().or_problem_range_err(self.h))
 
     @property
     def nrhs(self):

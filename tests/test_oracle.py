@@ -212,6 +212,38 @@ def test_demag_ref_and_fp64_agree(oracle):
     np.testing.assert_array_equal(Hr, H32[:, rows])
 
 
+def test_demag_int8_is_the_exact_fixed_point_product(oracle):
+    # mode 2 (twelve int8 limb products) must equal the plain definition
+    # -Ms 2^(-30-e_r) sum_j rint(K_rj 2^e_r) rint(m_j 2^30), computed here with numpy int64
+    res, L = [10, 4, 2], [50e-9, 20e-9, 10e-9]
+    n = 80
+    rng = np.random.default_rng(7)
+    m = rng.standard_normal((3, n))
+    m /= np.linalg.norm(m, axis=0)
+    K32, K64 = oracle.assemble(res, L, fp32=True, fp64=True)
+    blk = [[0, 1, 2], [1, 3, 4], [2, 4, 5]]
+    Kfull = np.block([[K32[blk[a][b]] for b in range(3)] for a in range(3)])      # rows (a,i), cols (b,j)
+    rowmax = np.abs(Kfull).max(axis=1)
+    _, e = np.frexp(rowmax)
+    ex = 22 - e
+    Kq = np.rint(np.ldexp(Kfull.astype(np.float64), ex[:, None])).astype(np.int64)
+    assert np.abs(Kq).max() < 2**22 and np.abs(Kq).max(axis=1).min() >= 2**21
+    mq = np.rint(m.reshape(-1) * 2.0**30).astype(np.int64)
+    Hint = Kq @ mq                                                       # |terms| < 2^53, exact in int64
+    Hdef = -8e5 * (Hint.astype(np.float64) * np.ldexp(1.0, -30 - ex))
+    P2 = oracle.Problem(res, L, mode=2, K32=K32)
+    H2 = P2.fields(0, m)[3].reshape(-1)
+    np.testing.assert_array_equal(H2, Hdef)
+    assert not P2.range_err
+    H64 = oracle.Problem(res, L, mode=1, K64=K64).fields(0, m)[3].reshape(-1)
+    assert np.abs(H2 - H64).max() <= 2e-5 * np.abs(H64).max()
+    # outside (-1.96, 1.96) the product flags a range error
+    m2 = m.copy()
+    m2[0, 3] = 2.0
+    P2.fields(0, m2)
+    assert P2.range_err
+
+
 def test_interp1_semantics(oracle):
     tab = np.array([[0.0, 1.0], [1.0, 3.0], [3.0, 7.0]])
     assert oracle.interp1(tab, 1, 0.5) == 2.0
