@@ -6,8 +6,9 @@ Ms 8e5 A/m, A 1.3e-11 J/m, K 0) sharing one demag tensor, each driven by a
 seeded in-plane field (angle U[0,360) deg, magnitude U[0,50] mT), integrated
 for 1 ns at alpha = gamma*0.02 (gamma = 2.211e5) from an s-state with per-
 instance RKSUITE 'M' step control, tol 1e-6, output every 1 ps.  The demag
-products run as one split-BF16 (bf16x3) tcgen05 GEMM per right-hand-side
-evaluation inside one persistent kernel.  Seeded synthetic inputs stand in
+products run as one exact fixed-point tcgen05 GEMM (int8 limbs, kind::i8) per
+right-hand-side evaluation inside one persistent kernel; --precision picks the
+split-FP16/BF16 or FP32 SIMT products instead.  Seeded synthetic inputs stand in
 for the std-problem-4 dataset workflow.  One step = every instance of the
 rank integrated over the window.
 
@@ -56,7 +57,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="film-batch", choices=["film-batch", "film-plain", "large-plain"])
     ap.add_argument("--instances", type=int, default=256, help="instances per rank (film-batch)")
-    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "bf16x2", "fp32"])
+    ap.add_argument("--precision", default="int8", choices=["int8", "fp16s", "bf16x3", "bf16x2", "fp32"])
+    ap.add_argument("--plain-sample", type=int, default=4,
+                    help="film-batch: instances of the same workload run through the plain FP32 path for the ratio")
     ap.add_argument("--window", type=float, default=None, help="simulated ns per instance per step")
     ap.add_argument("--cpu-window", type=float, default=0.3, help="simulated ns of the bounded CPU sample")
     ap.add_argument("--no-cpu", action="store_true")
@@ -153,8 +156,8 @@ def cpu_reference_sample(window_ns, workload="film"):
     _, _, _, st = P.solve(np.linspace(0, win, nt), m0, tol=1e-6)
     dt = time.perf_counter() - t0
     return {"value": window_ns / dt, "unit": "simulated ns/s", "cores": O.threads(), "kind": "port",
-            "sample": f"{window_ns} ns of one 80x20x1 film instance ({st['f_evals']} RHS evals, {dt:.1f} s, "
-                      f"FP32-demag restatement of the reference on the host cores)"}
+            "sample": f"{window_ns} ns of one {res[0]}x{res[1]}x{res[2]} instance ({st['f_evals']} RHS evals, "
+                      f"{dt:.1f} s, FP32-demag restatement of the reference on the host cores)"}
 
 
 def run_reference(args):
@@ -293,17 +296,21 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
             e2e.append((time.perf_counter() - t0) * 1e3)
             del y
         e2e_ms = statistics.median(e2e)
-    # the plain FP32 single-instance path on the same geometry and workload, for the ratio
-    plain_window = min(window, 0.05)
-    plain.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.02,
-                       hext=np.array([[0.0, *fields[0]], [plain_window * 1e-9, *fields[0]]]))
-    tp = np.linspace(0, plain_window * 1e-9, int(round(plain_window / 1e-3)) + 1)
-    plain.integrate(tp, m_s, tol=1e-6)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    _, _, _, pst = plain.integrate(tp, m_s, tol=1e-6)
-    torch.cuda.synchronize()
-    plain_rate = plain_window / (time.perf_counter() - t0)
+    # the plain FP32 single-instance path on the same workload, for the ratio: seeded instances
+    # of this rank's set, each integrated over the same window, one after another
+    pick = sorted(int(k) for k in np.random.default_rng(7).choice(B, size=min(args.plain_sample, B), replace=False))
+    plain_s, plain_evals = 0.0, 0
+    for k in pick:
+        plain.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.02,
+                           hext=np.array([[0.0, *fields[k]], [win, *fields[k]]]))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, yp, _, pst = plain.integrate(t, m_s, tol=1e-6)
+        torch.cuda.synchronize()
+        plain_s += time.perf_counter() - t0
+        plain_evals += pst["f_evals"]
+        del yp
+    plain_rate = len(pick) * window / plain_s
     step_ms = max(times)
     step_ms, e2e_red = max_over_ranks(torch, dist, [step_ms, e2e_ms or 0.0])
     if rank != 0:
@@ -328,10 +335,18 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
                    "l2": "flushed (256 MB write) before every timed step"},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
                      "frac": achieved / peak_tf, "traffic": None,
-                     "note": f"batch_kernel: 18*n^2 useful flops per instance RHS evaluation x {evals} evaluations "
-                             f"over {kms:.1f} ms of device time; peak = sustained cuBLAS bf16 ({src})"},
-        "plain_fp32_same_geometry": {"value": plain_rate, "unit": "simulated ns/s",
-                                     "note": f"single-instance FP32 path, {plain_window} ns window"},
+                     "note": f"batch_kernel (the whole persistent integrator, GEMM and RKSUITE coroutines): 18*n^2 "
+                             f"useful flops per instance RHS evaluation x {evals} evaluations over {kms:.1f} ms of "
+                             f"device time; peak = sustained cuBLAS bf16 ({src})"
+                             + ("; the int8 product executes 12 int8 limb products per useful product" if
+                                args.precision == "int8" else "")},
+        "rhs_evals_per_instance": {"min": int(min(x["f_evals"] for x in stats[-1])),
+                                   "median": float(np.median([x["f_evals"] for x in stats[-1]])),
+                                   "max": int(max(x["f_evals"] for x in stats[-1]))},
+        "plain_fp32_same_workload": {"value": plain_rate, "unit": "simulated ns/s",
+                                     "rhs_evals": plain_evals, "instances": pick,
+                                     "note": f"single-instance FP32 path (the reference's arithmetic) on {len(pick)} "
+                                             f"seeded instances of the same set, {window} ns each, one after another"},
         "batched_over_plain": value / ws / plain_rate,
         "gpu_launches": int(launches),
         "rhs_evals_per_s": evals / (sum(times) / 1e3) * ws,
