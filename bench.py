@@ -247,11 +247,8 @@ def run_ours(args):
 
 
 def max_over_ranks(torch, dist, vals):
-    if not dist:
-        return vals
-    tt = torch.tensor(vals, device="cuda", dtype=torch.float64)
-    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    return [float(x) for x in tt]
+    from magtense_b200.shard import max_over_ranks as mx
+    return mx(vals)
 
 
 def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
@@ -264,7 +261,10 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
     nt = int(round(window / 1e-3)) + 1
     t = np.linspace(0, win, nt)
     plain, m_s = relaxed_state(torch, res, L)
-    fields = instance_fields(1000 + rank, B)
+    # the global instance list (ws * B seeded fields), this rank's contiguous slice
+    from magtense_b200.shard import shard_range
+    a0, a1 = shard_range(ws * B, ws, rank)
+    fields = instance_fields(1000, ws * B)[a0:a1]
     hext = np.zeros((B, 2, 4))
     hext[:, 1, 0] = win
     hext[:, :, 1:] = fields[:, None, :]
@@ -382,7 +382,7 @@ def bench_plain(torch, args, ws, rank, local, dist, hbm, src):
         s.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.1, hext=np.array([[0.0, *h], [win, *h]]))
     else:
         s, m_s = relaxed_state(torch, res, L)
-        h = instance_fields(1000 + rank, 1)[0]
+        h = instance_fields(1000, ws)[rank]
         s.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.02, hext=np.array([[0.0, *h], [win, *h]]))
 
     def step():
