@@ -897,10 +897,9 @@ MT_DEV void i8_fill_cover(BCtx& X, SkCover* cov)
     }
 }
 
-MT_DEV void epilogue_cell(const BCtx& X, int b, double t_rhs, int arg, int dst, int i)
+MT_DEV void epilogue_cell(const BCtx& X, int b, const TimeScalars& ts, int arg, int dst, int i)
 {
     const int n = X.P.n;
-    const TimeScalars ts = inst_scalars(X, b, t_rhs);
     const double* m = VPOOL(X, arg, b);
     double* out = dst_ptr(X, dst, b);
     if (X.Q.prec == kPrecI8) {
@@ -1044,7 +1043,7 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
     X.smem = smem_raw;
     const bool i8 = Q.prec == kPrecI8;
     const bool tc = Q.prec != kPrecFP32 && !i8;
-    struct ReqDesc { double t; int on, arg, dst, pad; };
+    struct ReqDesc { TimeScalars ts; int on, arg, dst, pad; };
     __shared__ ReqDesc s_req[kInstBlock];
     TcState tcs;
     tcs.kb_done = 0; tcs.tiles = 0; tcs.tmem = 0;
@@ -1179,19 +1178,22 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
             const BInst& I = L[k];
             if (X.lane == 0) {
                 const int li = X.warp + k * X.nwarps;
-                s_req[li].on = (X.i0 + li < Q.B && I.req == 1) ? 1 : 0;
+                const bool on = X.i0 + li < Q.B && I.req == 1;
+                s_req[li].on = on ? 1 : 0;
                 s_req[li].arg = I.rhs_arg;
                 s_req[li].dst = I.rhs_dst;
-                s_req[li].t = I.t_rhs;
+                // field and damping of the instance at the request time, once per instance
+                if (on) s_req[li].ts = inst_scalars(X, X.i0 + li, I.t_rhs);
             }
         }
         __syncthreads();
         for (int e = threadIdx.x; e < X.ni * X.nc; e += blockDim.x) {
             const int li = e / X.nc, cell = e - li * X.nc;
             if (!s_req[li].on) continue;
-            epilogue_cell(X, X.i0 + li, s_req[li].t, s_req[li].arg, s_req[li].dst, X.c0 + cell);
+            epilogue_cell(X, X.i0 + li, s_req[li].ts, s_req[li].arg, s_req[li].dst, X.c0 + cell);
         }
         __syncthreads();
+        PROF_MARK(6);
         for (int k = 0; k < mine; ++k) {
             BInst& I = L[k];
             const int b = X.i0 + X.warp + k * X.nwarps;
@@ -1206,7 +1208,7 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
     }
     if (prof) {
         if (t == 0) {
-            for (int k = 0; k < 6; ++k) atomicAdd(&F.prof[k], acc[k]);
+            for (int k = 0; k < 7; ++k) atomicAdd(&F.prof[k], acc[k]);
             atomicAdd(&F.prof[7], (unsigned long long)ticks_run);
         }
         // busiest CTA per work phase (P2, GEMM, P1): value and CTA index

@@ -959,10 +959,12 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
         unsigned long long pr[16];
         CUDA_TRY(cudaMemcpy(pr, F.prof, sizeof(pr), cudaMemcpyDeviceToHost));
         const double tk = pr[7] ? (double)pr[7] : 1.0;
-        fprintf(stderr, "[batch profile] ticks %llu  per tick (us) at CTA 0: P2 %.2f B1 %.2f GEMM %.2f Bh %.2f P1 %.2f B2 %.2f"
-                "  busiest CTA: P2 %.2f (cta %llu) GEMM %.2f (cta %llu) P1 %.2f (cta %llu)\n",
-                pr[7], pr[0] / tk / 1e3, pr[1] / tk / 1e3, pr[2] / tk / 1e3, pr[3] / tk / 1e3, pr[4] / tk / 1e3,
-                pr[5] / tk / 1e3, pr[8] / tk / 1e3, pr[12], pr[9] / tk / 1e3, pr[13], pr[10] / tk / 1e3, pr[14]);
+        fprintf(stderr, "[batch profile] ticks %llu  per tick (us) at CTA 0: P2 %.2f B1 %.2f GEMM %.2f Bh %.2f "
+                "P1 epilogue %.2f advance %.2f B2 %.2f  busiest CTA: P2 %.2f (cta %llu) GEMM %.2f (cta %llu) "
+                "P1 advance %.2f (cta %llu)\n",
+                pr[7], pr[0] / tk / 1e3, pr[1] / tk / 1e3, pr[2] / tk / 1e3, pr[3] / tk / 1e3, pr[6] / tk / 1e3,
+                pr[4] / tk / 1e3, pr[5] / tk / 1e3, pr[8] / tk / 1e3, pr[12], pr[9] / tk / 1e3, pr[13],
+                pr[10] / tk / 1e3, pr[14]);
     }
     if (worst) return fail(MT_ERR_SOLVER, "an instance stopped with RKSUITE flag %d", worst);
     return MT_OK;
