@@ -1117,6 +1117,7 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
         ticks_run++;
         // P2: resolve reductions, advance
         int my_active = 0, my_rhs = 0;
+        int rhs_tile[2] = {0, 0};   // requests per 64-instance tile, tiles jb0 and jb0 + 1
         for (int k = 0; k < mine; ++k) {
             BInst& I = L[k];
             const int b = X.i0 + X.warp + k * X.nwarps;
@@ -1124,32 +1125,35 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
             if (I.req == 2) resolve_reduce(X, I, b);
             if (I.req == 0) advance(X, I, b);
             if (I.req != 3 && I.req != 4) my_active++;
-            if (I.req == 1) my_rhs++;
+            if (I.req == 1) { my_rhs++; rhs_tile[(b / kI8N - X.jb0) & 1]++; }
         }
         asm volatile("fence.proxy.async.global;" ::: "memory");   // operand stores -> TMA reads
         if (X.lane == 0 && X.cb == 0 && (my_active | my_rhs)) {
             atomicAdd(&ctr[0], (unsigned)my_active);
             atomicAdd(&ctr[1], (unsigned)my_rhs);
-            if (my_rhs) atomicAdd(&F.ibreq[(tick % 3) * Q.IB + X.ib], (unsigned)my_rhs);
+            for (int h = 0; h < 2; ++h)
+                if (rhs_tile[h]) atomicAdd(&F.ibreq[(tick % 3) * 2 * Q.IB + X.jb0 + h], (unsigned)rhs_tile[h]);
         }
         __syncthreads();
         PROF_MARK(0);
         if (!grid_sync(F.gs, 1)) { ok = false; break; }
         PROF_MARK(1);
         const unsigned active = __ldcg(&ctr[0]);
-        const unsigned nreq = __ldcg(&F.ibreq[(tick % 3) * Q.IB + X.ib]);   // requests in this tile's instances
+        // requests in this CTA's 128-instance block (its two 64-instance tiles)
+        const unsigned nreq = __ldcg(&F.ibreq[(tick % 3) * 2 * Q.IB + 2 * X.ib]) +
+                              __ldcg(&F.ibreq[(tick % 3) * 2 * Q.IB + 2 * X.ib + 1]);
         if (t == 0 && threadIdx.x == 0) {
             unsigned* nxt = F.counters + 2 * ((tick + 1) % 3);
             nxt[0] = 0; nxt[1] = 0;
-            for (int k = 0; k < Q.IB; ++k) F.ibreq[((tick + 1) % 3) * Q.IB + k] = 0;
+            for (int k = 0; k < 2 * Q.IB; ++k) F.ibreq[((tick + 1) % 3) * 2 * Q.IB + k] = 0;
         }
         if (active == 0) break;
         if (i8) {
-            // 64-instance tiles of the blocks with requests, in order; every CTA builds the same list
+            // 64-instance tiles with requests, in order; every CTA builds the same list
             if (threadIdx.x == 0) {
                 int na = 0;
                 for (int k = 0; k < 2 * Q.IB; ++k) {
-                    const bool on = __ldcg(&F.ibreq[(tick % 3) * Q.IB + k / 2]) > 0;
+                    const bool on = __ldcg(&F.ibreq[(tick % 3) * 2 * Q.IB + k]) > 0;
                     s_actpos[k] = on ? na : -1;
                     if (on) s_act[na++] = k;
                 }

@@ -58,7 +58,7 @@ struct BatchBufs {
     BInst* inst;       // [CB][Bp] private coroutine copies
     GridSync* gs;
     unsigned* counters;  // [3][2]: active instances, right-hand-side requests
-    unsigned* ibreq;     // [3][IB]: right-hand-side requests per instance block
+    unsigned* ibreq;     // [3][2 IB]: right-hand-side requests per 64-instance tile
     unsigned long long* prof;  // [8] phase times (ns) seen by CTA 0, or nullptr
     // per-instance inputs
     const double* hext;    // [Bp][nt_hext][4]

@@ -726,11 +726,11 @@ int batch_alloc(mt_batch* bt, BatchRun& R, int nt, cudaStream_t s)
     CUDA_TRY(R.A.get(&F.gs, 1));
     CUDA_TRY(R.A.get(&F.counters, 6));
     CUDA_TRY(cudaMemsetAsync(F.counters, 0, sizeof(unsigned) * 6, s));
-    CUDA_TRY(R.A.get(&F.ibreq, 3 * (size_t)bt->IB));
-    CUDA_TRY(cudaMemsetAsync(F.ibreq, 0, sizeof(unsigned) * 3 * bt->IB, s));
+    CUDA_TRY(R.A.get(&F.ibreq, 6 * (size_t)bt->IB));
+    CUDA_TRY(cudaMemsetAsync(F.ibreq, 0, sizeof(unsigned) * 6 * bt->IB, s));
     if (getenv("MT_BATCH_PROFILE")) {
-        CUDA_TRY(R.A.get(&F.prof, 16));
-        CUDA_TRY(cudaMemsetAsync(F.prof, 0, sizeof(unsigned long long) * 16, s));
+        CUDA_TRY(R.A.get(&F.prof, 32));
+        CUDA_TRY(cudaMemsetAsync(F.prof, 0, sizeof(unsigned long long) * 32, s));
     }
     F.hext = bt->hext;
     F.alpha0 = bt->alpha0;
@@ -903,7 +903,7 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
     for (;;) {
         CUDA_TRY(cudaMemsetAsync(F.gs, 0, sizeof(GridSync), s));
         CUDA_TRY(cudaMemsetAsync(F.counters, 0, sizeof(unsigned) * 6, s));
-        CUDA_TRY(cudaMemsetAsync(F.ibreq, 0, sizeof(unsigned) * 3 * bt->IB, s));
+        CUDA_TRY(cudaMemsetAsync(F.ibreq, 0, sizeof(unsigned) * 6 * bt->IB, s));
         CUDA_TRY(cudaEventRecord(ev0, s));
         CUDA_TRY(launch_batch(P, F, Q, bt->grid, bt->prec != MT_PREC_FP32 ? &R.maps : nullptr, s,
                               l2_bytes ? (bt->prec == MT_PREC_INT8 ? (const void*)bt->klimb : (const void*)bt->khi)
@@ -956,7 +956,7 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
     stats[0].launches = launches;
     stats[0].kernel_ms = kernel_ms;
     if (F.prof) {
-        unsigned long long pr[16];
+        unsigned long long pr[32];
         CUDA_TRY(cudaMemcpy(pr, F.prof, sizeof(pr), cudaMemcpyDeviceToHost));
         const double tk = pr[7] ? (double)pr[7] : 1.0;
         fprintf(stderr, "[batch profile] ticks %llu  per tick (us) at CTA 0: P2 %.2f B1 %.2f GEMM %.2f Bh %.2f "
@@ -965,6 +965,11 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
                 pr[7], pr[0] / tk / 1e3, pr[1] / tk / 1e3, pr[2] / tk / 1e3, pr[3] / tk / 1e3, pr[6] / tk / 1e3,
                 pr[4] / tk / 1e3, pr[5] / tk / 1e3, pr[8] / tk / 1e3, pr[12], pr[9] / tk / 1e3, pr[13],
                 pr[10] / tk / 1e3, pr[14]);
+        if (bt->prec == MT_PREC_INT8)
+            fprintf(stderr, "[batch profile] int8 GEMM at CTA 0 per tick (us): roles done %.2f, total %.2f; MMA waits "
+                    "full %.2f tfree %.2f; epilogue waits %.2f drains %.2f; producer waits %.2f; units %.1f segments %.2f\n",
+                    pr[23] / tk / 1e3, pr[24] / tk / 1e3, pr[16] / tk / 1e3, pr[17] / tk / 1e3, pr[18] / tk / 1e3,
+                    pr[19] / tk / 1e3, pr[20] / tk / 1e3, pr[21] / tk, pr[22] / tk);
     }
     if (worst) return fail(MT_ERR_SOLVER, "an instance stopped with RKSUITE flag %d", worst);
     return MT_OK;

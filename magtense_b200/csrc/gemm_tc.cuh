@@ -56,8 +56,11 @@ MT_DEV void mbar_expect_tx(uint32_t bar, uint32_t bytes)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
-// bounded wait on the given phase parity; false after the limit
-MT_DEV bool mbar_wait(uint32_t bar, uint32_t parity, GridSync* gs, int where)
+// bounded wait on the given phase parity; false after the limit.  sleep_ns > 0:
+// a patient waiter (the accumulator readers wait a whole segment of MMAs) that
+// backs off between polls, so it does not take issue slots from the warps that
+// drive the copies and the MMAs on the same SM sub-partition.
+MT_DEV bool mbar_wait(uint32_t bar, uint32_t parity, GridSync* gs, int where, unsigned sleep_ns = 0)
 {
     uint32_t done = 0;
     const uint64_t t0 = globaltimer_ns();
@@ -67,6 +70,7 @@ MT_DEV bool mbar_wait(uint32_t bar, uint32_t parity, GridSync* gs, int where)
                      : "r"(bar), "r"(parity)
                      : "memory");
         if (done) return true;
+        if (sleep_ns && it >= 4) __nanosleep(sleep_ns);
         if ((it & 255) == 255) {
             if (ld_volatile_i32(&gs->abort)) return false;
             if (globaltimer_ns() - t0 > 2000000000ULL) break;
@@ -259,7 +263,7 @@ MT_DEV bool tc_gemm_tile_impl(unsigned char* smem, const QT& Q, const FT& F, con
     }
     if (warp < 4) {
         const uint32_t ph = (uint32_t)(st.tiles & 1);
-        bool w = mbar_wait(smem_u32(L.accum), ph, F.gs, 202);
+        bool w = mbar_wait(smem_u32(L.accum), ph, F.gs, 202, 200);
         w = __all_sync(0xffffffffu, w);
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         if (w) {
@@ -428,6 +432,12 @@ MT_DEV SkCover sk_cover(long long t, long long nks, long long U)
     return cv;
 }
 
+// GEMM-internal timers of CTA 0 (prof slots 16..23) when profiling is on
+MT_DEV void i8_prof_add(unsigned long long* prof, int slot, unsigned long long v)
+{
+    if (prof && blockIdx.x == 0) atomicAdd(&prof[slot], v);
+}
+
 // The Stream-K share of this CTA in one tick: nact active instance tiles
 // (act_jb[0..nact), 64 instances each), RB row blocks, nks k steps per tile.
 // part: int64 slots [gridDim.x][maxseg][64][128].  Returns a CTA-uniform ok flag.
@@ -442,8 +452,11 @@ MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int
     bool ok = true;
     if (c >= G) return __syncthreads_and(1) != 0;
     const long long u0 = sk_start(c, U, G), u1 = sk_start(c + 1, U, G);
+    unsigned long long* prof = F.prof;
+    const uint64_t t_in = globaltimer_ns();
     if (warp == 4 && lane == 0) {
         long long g = st.kb_done;
+        unsigned long long wait_empty = 0;
         for (long long u = u0; u < u1 && ok;) {
             const int t = (int)(u / nks), ks0 = (int)(u - (long long)t * nks);
             const long long ue = min(u1, (long long)(t + 1) * nks);
@@ -451,7 +464,9 @@ MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int
             for (int ks = ks0; ks < ks0 + (int)(ue - u); ++ks, ++g) {
                 const int stg = (int)(g % kI8Stages);
                 const uint32_t ph = (uint32_t)((g / kI8Stages) & 1);
+                const uint64_t tw = globaltimer_ns();
                 if (!mbar_wait(smem_u32(&L.empty[stg]), ph ^ 1u, F.gs, 210)) { ok = false; break; }
+                wait_empty += globaltimer_ns() - tw;
                 uint8_t* base = L.stages + (size_t)stg * kI8StageBytes;
                 const uint32_t fb = smem_u32(&L.full[stg]);
                 mbar_expect_tx(fb, (uint32_t)kI8StageBytes);
@@ -463,6 +478,8 @@ MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int
             }
             u = ue;
         }
+        i8_prof_add(prof, 20, wait_empty);
+        i8_prof_add(prof, 21, (unsigned long long)(u1 - u0));
         if (!ok) {   // let loads already in flight land before the CTA moves on
             for (long long q = g - kI8Stages; q < g; ++q) {
                 if (q < st.kb_done) continue;
@@ -471,16 +488,21 @@ MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int
         }
     } else if (warp == 5 && lane == 0) {
         long long g = st.kb_done, seg = st.tiles;
+        unsigned long long wait_full = 0, wait_free = 0;
         for (long long u = u0; u < u1 && ok; ++seg) {
             const int t = (int)(u / nks), ks0 = (int)(u - (long long)t * nks);
             const long long ue = min(u1, (long long)(t + 1) * nks);
             // the accumulators of the previous segment must be drained first
+            const uint64_t tf = globaltimer_ns();
             if (seg > 0 && !mbar_wait(smem_u32(L.tfree), (uint32_t)((seg - 1) & 1), F.gs, 214)) { ok = false; break; }
+            wait_free += globaltimer_ns() - tf;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             for (int ks = ks0; ks < ks0 + (int)(ue - u); ++ks, ++g) {
                 const int stg = (int)(g % kI8Stages);
                 const uint32_t ph = (uint32_t)((g / kI8Stages) & 1);
+                const uint64_t tw = globaltimer_ns();
                 if (!mbar_wait(smem_u32(&L.full[stg]), ph, F.gs, 211)) { ok = false; break; }
+                wait_full += globaltimer_ns() - tw;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t base = smem_u32(L.stages + (size_t)stg * kI8StageBytes);
 #pragma unroll
@@ -503,15 +525,22 @@ MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int
             if (ok) umma_commit(smem_u32(L.accum));
             u = ue;
         }
+        i8_prof_add(prof, 16, wait_full);
+        i8_prof_add(prof, 17, wait_free);
+        i8_prof_add(prof, 22, (unsigned long long)(seg - st.tiles));
     }
     if (warp < 4) {
         long long seg = st.tiles;
         const long long tfirst = u0 / nks;
+        unsigned long long wait_acc = 0, drain = 0;
         for (long long u = u0; u < u1; ++seg) {
             const int t = (int)(u / nks);
             const long long ue = min(u1, (long long)(t + 1) * nks);
-            bool w = ok && mbar_wait(smem_u32(L.accum), (uint32_t)(seg & 1), F.gs, 212);
+            const uint64_t ta0 = globaltimer_ns();
+            bool w = ok && mbar_wait(smem_u32(L.accum), (uint32_t)(seg & 1), F.gs, 212, 200);
             w = __all_sync(0xffffffffu, w);
+            const uint64_t ta1 = globaltimer_ns();
+            wait_acc += ta1 - ta0;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (!w) { ok = false; break; }
             const int row = warp * 32 + lane;
@@ -536,9 +565,12 @@ MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(L.tfree));
+            drain += globaltimer_ns() - ta1;
             u = ue;
         }
+        if (warp == 0 && lane == 0) { i8_prof_add(prof, 18, wait_acc); i8_prof_add(prof, 19, drain); }
     }
+    const uint64_t t_body = globaltimer_ns();
     // every role walked the same segment list
     {
         long long nseg = 0, nk = 0;
@@ -552,7 +584,9 @@ MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int
         st.tiles += nseg;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    return __syncthreads_and(ok ? 1 : 0) != 0;
+    const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
+    if (threadIdx.x == 0) { i8_prof_add(prof, 23, t_body - t_in); i8_prof_add(prof, 24, globaltimer_ns() - t_in); }
+    return all_ok;
 }
 
 // exact int64 demag sum of row lr of a tile for instance lj: the slots of the
