@@ -154,10 +154,11 @@ typedef struct mt_batch mt_batch;
 #define MT_PREC_BF16X2 2   /* tcgen05, K split hi+lo, m in BF16, 2 products, FP32 accumulate */
 #define MT_PREC_FP16X3S 3  /* tcgen05, rows of K scaled by powers of two, K and m split into FP16 hi+lo,
                               3 products, FP32 accumulate (about FP32 accuracy) */
-#define MT_PREC_INT8 4     /* tcgen05 kind::i8, rows of K as 24-bit fixed point (3 int8 limbs), m as
-                              rint(m 2^30) (4 limbs), all 12 limb products accumulated exactly in
+#define MT_PREC_INT8 4     /* tcgen05 kind::i8, rows of K as 32-bit fixed point (4 int8 limbs), m as
+                              rint(m 2^30) (4 limbs), all 16 limb products accumulated exactly in
                               int32/int64: the product is exact for the quantised operands, so it
-                              carries no rounding noise; needs |m| < 1.96 (MT_ERR_ARG otherwise) */
+                              carries no rounding noise; needs |m| < 1.96 (MT_ERR_ARG otherwise) and
+                              at most 10624 cells */
 
 int mt_batch_create(const mt_grid* grid, int B, int precision, mt_batch** out);
 int mt_batch_destroy(mt_batch* b);

@@ -870,15 +870,15 @@ MT_DEV void advance(BCtx& X, BInst& I, int b)
 // LL epilogue for one instance on the owned cells: sum the S partial demag
 // products and write f to the requested destination.
 // ---------------------------------------------------------------------------
-// exact demag field of cell i, instance b (int8 backend): -Ms_i 2^(-30-e_r) H_int
+// exact demag field of cell i, instance b (int8 backend): -Ms_i 2^(-30-e_r) RN(H_int)
 MT_DEV void i8_cell_field(const BCtx& X, int b, int i, double hm[3])
 {
     const double ms = (double)__ldg(&X.P.Mfact[i]);
     const int jl = b / kI8N - X.jb0;
     for (int a = 0; a < 3; ++a) {
         const int r = a * X.Q.np + i;
-        const long long h = i8_tile_sum(X.F.part, X.Q.maxseg, X.cov[a * 2 + jl], r & 127, b % kI8N);
-        hm[a] = xmul(-ms, xmul((double)h, __ldg(&X.Q.row_scale[r])));
+        const double h = i8_tile_sum(X.F.part, X.Q.maxseg, X.cov[a * 2 + jl], r & 127, b % kI8N);
+        hm[a] = xmul(-ms, xmul(h, __ldg(&X.Q.row_scale[r])));
     }
 }
 
@@ -1086,8 +1086,8 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
                 double h;
                 if (i8) {
                     const int r = a * Q.np + i;
-                    const long long v = i8_tile_sum(F.part, Q.maxseg, s_cov[a * 2 + b / kI8N - X.jb0], r & 127, b % kI8N);
-                    h = xmul(-(double)__ldg(&P.Mfact[i]), xmul((double)v, __ldg(&Q.row_scale[r])));
+                    const double v = i8_tile_sum(F.part, Q.maxseg, s_cov[a * 2 + b / kI8N - X.jb0], r & 127, b % kI8N);
+                    h = xmul(-(double)__ldg(&P.Mfact[i]), xmul(v, __ldg(&Q.row_scale[r])));
                 } else {
                     float acc = 0.f;
                     for (int sp = 0; sp < Q.S; ++sp)
@@ -1279,7 +1279,7 @@ __global__ void split_tensor_kernel(const float* __restrict__ K, int n, int ldk,
     }
 }
 
-// int8 tensor rows: 2^e_r puts the largest |K| of row r into [2^21, 2^22);
+// int8 tensor rows: 2^e_r puts the largest |K| of row r into [2^29, 2^30);
 // row_scale[r] = 2^(-30 - e_r) converts the exact limb sum back (0 for empty rows)
 __global__ void i8_row_kernel(const float* __restrict__ K, int n, int ldk, int np, int* __restrict__ row_exp,
                               double* __restrict__ row_scale)
@@ -1301,14 +1301,14 @@ __global__ void i8_row_kernel(const float* __restrict__ K, int n, int ldk, int n
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, red[w]);
         int e = 0;
         if (m > 0.f) frexpf(m, &e);                // m = f 2^e, f in [0.5, 1)
-        const int ex = (m > 0.f) ? 22 - e : 0;     // m 2^ex in [2^21, 2^22)
+        const int ex = (m > 0.f) ? 30 - e : 0;     // m 2^ex in [2^29, 2^30)
         row_exp[row] = ex;
         row_scale[row] = (m > 0.f) ? ldexp(1.0, -30 - ex) : 0.0;
     }
 }
 
-// FP32 cell-row tensor -> three int8 limbs [3][3np][Kd] of Kq = rint(K 2^e_r),
-// Kq = k0 2^16 + k1 2^8 + k2 (signed digits, k2 lowest), zero padded
+// FP32 cell-row tensor -> four int8 limbs [4][3np][Kd] of Kq = rint(K 2^e_r),
+// Kq = k0 2^24 + k1 2^16 + k2 2^8 + k3 (signed digits, k3 lowest), zero padded
 __global__ void i8_limb_kernel(const float* __restrict__ K, int n, int ldk, int np, const int* __restrict__ row_exp,
                                int8_t* __restrict__ klimb)
 {
@@ -1321,13 +1321,13 @@ __global__ void i8_limb_kernel(const float* __restrict__ K, int n, int ldk, int 
         float v = 0.f;
         if (i < n && j < n) v = K[((size_t)i * 6 + blk[a][bb]) * ldk + j];
         long long x = __double2ll_rn(ldexp((double)v, row_exp[row]));
-        const int k2 = (int)(signed char)(x & 0xff);
-        x = (x - k2) >> 8;
-        const int k1 = (int)(signed char)(x & 0xff);
-        x = (x - k1) >> 8;
+#pragma unroll
+        for (int l = 3; l >= 1; --l) {
+            const int d = (int)(signed char)(x & 0xff);
+            klimb[(size_t)l * tot + e] = (int8_t)d;
+            x = (x - d) >> 8;
+        }
         klimb[e] = (int8_t)x;
-        klimb[tot + e] = (int8_t)k1;
-        klimb[2 * tot + e] = (int8_t)k2;
     }
 }
 

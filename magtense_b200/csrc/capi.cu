@@ -510,7 +510,7 @@ struct mt_batch {
     uint16_t* khi = nullptr;
     uint16_t* klo = nullptr;
     float* row_inv = nullptr;
-    int8_t* klimb = nullptr;      // int8 backend: [3][3np][Kd]
+    int8_t* klimb = nullptr;      // int8 backend: [4][3np][Kd]
     double* row_scale = nullptr;  // [3np]
     double* hext = nullptr;
     double* alpha0 = nullptr;
@@ -594,10 +594,10 @@ int mt_batch_create(const mt_grid* g, int B, int precision, mt_batch** out)
     bt->grid = batch_grid(h->n, B, h->num_sms, precision, &bt->CB, &bt->IB, &bt->S);
     bt->np = bt->CB * kCellBlock;
     bt->Kd = 3 * bt->np;
-    if (precision == MT_PREC_INT8 && bt->Kd > 43000) {
-        // D_s sums up to three limb products of magnitude <= 2^14 over the k range in int32
+    if (precision == MT_PREC_INT8 && bt->Kd > 32000) {
+        // D_s sums up to four limb products of magnitude <= 2^14 over the k range in int32
         mt_batch_destroy(bt);
-        return fail(MT_ERR_UNSUPPORTED, "int8 precision supports up to 14336 cells");
+        return fail(MT_ERR_UNSUPPORTED, "int8 precision supports up to 10624 cells");
     }
     *out = bt;
     return MT_OK;
@@ -651,7 +651,7 @@ int mt_batch_assemble_demag(mt_batch* bt, void* stream)
     if (bt->prec == MT_PREC_INT8) {
         const size_t cnt = (size_t)bt->Kd * bt->Kd;
         if (!bt->klimb) {
-            CUDA_TRY(dalloc(&bt->klimb, 3 * cnt));
+            CUDA_TRY(dalloc(&bt->klimb, 4 * cnt));
             CUDA_TRY(dalloc(&bt->row_scale, (size_t)bt->Kd));
         }
         CUDA_TRY(launch_limb_tensor(bt->h->K, bt->h->n, bt->h->ldk, bt->np, bt->klimb, bt->row_scale,
@@ -744,7 +744,7 @@ int batch_alloc(mt_batch* bt, BatchRun& R, int nt, cudaStream_t s)
     memset(&R.maps, 0, sizeof(R.maps));
     if (bt->prec == MT_PREC_INT8) {
         int rc;
-        if ((rc = make_tmap_i8(&R.maps.ahi, bt->klimb, bt->Kd, bt->Kd, 3, 128))) return rc;
+        if ((rc = make_tmap_i8(&R.maps.ahi, bt->klimb, bt->Kd, bt->Kd, 4, 128))) return rc;
         if ((rc = make_tmap_i8(&R.maps.bhi, F.mlimb, bt->Kd, Bp, 4, kI8N))) return rc;
     } else if (bt->prec != MT_PREC_FP32) {
         int rc;
@@ -884,7 +884,7 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
         int max_persist = 0, max_win = 0;
         cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, h->device);
         cudaDeviceGetAttribute(&max_win, cudaDevAttrMaxAccessPolicyWindowSize, h->device);
-        const size_t want = (bt->prec == MT_PREC_INT8 ? 3 : 4) * (size_t)bt->Kd * bt->Kd;
+        const size_t want = 4 * (size_t)bt->Kd * bt->Kd;
         if (max_persist > 0 && max_win > 0 && cudaDeviceGetLimit(&prev_limit, cudaLimitPersistingL2CacheSize) == cudaSuccess) {
             const size_t lim = std::min(want, (size_t)max_persist);
             if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, lim) == cudaSuccess) {

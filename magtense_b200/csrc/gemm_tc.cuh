@@ -296,21 +296,23 @@ MT_DEV bool tc_gemm_tile_impl(unsigned char* smem, const QT& Q, const FT& F, con
 // Exact fixed-point demag product on the integer tensor pipe (kind::i8).
 //
 // Tensor row r (component a, cell i; 3np rows) is scaled by 2^e_r so that its
-// largest entry lies in [2^21, 2^22) and rounded to an integer Kq (|Kq| < 2^22),
-// written as three signed 8-bit limbs Kq = k0 2^16 + k1 2^8 + k2.  Every source
-// value m_j (|m_j| < 1.96) is rounded to mq = rint(m_j 2^30) and written as four
-// limbs mq = m0 2^24 + m1 2^16 + m2 2^8 + m3.  All twelve limb products are
-// accumulated exactly in int32 TMEM accumulators grouped by s = a + b (D_s,
-// columns 64 s .. 64 s + 63) and combined in int64 as
-// H = sum_s 2^(8 (5 - s)) D_s = sum_j Kq_rj mq_j, exactly: the sum over sources
-// carries no rounding, does not depend on the order or split of the k range,
-// and the field 2^(-30 - e_r) H is the same bit pattern on every run.
+// largest entry lies in [2^29, 2^30) and rounded to an integer Kq (|Kq| < 2^30),
+// written as four signed 8-bit limbs Kq = k0 2^24 + k1 2^16 + k2 2^8 + k3.
+// Every source value m_j (|m_j| < 1.96) is rounded to mq = rint(m_j 2^30) and
+// written as four limbs mq = m0 2^24 + m1 2^16 + m2 2^8 + m3.  All sixteen limb
+// products are accumulated exactly in int32 TMEM accumulators grouped by
+// s = a + b (D_s, columns 64 s .. 64 s + 63) and combined in two int64 parts,
+// Hhi = sum_{s<=3} 2^(8 (3 - s)) D_s and Hlo = sum_{s>=4} 2^(8 (6 - s)) D_s, so
+// that sum_j Kq_rj mq_j = 2^24 Hhi + Hlo exactly and neither part can
+// overflow: the sum over sources carries no rounding, does not depend on the
+// order or split of the k range, and the field 2^(-30 - e_r) RN(2^24 Hhi + Hlo)
+// is the same bit pattern on every run.
 //
 // Work split (Stream-K): tile = 128 tensor rows x 64 instances, unit = one
 // 64-wide k step of a tile; the units of all active tiles are split into
 // contiguous non-empty ranges, one per CTA, so every SM gets the same number of
 // MMAs.  A CTA's range covers pieces ("segments") of one or more tiles; each
-// segment's exact int64 partial goes to its own slot [CTA][segment][inst][row],
+// segment's exact int64 partials go to its own slot [CTA][segment][part][inst][row],
 // and the reader sums the slots of the CTAs that cover the tile.
 // ---------------------------------------------------------------------------
 constexpr int kI8Stages = 4;
@@ -318,9 +320,9 @@ constexpr int kI8KB = 64;                                    // int8 sources per
 constexpr int kI8N = 64;                                     // instances per tile (MMA N)
 constexpr int kI8ATile = 128 * kI8KB;                        // one 128-row K limb tile, 8 KB
 constexpr int kI8BTile = kI8N * kI8KB;                       // one 64-row m limb tile, 4 KB
-constexpr int kI8KLimbs = 3, kI8MLimbs = 4, kI8Acc = 6;
-constexpr int kI8StageBytes = kI8KLimbs * kI8ATile + kI8MLimbs * kI8BTile;   // 40 KB
-constexpr int kI8SlotElems = kI8N * 128;                     // int64 per segment slot
+constexpr int kI8KLimbs = 4, kI8MLimbs = 4, kI8Acc = 7;
+constexpr int kI8StageBytes = kI8KLimbs * kI8ATile + kI8MLimbs * kI8BTile;   // 48 KB
+constexpr int kI8SlotElems = 2 * kI8N * 128;                 // int64 per segment slot (hi and lo parts)
 // D S32 (2 at bit 4), A and B signed 8-bit (1 at bits 7 and 10), N = 64, M = 128
 constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | (((uint32_t)kI8N >> 3) << 17) | ((128u >> 4) << 24);
 
@@ -514,7 +516,7 @@ MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int
                         for (int b = 0; b < kI8MLimbs; ++b) {
                             const uint64_t bd = sdesc_sw64(base + kI8KLimbs * kI8ATile + b * kI8BTile + kk * 32);
                             // the first product into each accumulator of the segment overwrites it:
-                            // (0,b) opens s = 0..3, (1,3) opens s = 4, (2,3) opens s = 5
+                            // (0,b) opens s = 0..3, (1,3), (2,3), (3,3) open s = 4, 5, 6
                             const bool first = ks == ks0 && kk == 0 && (a == 0 || b == kI8MLimbs - 1);
                             umma_i8(st.tmem + (uint32_t)((a + b) * kI8N), ad, bd, first ? 0u : 1u);
                         }
@@ -550,17 +552,22 @@ MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int
                 long long h[32];
                 int d[32];
                 const uint32_t ta = st.tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(grp * 32);
-                tmem_ld32_i(ta, d);
-#pragma unroll
-                for (int k = 0; k < 32; ++k) h[k] = (long long)d[k];
 #pragma unroll 1
-                for (int s = 1; s < kI8Acc; ++s) {
-                    tmem_ld32_i(ta + (uint32_t)(s * kI8N), d);
+                for (int part = 0; part < 2; ++part) {
+                    // part 0: D0..D3 (hi), part 1: D4..D6 (lo)
+                    const int s0 = part ? 4 : 0, s1 = part ? kI8Acc : 4;
+                    tmem_ld32_i(ta + (uint32_t)(s0 * kI8N), d);
 #pragma unroll
-                    for (int k = 0; k < 32; ++k) h[k] = h[k] * 256 + (long long)d[k];
+                    for (int k = 0; k < 32; ++k) h[k] = (long long)d[k];
+#pragma unroll 1
+                    for (int s = s0 + 1; s < s1; ++s) {
+                        tmem_ld32_i(ta + (uint32_t)(s * kI8N), d);
+#pragma unroll
+                        for (int k = 0; k < 32; ++k) h[k] = h[k] * 256 + (long long)d[k];
+                    }
+#pragma unroll
+                    for (int k = 0; k < 32; ++k) slot[(size_t)part * kI8N * 128 + (size_t)(grp * 32 + k) * 128 + row] = h[k];
                 }
-#pragma unroll
-                for (int k = 0; k < 32; ++k) slot[(size_t)(grp * 32 + k) * 128 + row] = h[k];
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
@@ -589,12 +596,18 @@ MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int
     return all_ok;
 }
 
-// exact int64 demag sum of row lr of a tile for instance lj: the slots of the
-// CTAs cv.first..cv.last that cover the tile
-MT_DEV long long i8_tile_sum(const long long* part, int maxseg, const SkCover& cv, int lr, int lj)
+// exact demag sum of row lr of a tile for instance lj, rounded once to double:
+// the hi and lo parts of the slots of the CTAs cv.first..cv.last that cover the
+// tile are summed exactly in int64 and combined as RN(2^24 hi + lo)
+MT_DEV double i8_tile_sum(const long long* part, int maxseg, const SkCover& cv, int lr, int lj)
 {
-    const size_t off = (size_t)lj * 128 + (size_t)lr;
-    long long acc = __ldcg(&part[((size_t)cv.first * maxseg + (size_t)cv.jf) * kI8SlotElems + off]);
-    for (int c = cv.first + 1; c <= cv.last; ++c) acc += __ldcg(&part[(size_t)c * maxseg * kI8SlotElems + off]);
-    return acc;
+    const size_t off = (size_t)lj * 128 + (size_t)lr, lo = (size_t)kI8N * 128;
+    const long long* p0 = part + ((size_t)cv.first * maxseg + (size_t)cv.jf) * kI8SlotElems + off;
+    long long hi_s = __ldcg(p0), lo_s = __ldcg(p0 + lo);
+    for (int c = cv.first + 1; c <= cv.last; ++c) {
+        const long long* pc = part + (size_t)c * maxseg * kI8SlotElems + off;
+        hi_s += __ldcg(pc);
+        lo_s += __ldcg(pc + lo);
+    }
+    return __dadd_rn(__dmul_rn((double)hi_s, 16777216.0), (double)lo_s);
 }

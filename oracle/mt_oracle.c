@@ -32,9 +32,9 @@
  * FP32 demag product; mode 1 ("fp64") keeps the tensor and the product in
  * FP64 and serves the error statements against FP64; mode 2 ("int8") is the
  * exact fixed-point product of the GPU's int8 backend, restated from its
- * definition (rows of the FP32 tensor as 24-bit fixed point in three int8
- * limbs, m as rint(m 2^30) in four limbs, all twelve limb products summed
- * exactly), so the GPU must reproduce it bit for bit.
+ * definition (rows of the FP32 tensor as 32-bit fixed point in four int8
+ * limbs, m as rint(m 2^30) in four limbs, all sixteen limb products summed
+ * exactly, one rounding to double), so the GPU must reproduce it bit for bit.
  *
  * Summation order of the FP32 demag product follows the reference BLAS SGEMV
  * column sweep (y(i) += (-x(j))*A(i,j), j = 1..n, one block after the other);
@@ -281,7 +281,7 @@ typedef struct {
     int renorm;                       /* per-cell |m| renormalisation after accepted steps */
     float* ms;                        /* FP32 copy of m for the demag product */
     long nrhs;
-    /* mode 2: limbs [3][3n][3n] of the fixed-point tensor rows, 2^(-30-e_r) per row */
+    /* mode 2: limbs [4][3n][3n] of the fixed-point tensor rows, 2^(-30-e_r) per row */
     signed char* klimb;
     double* row_scale;
     int* mlimb;                       /* [4][3n] limbs of the current m */
@@ -346,15 +346,15 @@ void or_problem_destroy(or_problem* p)
 int or_problem_range_err(const or_problem* p) { return p->range_err; }
 
 /* mode 2 tensor limbs from the FP32 tensor: row r = (a, i), column (b, j).
- * 2^e_r puts the row's largest |K| in [2^21, 2^22); Kq = rint(K 2^e_r) =
- * k0 2^16 + k1 2^8 + k2 with signed 8-bit digits (k2 the lowest);
+ * 2^e_r puts the row's largest |K| in [2^29, 2^30); Kq = rint(K 2^e_r) =
+ * k0 2^24 + k1 2^16 + k2 2^8 + k3 with signed 8-bit digits (k3 the lowest);
  * row_scale = 2^(-30 - e_r). */
 static void or_i8_build(or_problem* p)
 {
     const int n = p->n, n3 = 3 * n;
     static const int blk[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
     const size_t tot = (size_t)n3 * n3;
-    p->klimb = (signed char*)malloc(3 * tot);
+    p->klimb = (signed char*)malloc(4 * tot);
     p->row_scale = (double*)malloc(sizeof(double) * n3);
     p->mlimb = (int*)malloc(sizeof(int) * 4 * (size_t)n3);
 #pragma omp parallel for schedule(static)
@@ -368,27 +368,27 @@ static void or_i8_build(or_problem* p)
             }
         int e = 0;
         if (mx > 0.0f) frexpf(mx, &e);
-        const int ex = (mx > 0.0f) ? 22 - e : 0;
+        const int ex = (mx > 0.0f) ? 30 - e : 0;
         p->row_scale[r] = (mx > 0.0f) ? ldexp(1.0, -30 - ex) : 0.0;
         for (int b = 0; b < 3; ++b)
             for (int j = 0; j < n; ++j) {
                 const float v = p->K32[((size_t)blk[a][b] * n + i) * (size_t)n + j];
                 long long x = llrint(ldexp((double)v, ex));
-                const int k2 = (int)(signed char)(x & 0xff);
-                x = (x - k2) >> 8;
-                const int k1 = (int)(signed char)(x & 0xff);
-                x = (x - k1) >> 8;
                 const size_t e2 = (size_t)r * n3 + (size_t)b * n + j;
+                for (int l = 3; l >= 1; --l) {
+                    const int d = (int)(signed char)(x & 0xff);
+                    p->klimb[(size_t)l * tot + e2] = (signed char)d;
+                    x = (x - d) >> 8;
+                }
                 p->klimb[e2] = (signed char)x;
-                p->klimb[tot + e2] = (signed char)k1;
-                p->klimb[2 * tot + e2] = (signed char)k2;
             }
     }
 }
 
-/* mode 2 demag field: Hm = -Ms_i * 2^(-30-e_r) * H_int with the exact
- * H_int = sum_j Kq_rj mq_j = sum_s 2^(8(5-s)) D_s, D_s = sum_j sum_{a+b=s} k_a m_b
- * (all twelve limb products), converted to double once */
+/* mode 2 demag field: Hm = -Ms_i * 2^(-30-e_r) * RN(H_int) with the exact
+ * H_int = sum_j Kq_rj mq_j = sum_s 2^(8(6-s)) D_s, D_s = sum_j sum_{a+b=s} k_a m_b
+ * (all sixteen limb products), kept as 2^24 Hhi + Hlo (Hhi from D0..D3, Hlo
+ * from D4..D6) so that no int64 overflows, and rounded to double once */
 static void or_i8_demag(or_problem* p, const double* m, double* Hm)
 {
     const int n = p->n, n3 = 3 * n;
@@ -410,8 +410,8 @@ static void or_i8_demag(or_problem* p, const double* m, double* Hm)
     }
 #pragma omp parallel for schedule(static)
     for (int r = 0; r < n3; ++r) {
-        int D[6] = {0, 0, 0, 0, 0, 0};
-        for (int a = 0; a < 3; ++a)
+        int D[7] = {0, 0, 0, 0, 0, 0, 0};
+        for (int a = 0; a < 4; ++a)
             for (int b = 0; b < 4; ++b) {
                 const signed char* kr = p->klimb + (size_t)a * tot + (size_t)r * n3;
                 const int* mr = ml + (size_t)b * n3;
@@ -419,10 +419,13 @@ static void or_i8_demag(or_problem* p, const double* m, double* Hm)
                 for (int j = 0; j < n3; ++j) acc += (int)kr[j] * mr[j];
                 D[a + b] += acc;
             }
-        long long h = (long long)D[0];
-        for (int s2 = 1; s2 < 6; ++s2) h = h * 256 + (long long)D[s2];
+        long long hi = (long long)D[0];
+        for (int s2 = 1; s2 < 4; ++s2) hi = hi * 256 + (long long)D[s2];
+        long long lo = (long long)D[4];
+        for (int s2 = 5; s2 < 7; ++s2) lo = lo * 256 + (long long)D[s2];
+        const double h = (double)hi * 16777216.0 + (double)lo;
         const int i = r % n;
-        Hm[r] = (-(double)p->Mfact[i]) * ((double)h * p->row_scale[r]);
+        Hm[r] = (-(double)p->Mfact[i]) * (h * p->row_scale[r]);
     }
 }
 

@@ -149,7 +149,7 @@ class Problem:
     mode 0 ("ref"): FP32 tensor and FP32 demag product, as the reference.
     mode 1 ("fp64"): FP64 tensor and FP64 product.
     mode 2 ("int8"): the exact fixed-point product of the int8 backend, from
-    the FP32 tensor (24-bit rows, m as rint(m 2^30), twelve limb products).
+    the FP32 tensor (32-bit rows, m as rint(m 2^30), sixteen limb products).
     """
 
     def __init__(self, res, L, *, solver=2, mode=0, A0=1.3e-11, Ms=8e5, K0=0.0, u_ea=None,

@@ -6,7 +6,8 @@ agree to 2 FP32 ulp only).  The product is exact, so the demag field must
 match the oracle bit for bit, whatever the Stream-K split of the k range; the
 whole right-hand side then matches too, and so do the per-instance RKSUITE
 trajectories.  Accuracy against the FP64 tensor and product: 2e-5 of the
-largest component (24-bit fixed-point tensor rows)."""
+largest component (32-bit fixed-point tensor rows; the FP32 tensor the rows
+are made from carries most of it)."""
 import numpy as np
 import pytest
 

@@ -213,8 +213,8 @@ def test_demag_ref_and_fp64_agree(oracle):
 
 
 def test_demag_int8_is_the_exact_fixed_point_product(oracle):
-    # mode 2 (twelve int8 limb products) must equal the plain definition
-    # -Ms 2^(-30-e_r) sum_j rint(K_rj 2^e_r) rint(m_j 2^30), computed here with numpy int64
+    # mode 2 (sixteen int8 limb products) must equal the plain definition
+    # -Ms 2^(-30-e_r) RN(sum_j rint(K_rj 2^e_r) rint(m_j 2^30)), computed here with Python integers
     res, L = [10, 4, 2], [50e-9, 20e-9, 10e-9]
     n = 80
     rng = np.random.default_rng(7)
@@ -225,12 +225,12 @@ def test_demag_int8_is_the_exact_fixed_point_product(oracle):
     Kfull = np.block([[K32[blk[a][b]] for b in range(3)] for a in range(3)])      # rows (a,i), cols (b,j)
     rowmax = np.abs(Kfull).max(axis=1)
     _, e = np.frexp(rowmax)
-    ex = 22 - e
+    ex = 30 - e
     Kq = np.rint(np.ldexp(Kfull.astype(np.float64), ex[:, None])).astype(np.int64)
-    assert np.abs(Kq).max() < 2**22 and np.abs(Kq).max(axis=1).min() >= 2**21
+    assert np.abs(Kq).max() < 2**30 and np.abs(Kq).max(axis=1).min() >= 2**29
     mq = np.rint(m.reshape(-1) * 2.0**30).astype(np.int64)
-    Hint = Kq @ mq                                                       # |terms| < 2^53, exact in int64
-    Hdef = -8e5 * (Hint.astype(np.float64) * np.ldexp(1.0, -30 - ex))
+    Hint = Kq.astype(object) @ mq.astype(object)                         # exact big integers
+    Hdef = -8e5 * (np.array([float(h) for h in Hint]) * np.ldexp(1.0, -30 - ex))
     P2 = oracle.Problem(res, L, mode=2, K32=K32)
     H2 = P2.fields(0, m)[3].reshape(-1)
     np.testing.assert_array_equal(H2, Hdef)
