@@ -109,6 +109,16 @@ int mt_fields(mt_handle* h, double t, const double* m_dev, double* Hj_dev, doubl
 /* dm/dt of the Landau-Lifshitz equation (dmdt_fct :220-273). */
 int mt_rhs(mt_handle* h, double t, const double* m_dev, double* dmdt_dev, void* stream);
 
+/* Vector-Jacobian product of mt_rhs at (t, m) for the cotangent lam (3n): the
+ * gradient with respect to m (gm, 3n), the cotangent of the internal field
+ * he = Hh + Hj + Hm + Hk (ghe, 3n; the applied-field gradient is -sum over
+ * cells of ghe) and the gradient with respect to the per-cell Ms (gms, n).
+ * The demag and exchange operators are symmetric, so their transposes run the
+ * forward kernels.  No counterpart in the reference (it has no derivatives);
+ * used by the adjoint of a trajectory (magtense_b200.adjoint). */
+int mt_rhs_vjp(mt_handle* h, double t, const double* m_dev, const double* lam_dev, double* gm_dev,
+               double* ghe_dev, double* gms_dev, void* stream);
+
 /* Allocation-free dm/dt.  No counterpart in the reference: it exists for
  * callers that may not allocate device memory (for example code running while
  * a CUDA graph is captured, or a host framework that owns all device memory

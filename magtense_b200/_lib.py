@@ -66,6 +66,7 @@ SIGNATURES = {
     "mt_demag_field": [VP, VP, VP, VP],
     "mt_fields": [VP, C.c_double, VP, VP, VP, VP, VP, VP],
     "mt_rhs": [VP, C.c_double, VP, VP, VP],
+    "mt_rhs_vjp": [VP, C.c_double, VP, VP, VP, VP, VP, VP],
     "mt_rhs_noalloc": [VP, C.c_double, VP, VP, VP],
     "mt_integrate": [VP, D, C.c_int, VP, C.c_double, C.c_double, D, C.c_int, C.c_double, D, VP, I,
                      C.POINTER(Stats), VP],

@@ -1430,8 +1430,7 @@ cudaError_t launch_batch(const DevProb& P, const BatchBufs& Bf, const BatchParam
     TcMaps m;
     memset(&m, 0, sizeof(m));
     if (tmaps) memcpy(&m, tmaps, sizeof(m));
-    cudaLaunchConfig_t cfg;
-    memset(&cfg, 0, sizeof(cfg));
+    cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
     cfg.blockDim = dim3(kBatchThreads);
     cfg.dynamicSmemBytes = smem;

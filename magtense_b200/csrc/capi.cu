@@ -74,6 +74,9 @@ struct mt_handle {
     float* K = nullptr; bool have_K = false;
     // scratch
     float* m32 = nullptr;
+    double* vjp_buf = nullptr;   // [lam (3n) | g_Ms (n)]
+    double* vjp_z = nullptr;     // Jfact g_he (3n)
+    float* vjp_v32 = nullptr;    // Ms g_he, FP32 [3][ldk] (padding stays 0)
 };
 
 namespace {
@@ -170,6 +173,7 @@ int mt_destroy(mt_handle* h)
     if (!h) return MT_OK;
     free_ptr(h->Jfact); free_ptr(h->Kfact); free_ptr(h->Mfact); free_ptr(h->A6);
     free_ptr(h->hext); free_ptr(h->alpha_tab); free_ptr(h->K); free_ptr(h->m32);
+    free_ptr(h->vjp_buf); free_ptr(h->vjp_z); free_ptr(h->vjp_v32);
     delete h;
     return MT_OK;
 }
@@ -309,6 +313,30 @@ int mt_rhs(mt_handle* h, double t, const double* m_dev, double* dmdt_dev, void* 
     DevProb P = make_prob(h);
     CUDA_TRY(launch_m_to_f32(m_dev, h->n, h->ldk, h->m32, s));
     CUDA_TRY(launch_field(2, P, m_dev, h->m32, t, dmdt_dev, nullptr, nullptr, nullptr, nullptr, 0.f, h->num_sms, s));
+    return MT_OK;
+}
+
+int mt_rhs_vjp(mt_handle* h, double t, const double* m_dev, const double* lam_dev, double* gm_dev, double* ghe_dev,
+               double* gms_dev, void* stream)
+{
+    int rc = check_ready(h, true, true);
+    if (rc) return rc;
+    if (!m_dev || !lam_dev || !gm_dev || !ghe_dev || !gms_dev) return fail(MT_ERR_ARG, "null device pointer");
+    if ((rc = ensure_m32(h))) return rc;
+    const size_t n = (size_t)h->n;
+    if (!h->vjp_buf) {
+        CUDA_TRY(dalloc(&h->vjp_buf, 4 * n));
+        CUDA_TRY(dalloc(&h->vjp_z, 3 * n));
+        CUDA_TRY(dalloc(&h->vjp_v32, 3 * (size_t)h->ldk));
+        CUDA_TRY(cudaMemset(h->vjp_v32, 0, sizeof(float) * 3 * (size_t)h->ldk));
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    DevProb P = make_prob(h);
+    CUDA_TRY(launch_m_to_f32(m_dev, h->n, h->ldk, h->m32, s));
+    CUDA_TRY(cudaMemcpyAsync(h->vjp_buf, lam_dev, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(launch_field(4, P, m_dev, h->m32, t, gm_dev, h->vjp_z, ghe_dev, h->vjp_buf, h->vjp_v32, 0.f, h->num_sms, s));
+    CUDA_TRY(launch_field(5, P, m_dev, h->vjp_v32, t, gm_dev, h->vjp_z, nullptr, nullptr, nullptr, 0.f, h->num_sms, s));
+    CUDA_TRY(cudaMemcpyAsync(gms_dev, h->vjp_buf + 3 * n, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     return MT_OK;
 }
 

@@ -28,6 +28,49 @@ __global__ void pack3_f32_kernel(const float* __restrict__ x, const float* __res
     m32[e] = (i < n) ? src[i] : 0.0f;
 }
 
+// Vector-Jacobian product of dm/dt = -gamma c - alpha (m x c), c = he x m
+// (he = hh + hj + hm + hk, the internal field of cell_rhs) for a cotangent lam:
+// with u = he x m and w = -gamma lam - alpha (lam x m),
+//   d/dhe = m x w,   d/dm (through the cross products) = w x he - alpha (u x lam).
+// The field terms then add (all three operators are symmetric):
+//   exchange  hj = -2 Jfact L m        ->  -2 L (Jfact g_he)       (mode 5)
+//   demag     hm = -Ms K m (FP32 K)    ->  -K (Ms g_he)            (mode 5, same streaming product)
+//   anisotropy hk = -2 Kfact A m       ->  -2 Kfact A g_he         (here)
+//   Zeeman    hh = -hext(t)            ->  d/dhext = -sum_i g_he   (by the caller)
+//   per-cell Ms: d hm/dMs = -K m, d hj/dMs = -hj/Ms, d hk/dMs = -hk/Ms.
+MT_DEV void cell_vjp(const DevProb& P, const double* m, int i, const float S[3], const TimeScalars& ts,
+                     const double* lam, double gm[3], double ghe[3], double* gms)
+{
+    const int n = P.n;
+    CellFields F = cell_fields(P, m, i, S, ts);
+    const double mv[3] = {ldcg(&m[i]), ldcg(&m[n + i]), ldcg(&m[2 * n + i])};
+    const double lv[3] = {lam[i], lam[n + i], lam[2 * n + i]};
+    double he[3], u[3], w[3], lxm[3], wxh[3], uxl[3];
+    for (int a = 0; a < 3; ++a) he[a] = F.hh[a] + F.hj[a] + F.hm[a] + F.hk[a];
+    auto cross = [](const double* x, const double* y, double* z) {
+        z[0] = x[1] * y[2] - x[2] * y[1];
+        z[1] = x[2] * y[0] - x[0] * y[2];
+        z[2] = x[0] * y[1] - x[1] * y[0];
+    };
+    cross(he, mv, u);
+    cross(lv, mv, lxm);
+    for (int a = 0; a < 3; ++a) w[a] = -P.gamma * lv[a] - ts.alpha * lxm[a];
+    cross(mv, w, ghe);
+    cross(w, he, wxh);
+    cross(u, lv, uxl);
+    const double k2 = -2.0 * __ldg(&P.Kfact[i]);
+    const double A[6] = {__ldg(&P.A6[0 * (size_t)n + i]), __ldg(&P.A6[1 * (size_t)n + i]),
+                         __ldg(&P.A6[2 * (size_t)n + i]), __ldg(&P.A6[3 * (size_t)n + i]),
+                         __ldg(&P.A6[4 * (size_t)n + i]), __ldg(&P.A6[5 * (size_t)n + i])};
+    const double Ag[3] = {A[0] * ghe[0] + A[1] * ghe[1] + A[2] * ghe[2], A[1] * ghe[0] + A[3] * ghe[1] + A[4] * ghe[2],
+                          A[2] * ghe[0] + A[4] * ghe[1] + A[5] * ghe[2]};
+    for (int a = 0; a < 3; ++a) gm[a] = wxh[a] - ts.alpha * uxl[a] + k2 * Ag[a];
+    const double ms = (double)__ldg(&P.Mfact[i]);
+    double g = 0.0;
+    for (int a = 0; a < 3; ++a) g += ghe[a] * (-(double)S[a] - F.hj[a] / ms - F.hk[a] / ms);
+    *gms = g;
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(kFieldThreads)
 field_kernel(DevProb P, const double* __restrict__ m, const float* __restrict__ m32, double t, int cells_per_cta,
@@ -50,6 +93,16 @@ field_kernel(DevProb P, const double* __restrict__ m, const float* __restrict__ 
         }
         return;
     }
+    if (MODE == 5) {   // VJP, second pass: m32 holds Ms g_he; o1 holds Jfact g_he; o0 += -K(Ms g_he) - 2 L(Jfact g_he)
+        for (int cell = threadIdx.x; cell < nc; cell += blockDim.x) {
+            const int i = c0 + cell;
+            for (int a = 0; a < 3; ++a) {
+                const double lz = lap_cell_dev(P, o1 + (size_t)a * n, i);
+                o0[(size_t)a * n + i] += -(double)sm_S[cell * 3 + a] - 2.0 * lz;
+            }
+        }
+        return;
+    }
     const TimeScalars ts = time_scalars(P, t);
     for (int cell = threadIdx.x; cell < nc; cell += blockDim.x) {
         const int i = c0 + cell;
@@ -64,6 +117,19 @@ field_kernel(DevProb P, const double* __restrict__ m, const float* __restrict__ 
                 o2[(size_t)a * n + i] = F.hk[a];
                 o3[(size_t)a * n + i] = F.hm[a];
             }
+        } else if (MODE == 4) {   // VJP, first pass: o3 = [lam (3n) | g_Ms (n)]; o0 = g_m (local part),
+                                  // o1 = Jfact g_he, o2 = g_he, h32 = Ms g_he (FP32, [3][ldk])
+            double gm[3], ghe[3], gms;
+            cell_vjp(P, m, i, &sm_S[cell * 3], ts, o3, gm, ghe, &gms);
+            const double jf = __ldg(&P.Jfact[i]);
+            const float ms = __ldg(&P.Mfact[i]);
+            for (int a = 0; a < 3; ++a) {
+                o0[(size_t)a * n + i] = gm[a];
+                o1[(size_t)a * n + i] = jf * ghe[a];
+                o2[(size_t)a * n + i] = ghe[a];
+                h32[(size_t)a * P.ldk + i] = (float)((double)ms * ghe[a]);
+            }
+            o3[3 * (size_t)n + i] = gms;
         } else {
             double o[3];
             cell_rhs(P, m, i, &sm_S[cell * 3], ts, o);
@@ -116,6 +182,8 @@ cudaError_t launch_field(int mode, const DevProb& P, const double* m, const floa
         case 1: MT_LAUNCH(1); break;
         case 2: MT_LAUNCH(2); break;
         case 3: MT_LAUNCH(3); break;
+        case 4: MT_LAUNCH(4); break;
+        case 5: MT_LAUNCH(5); break;
         default: return cudaErrorInvalidValue;
     }
 #undef MT_LAUNCH

@@ -8,7 +8,8 @@ cudaError_t launch_m_to_f32(const double* m, int n, int ldk, float* m32, cudaStr
 cudaError_t launch_pack3_f32(const float* x, const float* y, const float* z, int n, int ldk, float* m32,
                              cudaStream_t s);
 int field_cells_per_cta(int n, int num_sms);
-// mode 0: internal demag field (o0); 1: Hj,Hh,Hk,Hm (o0..o3); 2: dm/dt (o0); 3: pref*K*m32 -> h32 (FP32)
+// mode 0: internal demag field (o0); 1: Hj,Hh,Hk,Hm (o0..o3); 2: dm/dt (o0); 3: pref*K*m32 -> h32 (FP32);
+// 4, 5: the two passes of the vector-Jacobian product of dm/dt (see fields.cu)
 cudaError_t launch_field(int mode, const DevProb& P, const double* m, const float* m32, double t, double* o0,
                          double* o1, double* o2, double* o3, float* h32, float pref, int num_sms, cudaStream_t s);
 

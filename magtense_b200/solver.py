@@ -138,6 +138,19 @@ class Solver:
             check(_lib.lib().mt_rhs(self._h, float(t), _dptr(m), _dptr(out), _stream(stream)), "mt_rhs")
         return out
 
+    def rhs_vjp(self, t, m, lam, stream=None):
+        """Vector-Jacobian product of rhs at (t, m) for the cotangent lam (3n):
+        returns (d/dm (3n), d/dhe (3n), d/dMs (n)); d/dhext = -(d/dhe).reshape(3, n).sum(1)."""
+        m = self._vec(m)
+        lam = self._vec(lam)
+        gm = torch.empty(3 * self.n, dtype=torch.float64, device=self.device)
+        ghe = torch.empty_like(gm)
+        gms = torch.empty(self.n, dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            check(_lib.lib().mt_rhs_vjp(self._h, float(t), _dptr(m), _dptr(lam), _dptr(gm), _dptr(ghe), _dptr(gms),
+                                        _stream(stream)), "mt_rhs_vjp")
+        return gm, ghe, gms
+
     # ---------------------------------------------------------------- integrate
     def integrate(self, t, m0, *, tol=1e-4, thres=1e-6, t_conv=None, conv_tol=1e-4, y_out=None, stream=None):
         """MagTense_ODE_RKSuite on the device.
