@@ -18,4 +18,7 @@ def __getattr__(name):
     if name in ("Solver", "BatchSolver", "grid_points"):
         from . import solver
         return getattr(solver, name)
+    if name in ("TrajectoryProblem", "mean_m_trajectory", "LLTrajectory"):
+        from . import adjoint
+        return getattr(adjoint, name)
     raise AttributeError(name)
