@@ -1,0 +1,209 @@
+"""The adjoint gradient of a Landau-Lifshitz trajectory (the differentiation
+configuration, on its 20x5x1 subgrid): piecewise-constant in-plane applied
+field (10 segments of 10 ps), per-cell Ms ~ U[7.5e5, 8.5e5] A/m, loss
+sum_t (<m_x>(t) - target(t))^2 with a seeded three-sinusoid target of
+amplitude 0.5, fixed-step RK4 (dt = 0.5 ps).
+
+- The vector-Jacobian product of the device right-hand side (mt_rhs_vjp)
+  against central differences of mt_rhs in m, the applied field and Ms.
+- The trajectory gradient against central differences of the device forward
+  pass (1e-3 relative), and against torch autograd of a plain FP64 torch
+  right-hand side (FP64 tensor from the oracle) on the same RK4 scheme (1e-2:
+  the device forward keeps the reference's FP32 demag product).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+MU0 = 4 * np.pi * 1e-7
+GAMMA = 2.211e5
+RES, L = (20, 5, 1), (125e-9, 31.25e-9, 3e-9)
+N = 100
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    torch.cuda.set_device(0)
+    return torch
+
+
+def config(seed=4):
+    rng = np.random.default_rng(seed)
+    S = 10
+    hseg = np.zeros((S, 3))
+    hseg[:, :2] = rng.uniform(-20e-3, 20e-3, (S, 2)) / MU0
+    Ms = rng.uniform(7.5e5, 8.5e5, N)
+    m0 = np.ones((3, N)) / np.sqrt(3) + 0.01 * rng.standard_normal((3, N))
+    m0 /= np.linalg.norm(m0, axis=0)
+    a = rng.uniform(0.0, 0.5 / 3, 3)
+    w = rng.uniform(2 * np.pi * 5e9, 2 * np.pi * 30e9, 3)
+    ph = rng.uniform(0, 2 * np.pi, 3)
+    return hseg, Ms, m0.reshape(-1), (a, w, ph)
+
+
+def target(t, tg):
+    a, w, ph = tg
+    return (a[None, :] * np.sin(w[None, :] * t[:, None] + ph[None, :])).sum(1)
+
+
+def problem(m0):
+    from magtense_b200 import TrajectoryProblem
+    return TrajectoryProblem(RES, L, gamma=GAMMA, alpha=GAMMA * 0.02, m0=m0, t_seg=10e-12, steps_per_segment=20,
+                             sample_every=10, checkpoint_every=50)
+
+
+def loss_of(samples, tgt):
+    return ((samples[:, 0] - tgt) ** 2).sum()
+
+
+def test_rhs_vjp_matches_central_differences(torch_cuda):
+    from magtense_b200 import Solver
+    torch = torch_cuda
+    rng = np.random.default_rng(7)
+    axis = rng.standard_normal(3)
+    axis /= np.linalg.norm(axis)
+    Ms = rng.uniform(7.5e5, 8.5e5, N)
+    s = Solver(RES, L, K0=4e3, u_ea=np.tile(axis, (N, 1)), Ms=Ms)
+    s.assemble()
+    h = np.array([8e3, -5e3, 1e3])
+    s.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.1, hext=np.array([[0.0, *h], [1e-9, *h]]))
+    m = rng.standard_normal((3, N))
+    m /= np.linalg.norm(m, axis=0)
+    m = torch.as_tensor(m.reshape(-1), device="cuda")
+    lam = torch.as_tensor(rng.standard_normal(3 * N), device="cuda")
+    t = 0.3e-9
+    gm, ghe, gms = s.rhs_vjp(t, m, lam)
+    f = lambda mm: float((s.rhs(t, mm) * lam).sum())
+    # direction in m
+    v = torch.as_tensor(rng.standard_normal(3 * N), device="cuda")
+    eps = 1e-2
+    fd = (f(m + eps * v) - f(m - eps * v)) / (2 * eps)
+    adj = float((gm * v).sum())
+    assert abs(fd - adj) <= 2e-3 * abs(adj), (fd, adj)
+    # applied field (x component)
+    eh = 20.0
+    def f_h(dh):
+        hh = h + np.array([dh, 0.0, 0.0])
+        s.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.1, hext=np.array([[0.0, *hh], [1e-9, *hh]]))
+        return f(m)
+    fd = (f_h(eh) - f_h(-eh)) / (2 * eh)
+    adj = float(-ghe.reshape(3, N)[0].sum())
+    assert abs(fd - adj) <= 2e-3 * abs(adj), (fd, adj)
+    s.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.1, hext=np.array([[0.0, *h], [1e-9, *h]]))
+    # per-cell Ms along a random direction
+    wv = rng.standard_normal(N)
+    em = 500.0
+    def f_ms(d):
+        s.set_material(1.3e-11, Ms + d * wv, 4e3, np.tile(axis, (N, 1)))
+        return f(m)
+    fd = (f_ms(em) - f_ms(-em)) / (2 * em)
+    adj = float((gms.cpu().numpy() * wv).sum())
+    assert abs(fd - adj) <= 2e-3 * abs(adj), (fd, adj)
+    s.close()
+
+
+def fp64_reference_gradient(torch, oracle, hseg, Ms, m0, tgt_vals, prob):
+    """Gradient of the same loss by torch autograd of a plain FP64 RHS and the same RK4 scheme."""
+    _, K64 = oracle.assemble(list(RES), list(L), fp32=False, fp64=True)
+    blk = [[0, 1, 2], [1, 3, 4], [2, 4, 5]]
+    K = torch.as_tensor(np.block([[K64[blk[a][b]] for b in range(3)] for a in range(3)]), device="cuda")
+    nx, ny, nz = RES
+    d = [L[0] / nx, L[1] / ny, L[2] / nz]
+    mu0 = (4.0 * np.pi) * 1e-7
+
+    def lap(m):
+        g = m.reshape(3, nz, ny, nx)
+        out = torch.zeros_like(g)
+        for ax, (nn, dd) in zip((3, 2, 1), zip((nx, ny, nz), d)):
+            if nn < 2:
+                continue
+            lo = torch.cat([g.narrow(ax, 0, 1), g.narrow(ax, 0, nn - 1)], dim=ax)
+            hi = torch.cat([g.narrow(ax, 1, nn - 1), g.narrow(ax, nn - 1, 1)], dim=ax)
+            out = out + (lo - 2 * g + hi) / (dd * dd)
+        return out.reshape(3, -1)
+
+    hs = torch.tensor(hseg, device="cuda", requires_grad=True)
+    ms = torch.tensor(Ms, device="cuda", requires_grad=True)
+
+    def rhs(m, h):
+        Jf = 1.3e-11 / (mu0 * ms)
+        he = -h[:, None] - 2 * Jf * lap(m) - ms * (K @ m.reshape(-1)).reshape(3, -1)
+        c = torch.cross(he, m, dim=0)
+        return -GAMMA * c - prob.alpha * torch.cross(m, c, dim=0)
+
+    m = torch.as_tensor(m0.reshape(3, -1), device="cuda")
+    dt = prob.dt
+    samples = []
+    for k in range(hseg.shape[0] * prob.steps_per_segment):
+        h = hs[k // prob.steps_per_segment]
+        k1 = rhs(m, h)
+        k2 = rhs(m + 0.5 * dt * k1, h)
+        k3 = rhs(m + 0.5 * dt * k2, h)
+        k4 = rhs(m + dt * k3, h)
+        m = m + (dt / 6.0) * (k1 + 2 * k2 + 2 * k3 + k4)
+        if (k + 1) % prob.sample_every == 0:
+            samples.append(m.mean(dim=1))
+    loss = loss_of(torch.stack(samples), torch.as_tensor(tgt_vals, device="cuda"))
+    gh, gm = torch.autograd.grad(loss, (hs, ms))
+    return gh.cpu().numpy(), gm.cpu().numpy(), float(loss)
+
+
+def test_adjoint_gradient_matches_fp64_autograd(torch_cuda, oracle):
+    from magtense_b200 import mean_m_trajectory
+    torch = torch_cuda
+    hseg, Ms, m0, tg = config()
+    prob = problem(m0)
+    nsamp = hseg.shape[0] * prob.steps_per_segment // prob.sample_every
+    t_s = prob.dt * prob.sample_every * np.arange(1, nsamp + 1)
+    tgt = target(t_s, tg)
+    hs = torch.tensor(hseg, device="cuda", requires_grad=True)
+    ms = torch.tensor(Ms, device="cuda", requires_grad=True)
+    loss = loss_of(mean_m_trajectory(hs, ms, prob), torch.as_tensor(tgt, device="cuda"))
+    loss.backward()
+    gh_ref, gm_ref, loss_ref = fp64_reference_gradient(torch, oracle, hseg, Ms, m0, tgt, prob)
+    print(f"\nloss: device FP32-demag {float(loss):.9e}, FP64 reference {loss_ref:.9e}")
+    assert abs(float(loss) - loss_ref) <= 1e-3 * abs(loss_ref)
+    eh = np.linalg.norm(hs.grad.cpu().numpy() - gh_ref) / np.linalg.norm(gh_ref)
+    em = np.linalg.norm(ms.grad.cpu().numpy() - gm_ref) / np.linalg.norm(gm_ref)
+    print(f"\nadjoint vs FP64 autograd: field {eh:.2e}, Ms {em:.2e}")
+    # the device forward runs the reference's FP32 demag product, which moves <m>(t) by ~2e-5
+    # against the FP64 model at alpha_G = 0.02: the gradients agree to a few 1e-3 (measured
+    # 2.6e-3 for the field, 5.2e-3 for Ms); the adjoint itself is held to 1e-3 against
+    # central differences of its own forward pass below
+    assert eh <= 1e-2 and em <= 1e-2, (eh, em)
+
+
+def test_adjoint_gradient_matches_central_differences(torch_cuda):
+    from magtense_b200 import mean_m_trajectory
+    torch = torch_cuda
+    hseg, Ms, m0, tg = config()
+    prob = problem(m0)
+    nsamp = hseg.shape[0] * prob.steps_per_segment // prob.sample_every
+    tgt = torch.as_tensor(target(prob.dt * prob.sample_every * np.arange(1, nsamp + 1), tg), device="cuda")
+    hs = torch.tensor(hseg, device="cuda", requires_grad=True)
+    ms = torch.tensor(Ms, device="cuda", requires_grad=True)
+    loss_of(mean_m_trajectory(hs, ms, prob), tgt).backward()
+
+    def L_at(h, m):
+        with torch.no_grad():
+            return float(loss_of(mean_m_trajectory(torch.as_tensor(h, device="cuda"),
+                                                   torch.as_tensor(m, device="cuda"), prob), tgt))
+
+    checks = []
+    for (k, c) in [(2, 0), (7, 1)]:
+        e = 0.01 * 20e-3 / MU0
+        hp, hm = hseg.copy(), hseg.copy()
+        hp[k, c] += e
+        hm[k, c] -= e
+        checks.append(((L_at(hp, Ms) - L_at(hm, Ms)) / (2 * e), float(hs.grad[k, c])))
+    for i in (13, 71):
+        e = 0.01 * Ms[i]
+        mp, mm = Ms.copy(), Ms.copy()
+        mp[i] += e
+        mm[i] -= e
+        checks.append(((L_at(hseg, mp) - L_at(hseg, mm)) / (2 * e), float(ms.grad[i])))
+    print("\ncentral differences vs adjoint:", [f"{a:.6e}/{b:.6e}" for a, b in checks])
+    for fd, adj in checks:
+        assert abs(fd - adj) <= 1e-3 * max(abs(adj), 1e-3 * max(abs(x[1]) for x in checks)), (fd, adj)
