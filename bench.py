@@ -13,11 +13,14 @@ for the std-problem-4 dataset workflow.  One step = every instance of the
 rank integrated over the window.
 
 Other workloads: "film-plain" (the same film, single-instance FP32 path) and
+"adjoint" (the differentiation configuration: forward and adjoint backward of
+a 2 ns fixed-step RK4 trajectory of the film with 200 piecewise-constant field
+segments and per-cell Ms) and
 "large-plain" (64x64x8 cubes of 5 nm, n = 32768, 25.8 GB FP32 tensor, the
 HBM-bound demag matvec).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload film-batch|film-plain|large-plain]
+                  [--workload film-batch|film-plain|large-plain|adjoint]
 
 Multi-GPU: one process per GPU (torchrun); instances are sharded across ranks
 with no data-path collective ("scaling": "weak"); the step time is the max over
@@ -55,7 +58,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="film-batch", choices=["film-batch", "film-plain", "large-plain"])
+    ap.add_argument("--workload", default="film-batch", choices=["film-batch", "film-plain", "large-plain", "adjoint"])
     ap.add_argument("--instances", type=int, default=256, help="instances per rank (film-batch)")
     ap.add_argument("--precision", default="int8", choices=["int8", "fp16s", "bf16x3", "bf16x2", "fp32"])
     ap.add_argument("--plain-sample", type=int, default=4,
@@ -235,11 +238,14 @@ def run_ours(args):
     line = None
     if args.workload == "film-batch":
         line = bench_film_batch(torch, args, ws, rank, local, dist, hbm, bf16_sus, src)
+    elif args.workload == "adjoint":
+        line = bench_adjoint(torch, args, ws, rank, local, dist, hbm, src)
     else:
         line = bench_plain(torch, args, ws, rank, local, dist, hbm, src)
     if rank == 0 and line is not None:
         if not args.no_cpu:
-            line["cpu_baseline"] = cpu_reference_sample(args.cpu_window, args.workload)
+            line["cpu_baseline"] = (cpu_adjoint_sample(args.cpu_window) if args.workload == "adjoint" else
+                                    cpu_reference_sample(args.cpu_window, args.workload))
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -356,6 +362,140 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
         line["e2e"] = {"value": sim_ns / (e2e_red / 1e3), "unit": "simulated ns/s",
                        "h2d_bytes_per_step": B * 3 * n * 8, "d2h_bytes_per_step": B * nt * 3 * n * 8}
     return line
+
+
+def adjoint_config(seed):
+    """The differentiation configuration: per-cell Ms ~ U[7.5e5, 8.5e5] A/m, 200 field
+    segments over 2 ns with in-plane components ~ U[-20, 20] mT, a seeded three-sinusoid
+    target of amplitude 0.5 for <m_x>(t), config-0 start state."""
+    rng = np.random.default_rng(seed)
+    n = int(np.prod(FILM_RES))
+    S = 200
+    hseg = np.zeros((S, 3))
+    hseg[:, :2] = rng.uniform(-20e-3, 20e-3, (S, 2)) / MU0
+    Ms = rng.uniform(7.5e5, 8.5e5, n)
+    tg = (rng.uniform(0.0, 0.5 / 3, 3), rng.uniform(2 * np.pi * 1e9, 2 * np.pi * 10e9, 3), rng.uniform(0, 2 * np.pi, 3))
+    return hseg, Ms, start_state(n), tg
+
+
+def adjoint_target(t, tg):
+    a, w, ph = tg
+    return (a[None, :] * np.sin(w[None, :] * t[:, None] + ph[None, :])).sum(1)
+
+
+def cpu_adjoint_sample(window_ns):
+    """Torch FP64 autograd of a plain right-hand side (FP64 tensor from the oracle) on the
+    host cores, same RK4 scheme, on the first window_ns of the trajectory."""
+    import torch
+    from oracle import oracle as O
+    hseg, Ms, m0, tg = adjoint_config(4)
+    res, L = FILM_RES, FILM_L
+    n = int(np.prod(res))
+    _, K64 = O.assemble(list(res), list(L), fp32=False, fp64=True)
+    blk = [[0, 1, 2], [1, 3, 4], [2, 4, 5]]
+    K = torch.as_tensor(np.block([[K64[blk[a][b]] for b in range(3)] for a in range(3)]))
+    nx, ny, _ = res
+    d = [L[0] / nx, L[1] / ny]
+    mu0 = (4.0 * np.pi) * 1e-7
+
+    def lap(m):
+        g = m.reshape(3, ny, nx)
+        out = torch.zeros_like(g)
+        for ax, nn, dd in ((2, nx, d[0]), (1, ny, d[1])):
+            lo = torch.cat([g.narrow(ax, 0, 1), g.narrow(ax, 0, nn - 1)], dim=ax)
+            hi = torch.cat([g.narrow(ax, 1, nn - 1), g.narrow(ax, nn - 1, 1)], dim=ax)
+            out = out + (lo - 2 * g + hi) / (dd * dd)
+        return out.reshape(3, -1)
+
+    dt, spseg, every = 1e-12, 10, 10
+    steps = int(round(window_ns * 1e-9 / dt))
+    hs = torch.tensor(hseg, requires_grad=True)
+    ms = torch.tensor(Ms, requires_grad=True)
+
+    def rhs(m, h):
+        he = -h[:, None] - 2 * (1.3e-11 / (mu0 * ms)) * lap(m) - ms * (K @ m.reshape(-1)).reshape(3, -1)
+        c = torch.cross(he, m, dim=0)
+        return -GAMMA * c - GAMMA * 0.02 * torch.cross(m, c, dim=0)
+
+    t0 = time.perf_counter()
+    m = torch.as_tensor(m0.reshape(3, -1))
+    samples = []
+    for k in range(steps):
+        h = hs[k // spseg]
+        k1 = rhs(m, h)
+        k2 = rhs(m + 0.5 * dt * k1, h)
+        k3 = rhs(m + 0.5 * dt * k2, h)
+        k4 = rhs(m + dt * k3, h)
+        m = m + (dt / 6.0) * (k1 + 2 * k2 + 2 * k3 + k4)
+        if (k + 1) % every == 0:
+            samples.append(m.mean(dim=1))
+    tt = dt * every * np.arange(1, len(samples) + 1)
+    loss = ((torch.stack(samples)[:, 0] - torch.as_tensor(adjoint_target(tt, tg))) ** 2).sum()
+    loss.backward()
+    dtw = time.perf_counter() - t0
+    return {"value": window_ns / dtw, "unit": "simulated ns/s", "cores": torch.get_num_threads(), "kind": "port",
+            "sample": f"{window_ns} ns of the 80x20x1 trajectory, forward and backward by torch FP64 autograd on the "
+                      f"host ({steps} RK4 steps, {dtw:.1f} s); the reference itself computes no gradients"}
+
+
+def bench_adjoint(torch, args, ws, rank, local, dist, hbm, src):
+    from magtense_b200 import TrajectoryProblem, mean_m_trajectory
+    n = int(np.prod(FILM_RES))
+    hseg, Ms, m0, tg = adjoint_config(4 + rank)
+    prob = TrajectoryProblem(FILM_RES, FILM_L, gamma=GAMMA, alpha=GAMMA * 0.02, m0=m0, t_seg=10e-12,
+                             steps_per_segment=10, sample_every=10, checkpoint_every=50)
+    window = 2.0
+    steps = hseg.shape[0] * prob.steps_per_segment
+    tt = prob.dt * prob.sample_every * np.arange(1, steps // prob.sample_every + 1)
+    tgt = torch.as_tensor(adjoint_target(tt, tg), device="cuda")
+    hs_host, ms_host = torch.as_tensor(hseg), torch.as_tensor(Ms)
+    out = {}
+
+    def step():
+        hs = hs_host.to("cuda").requires_grad_(True)
+        ms = ms_host.to("cuda").requires_grad_(True)
+        loss = ((mean_m_trajectory(hs, ms, prob)[:, 0] - tgt) ** 2).sum()
+        loss.backward()
+        out["g"] = (hs.grad, ms.grad)
+        return [{"f_evals": 0, "kernel_ms": 0.0, "launches": 0}]
+
+    times, _, clocks, flush = timed_steps(torch, step, args.steps, args.warmup, dist, local)
+    e2e = []
+    for _ in range(max(1, args.steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        step()
+        gh, gm = out["g"][0].cpu(), out["g"][1].cpu()
+        torch.cuda.synchronize()
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    step_ms, e2e_ms = max_over_ranks(torch, dist, [max(times), statistics.median(e2e)])
+    if rank != 0:
+        return None
+    # right-hand sides per step: forward 4 RK4 stages; backward 4 recomputed stages plus 4
+    # vector-Jacobian products (each two streaming demag passes)
+    rhs_like = steps * (4 + 4 + 2 * 4)
+    achieved = 24.0 * n * n * rhs_like / (step_ms / 1e3) / 1e9
+    sim_ns = ws * window
+    return {
+        "metric": "simulated ns/s", "value": sim_ns / (step_ms / 1e3), "unit": "simulated ns/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 (FP32 demag)", "data": "synthetic",
+        "config": {"workload": "adjoint: 80x20x1 film, per-cell Ms ~ U[7.5e5, 8.5e5], 200 piecewise-constant "
+                               "in-plane field segments over 2 ns ~ U[-20, 20] mT, loss sum_t (<m_x> - target)^2, "
+                               "fixed-step RK4 dt = 1 ps, checkpoints every 50 steps; one step = forward + adjoint "
+                               "backward (gradients for the 600 field values and 1600 Ms values)",
+                   "window_ns": window, "rk4_steps": steps, "parallelism": f"one trajectory per rank, {ws} rank(s)",
+                   "l2": "flushed (256 MB write) before every timed step"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None,
+                     "note": f"field_kernel streaming demag: 24*n^2 bytes x {rhs_like} products per step over the "
+                             f"whole step time (launch- and latency-bound at n = 1600: the 61 MB tensor sits in L2); "
+                             f"peak {src} HBM copy"},
+        "e2e": {"value": sim_ns / (e2e_ms / 1e3), "unit": "simulated ns/s",
+                "h2d_bytes_per_step": (hseg.size + Ms.size) * 8, "d2h_bytes_per_step": (hseg.size + Ms.size) * 8},
+        "gpu_launches": int(steps * (4 * 2 + 4 * 2 + 4 * 2)),
+        "clocks": clocks,
+    }
 
 
 def bench_plain(torch, args, ws, rank, local, dist, hbm, src):
