@@ -119,6 +119,20 @@ int mt_rhs(mt_handle* h, double t, const double* m_dev, double* dmdt_dev, void* 
 int mt_rhs_vjp(mt_handle* h, double t, const double* m_dev, const double* lam_dev, double* gm_dev,
                double* ghe_dev, double* gms_dev, void* stream);
 
+/* Ragged batch: ninst independent instances, each with its own handle (grid,
+ * tensor, material, dynamics), integrated like mt_integrate over the same
+ * output times in ONE cooperative launch (relaunched in slices of about 0.25 s).
+ * Instance k runs on its own group of CTAs, sized by its demag work n_k^2, with
+ * its own barrier and adaptive steps; ninst must not exceed the SM count.
+ * m0_dev[k], y_out_dev[k] (nt * 3 n_k): device buffers of instance k; t_out,
+ * flags: ninst * nt; stats: ninst (launches and kernel_ms in stats[0]).
+ * options: MT_RAGGED_GRAPH captures the launch sequence in a CUDA graph once
+ * and replays it.  No counterpart in the reference (one problem per process). */
+#define MT_RAGGED_GRAPH 1
+int mt_integrate_ragged(mt_handle* const* hs, int ninst, const double* t, int nt, const double* const* m0_dev,
+                        double tol, double thres, double* t_out, double* const* y_out_dev, int* flags,
+                        mt_stats* stats, int options, void* stream);
+
 /* Allocation-free dm/dt.  No counterpart in the reference: it exists for
  * callers that may not allocate device memory (for example code running while
  * a CUDA graph is captured, or a host framework that owns all device memory

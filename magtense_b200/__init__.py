@@ -15,7 +15,7 @@ def __getattr__(name):
     if name in ("MicromagProblem", "load_demag_tensor", "save_demag_tensor"):
         from . import micromag
         return getattr(micromag, name)
-    if name in ("Solver", "BatchSolver", "grid_points"):
+    if name in ("Solver", "BatchSolver", "grid_points", "integrate_ragged"):
         from . import solver
         return getattr(solver, name)
     if name in ("TrajectoryProblem", "mean_m_trajectory", "LLTrajectory"):

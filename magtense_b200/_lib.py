@@ -68,6 +68,8 @@ SIGNATURES = {
     "mt_rhs": [VP, C.c_double, VP, VP, VP],
     "mt_rhs_vjp": [VP, C.c_double, VP, VP, VP, VP, VP, VP],
     "mt_rhs_noalloc": [VP, C.c_double, VP, VP, VP],
+    "mt_integrate_ragged": [C.POINTER(VP), C.c_int, D, C.c_int, C.POINTER(VP), C.c_double, C.c_double, D,
+                            C.POINTER(VP), I, C.POINTER(Stats), C.c_int, VP],
     "mt_integrate": [VP, D, C.c_int, VP, C.c_double, C.c_double, D, C.c_int, C.c_double, D, VP, I,
                      C.POINTER(Stats), VP],
     "mt_batch_create": [C.POINTER(Grid), C.c_int, C.c_int, C.POINTER(VP)],

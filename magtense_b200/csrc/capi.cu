@@ -14,6 +14,7 @@
 #include <mutex>
 #include <string>
 #include <vector>
+#include <memory>
 
 #include "../../include/magtense_b200.h"
 #include "common.cuh"
@@ -366,15 +367,28 @@ struct IntegAlloc {
 
 extern "C" {
 
-int mt_integrate(mt_handle* h, const double* t, int nt, const double* m0_dev, double tol, double thres,
-                 const double* t_conv, int nt_conv, double conv_tol, double* t_out, double* y_out_dev, int* flags,
-                 mt_stats* stats, void* stream)
+}  // extern "C"
+
+namespace {
+
+// One instance's integration state on the device: RKSUITE buffers, parameters and outputs.
+struct IntegRun {
+    IntegAlloc A;
+    IntegBufs B;
+    IntegParams Q;
+    DevProb P;
+    double* d_tout = nullptr;
+    int* d_flags = nullptr;
+    int grid = 0;
+    size_t smem = 0;
+};
+
+// setup_r1 checks, merged output/convergence times, buffers and the initial RKSUITE
+// state of one instance, to be integrated by a group of `grid` CTAs
+int integ_prepare(mt_handle* h, const double* t, int nt, const double* m0_dev, double tol, double thres,
+                  const double* t_conv, int nt_conv, double conv_tol, double* y_out_dev, int grid, IntegRun& R,
+                  mt_stats* stats, cudaStream_t s)
 {
-    int rc = check_ready(h, true, true);
-    if (rc) return rc;
-    if (!t || nt < 2 || !m0_dev || !t_out || !y_out_dev || !stats) return fail(MT_ERR_ARG, "bad argument (nt >= 2 required)");
-    if (nt_conv < 0 || (nt_conv > 0 && !t_conv)) return fail(MT_ERR_ARG, "bad convergence-time list");
-    cudaStream_t s = (cudaStream_t)stream;
     memset(stats, 0, sizeof(*stats));
     stats->converged_at = -1;
     const int n = h->n, n3 = 3 * n;
@@ -409,8 +423,8 @@ int mt_integrate(mt_handle* h, const double* t, int nt, const double* m0_dev, do
     }
 
     // ---- buffers ----
-    IntegAlloc A;
-    IntegBufs B;
+    IntegAlloc& A = R.A;
+    IntegBufs& B = R.B;
     memset(&B, 0, sizeof(B));
     for (int k = 0; k < 4; ++k) {
         CUDA_TRY(A.get(&B.pool[k], n3));
@@ -425,11 +439,12 @@ int mt_integrate(mt_handle* h, const double* t, int nt, const double* m0_dev, do
     CUDA_TRY(A.get(&B.ylast, n3));
     CUDA_TRY(A.get(&B.ystep, n3));
     B.y_out = y_out_dev;
-    const int grid = integrate_grid_size(n, h->num_sms);
     CUDA_TRY(A.get(&B.partials, 2 * (size_t)grid * 4));
     CUDA_TRY(A.get(&B.gs, 1));
     CUDA_TRY(A.get(&B.state, 1));
-    double* d_comb = nullptr; int* d_cflags = nullptr; double* d_tout = nullptr; int* d_flags = nullptr;
+    double* d_comb = nullptr; int* d_cflags = nullptr;
+    double*& d_tout = R.d_tout;
+    int*& d_flags = R.d_flags;
     CUDA_TRY(A.get(&d_comb, comb.size()));
     CUDA_TRY(A.get(&d_cflags, comb.size()));
     CUDA_TRY(A.get(&d_tout, nt));
@@ -458,7 +473,7 @@ int mt_integrate(mt_handle* h, const double* t, int nt, const double* m0_dev, do
     st.converged_at = -1;
     CUDA_TRY(cudaMemcpyAsync(B.state, &st, sizeof(st), cudaMemcpyHostToDevice, s));
 
-    IntegParams Q;
+    IntegParams& Q = R.Q;
     memset(&Q, 0, sizeof(Q));
     Q.thres = thres; Q.round_off = round_off; Q.sqrrmc = sqrrmc; Q.cubrmc = cubrmc; Q.sqtiny = sqtiny;
     Q.toosml = toosml; Q.conv_tol = conv_tol;
@@ -473,8 +488,59 @@ int mt_integrate(mt_handle* h, const double* t, int nt, const double* m0_dev, do
     }
     // co-residency of the persistent grid
     const size_t smem = integrate_smem_bytes(n, h->ldk, grid);
+    R.smem = smem;
     if (smem > 227 * 1024) return fail(MT_ERR_UNSUPPORTED, "integrator shared memory %zu exceeds 227 KB", smem);
-    DevProb P = make_prob(h);
+    R.P = make_prob(h);
+    R.grid = grid;
+    return MT_OK;
+}
+
+// outputs and statistics of a finished instance
+int integ_finish(IntegRun& R, const RKS& hs, const double* t, int nt, double* t_out, int* flags, mt_stats* stats)
+{
+    std::vector<int> fl(nt);
+    const double* d_tout = R.d_tout;
+    const int* d_flags = R.d_flags;
+    CUDA_TRY(cudaMemcpy(t_out, d_tout, sizeof(double) * nt, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(fl.data(), d_flags, sizeof(int) * nt, cudaMemcpyDeviceToHost));
+    t_out[0] = t[0];
+    fl[0] = 0;
+    if (flags) memcpy(flags, fl.data(), sizeof(int) * nt);
+    stats->f_evals = hs.full_f_count + hs.f_count;
+    stats->steps = hs.step_count;
+    stats->bad_steps = hs.bad_step_count;
+    stats->n_flag3 = hs.n_flag3;
+    stats->n_flag4 = hs.n_flag4;
+    stats->n_out = hs.ko;
+    stats->status = hs.status;
+    stats->converged_at = hs.converged_at;
+    if (hs.status != 0) return fail(MT_ERR_SOLVER, "integrator stopped with RKSUITE flag %d", hs.status);
+    return MT_OK;
+}
+
+
+
+}  // namespace
+
+extern "C" {
+
+int mt_integrate(mt_handle* h, const double* t, int nt, const double* m0_dev, double tol, double thres,
+                 const double* t_conv, int nt_conv, double conv_tol, double* t_out, double* y_out_dev, int* flags,
+                 mt_stats* stats, void* stream)
+{
+    int rc = check_ready(h, true, true);
+    if (rc) return rc;
+    if (!t || nt < 2 || !m0_dev || !t_out || !y_out_dev || !stats) return fail(MT_ERR_ARG, "bad argument (nt >= 2 required)");
+    if (nt_conv < 0 || (nt_conv > 0 && !t_conv)) return fail(MT_ERR_ARG, "bad convergence-time list");
+    cudaStream_t s = (cudaStream_t)stream;
+    IntegRun R;
+    int prc = integ_prepare(h, t, nt, m0_dev, tol, thres, t_conv, nt_conv, conv_tol, y_out_dev,
+                            integrate_grid_size(h->n, h->num_sms), R, stats, s);
+    if (prc) return prc;
+    DevProb P = R.P;
+    IntegBufs& B = R.B;
+    IntegParams& Q = R.Q;
+    const int grid = R.grid;
     RKS hs;
     long long last_evals = -1;
     int last_ci = -1;
@@ -507,24 +573,158 @@ int mt_integrate(mt_handle* h, const double* t, int nt, const double* m0_dev, do
         last_evals = evals;
         last_ci = hs.ci;
     }
-    std::vector<int> fl(nt);
-    CUDA_TRY(cudaMemcpy(t_out, d_tout, sizeof(double) * nt, cudaMemcpyDeviceToHost));
-    CUDA_TRY(cudaMemcpy(fl.data(), d_flags, sizeof(int) * nt, cudaMemcpyDeviceToHost));
-    t_out[0] = t[0];
-    fl[0] = 0;
-    if (flags) memcpy(flags, fl.data(), sizeof(int) * nt);
-    stats->f_evals = hs.full_f_count + hs.f_count;
-    stats->steps = hs.step_count;
-    stats->bad_steps = hs.bad_step_count;
-    stats->n_flag3 = hs.n_flag3;
-    stats->n_flag4 = hs.n_flag4;
-    stats->n_out = hs.ko;
-    stats->status = hs.status;
-    stats->converged_at = hs.converged_at;
-    if (hs.status != 0) return fail(MT_ERR_SOLVER, "integrator stopped with RKSUITE flag %d", hs.status);
-    return MT_OK;
+    return integ_finish(R, hs, t, nt, t_out, flags, stats);
 }
 
+
+int mt_integrate_ragged(mt_handle* const* hs, int ninst, const double* t, int nt, const double* const* m0_dev,
+                        double tol, double thres, double* t_out, double* const* y_out_dev, int* flags, mt_stats* stats,
+                        int options, void* stream)
+{
+    if (!hs || ninst < 1 || !t || nt < 2 || !m0_dev || !t_out || !y_out_dev || !stats)
+        return fail(MT_ERR_ARG, "bad argument (ninst >= 1, nt >= 2 required)");
+    int rc;
+    for (int k = 0; k < ninst; ++k) {
+        if (!hs[k] || !m0_dev[k] || !y_out_dev[k]) return fail(MT_ERR_ARG, "null handle or buffer of instance %d", k);
+        if ((rc = check_ready(hs[k], true, true))) return rc;
+        if (hs[k]->device != hs[0]->device) return fail(MT_ERR_ARG, "all instances must live on one device");
+    }
+    const int G = hs[0]->num_sms;
+    if (ninst > G) return fail(MT_ERR_UNSUPPORTED, "%d instances exceed the %d SMs of one launch", ninst, G);
+    // CTA groups in proportion to the demag work n^2, at least one CTA, at most n/8
+    std::vector<double> w(ninst);
+    double wsum = 0.0;
+    for (int k = 0; k < ninst; ++k) { w[k] = (double)hs[k]->n * (double)hs[k]->n; wsum += w[k]; }
+    std::vector<int> ncta(ninst), cap(ninst);
+    int used = 0;
+    for (int k = 0; k < ninst; ++k) {
+        cap[k] = integrate_grid_size(hs[k]->n, G);
+        ncta[k] = std::min(cap[k], std::max(1, (int)((double)G * w[k] / wsum)));
+        used += ncta[k];
+    }
+    while (used > G) {   // the floor of one CTA each can overshoot: take from the largest group
+        int j = (int)(std::max_element(ncta.begin(), ncta.end()) - ncta.begin());
+        ncta[j]--; used--;
+    }
+    for (bool grew = true; grew && used < G;) {   // hand out the rest to the most loaded groups
+        grew = false;
+        int j = -1;
+        double best = 0.0;
+        for (int k = 0; k < ninst; ++k)
+            if (ncta[k] < cap[k] && w[k] / ncta[k] > best) { best = w[k] / ncta[k]; j = k; }
+        if (j >= 0) { ncta[j]++; used++; grew = true; }
+    }
+    cudaStream_t cs = (cudaStream_t)stream;
+    std::vector<std::unique_ptr<IntegRun>> runs(ninst);
+    size_t smem = 0;
+    std::vector<RaggedInst> tab(ninst);
+    std::vector<int> cta_inst(used);
+    int c0 = 0;
+    for (int k = 0; k < ninst; ++k) {
+        runs[k].reset(new IntegRun());
+        if ((rc = integ_prepare(hs[k], t, nt, m0_dev[k], tol, thres, nullptr, 0, 0.0, y_out_dev[k], ncta[k], *runs[k],
+                                &stats[k], cs)))
+            return rc;
+        smem = std::max(smem, runs[k]->smem);
+        // about 0.25 s per launch for this group: 24 n^2 bytes per evaluation over ncta SMs
+        const double t_eval = 24.0 * (double)hs[k]->n * (double)hs[k]->ldk / (ncta[k] * 30.0e9) + 15e-6;
+        runs[k]->Q.evals_per_launch = std::min(100000LL, std::max(64LL, (long long)(0.25 / t_eval)));
+        tab[k].P = runs[k]->P; tab[k].B = runs[k]->B; tab[k].Q = runs[k]->Q;
+        tab[k].cta0 = c0; tab[k].ncta = ncta[k];
+        for (int j = 0; j < ncta[k]; ++j) cta_inst[c0 + j] = k;
+        c0 += ncta[k];
+    }
+    IntegAlloc A;
+    RaggedInst* d_tab = nullptr;
+    int* d_cta = nullptr;
+    CUDA_TRY(A.get(&d_tab, (size_t)ninst));
+    CUDA_TRY(A.get(&d_cta, (size_t)used));
+    CUDA_TRY(cudaMemcpyAsync(d_tab, tab.data(), sizeof(RaggedInst) * ninst, cudaMemcpyHostToDevice, cs));
+    CUDA_TRY(cudaMemcpyAsync(d_cta, cta_inst.data(), sizeof(int) * used, cudaMemcpyHostToDevice, cs));
+    // pinned read-back of every instance's barrier and RKSUITE state after a launch
+    struct Back { GridSync gs; RKS st; };
+    Back* back = nullptr;
+    CUDA_TRY(cudaMallocHost((void**)&back, sizeof(Back) * ninst));
+    struct HostFree { void* p; ~HostFree() { cudaFreeHost(p); } } hf{back};
+    // private stream (the caller's may be the legacy default stream, which cannot be captured)
+    cudaStream_t s = nullptr;
+    CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamDestroy(s); } } sg{s};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evc = nullptr;
+    CUDA_TRY(cudaEventCreate(&ev0));
+    CUDA_TRY(cudaEventCreate(&ev1));
+    CUDA_TRY(cudaEventCreateWithFlags(&evc, cudaEventDisableTiming));
+    struct EvGuard { cudaEvent_t a, b, c; ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); cudaEventDestroy(c); } }
+        evg{ev0, ev1, evc};
+    CUDA_TRY(cudaEventRecord(evc, cs));
+    CUDA_TRY(cudaStreamWaitEvent(s, evc, 0));
+    auto enqueue = [&]() -> cudaError_t {
+        cudaError_t e = cudaSuccess;
+        for (int k = 0; k < ninst && e == cudaSuccess; ++k) e = cudaMemsetAsync(runs[k]->B.gs, 0, sizeof(GridSync), s);
+        if (e == cudaSuccess) e = launch_integrate_ragged(d_tab, d_cta, used, smem, s);
+        for (int k = 0; k < ninst && e == cudaSuccess; ++k) {
+            e = cudaMemcpyAsync(&back[k].gs, runs[k]->B.gs, sizeof(GridSync), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(&back[k].st, runs[k]->B.state, sizeof(RKS), cudaMemcpyDeviceToHost, s);
+        }
+        return e;
+    };
+    cudaGraphExec_t gexec = nullptr;
+    struct GraphGuard { cudaGraphExec_t g; ~GraphGuard() { if (g) cudaGraphExecDestroy(g); } } gg{nullptr};
+    if (options & MT_RAGGED_GRAPH) {
+        cudaGraph_t graph = nullptr;
+        CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = enqueue();
+        cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            return fail(MT_ERR_CUDA, "capturing the ragged launch: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+        }
+        e = cudaGraphInstantiate(&gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return fail(MT_ERR_CUDA, "instantiating the ragged launch: %s", cudaGetErrorString(e));
+        gg.g = gexec;
+    }
+    double kernel_ms = 0.0;
+    long long launches = 0;
+    std::vector<long long> last(ninst, -1);
+    for (;;) {
+        CUDA_TRY(cudaEventRecord(ev0, s));
+        if (gexec) CUDA_TRY(cudaGraphLaunch(gexec, s));
+        else CUDA_TRY(enqueue());
+        CUDA_TRY(cudaEventRecord(ev1, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        float ms = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, ev0, ev1));
+        kernel_ms += ms;
+        launches++;
+        bool all = true, progress = false;
+        for (int k = 0; k < ninst; ++k) {
+            const Back& bk = back[k];
+            if (bk.gs.err != 0 || bk.gs.abort)
+                return fail(MT_ERR_TIMEOUT, "instance %d: group barrier gave up (code %d at %d)", k, bk.gs.err,
+                            bk.gs.err_where);
+            if (!bk.st.finished) all = false;
+            const long long sig = bk.st.full_f_count + bk.st.f_count + bk.st.ci;
+            if (sig != last[k]) progress = true;
+            last[k] = sig;
+        }
+        if (all) break;
+        if (!progress) return fail(MT_ERR_SOLVER, "ragged integrator made no progress");
+    }
+    CUDA_TRY(cudaEventRecord(evc, s));
+    CUDA_TRY(cudaStreamWaitEvent(cs, evc, 0));
+    int worst = MT_OK;
+    for (int k = 0; k < ninst; ++k) {
+        const int r = integ_finish(*runs[k], back[k].st, t, nt, t_out + (size_t)k * nt, flags ? flags + (size_t)k * nt : nullptr,
+                                   &stats[k]);
+        if (r && worst == MT_OK) worst = r;
+    }
+    stats[0].launches = launches;
+    stats[0].kernel_ms = kernel_ms;
+    return worst;
+}
 
 // ---------------------------------------------------------------------------
 // batched instances

@@ -45,7 +45,9 @@ MT_DEV uint64_t globaltimer_ns()
 constexpr long long kSpinLimit = 20000000LL;
 constexpr uint64_t kTimeoutNs = 4000000000ULL;
 
-MT_DEV bool grid_sync(GridSync* gs, int where)
+// The same for a group of nctas CTAs that share one GridSync (the CTA groups
+// of a ragged launch; every CTA of a group calls it the same number of times).
+MT_DEV bool group_sync(GridSync* gs, unsigned nctas, int where)
 {
     __shared__ int s_ok;
     __syncthreads();
@@ -57,7 +59,7 @@ MT_DEV bool grid_sync(GridSync* gs, int where)
             unsigned g = ld_acquire_u32(&gs->gen);
             __threadfence();
             unsigned prev = atomicAdd(&gs->count, 1u);
-            if (prev == gridDim.x - 1) {
+            if (prev == nctas - 1) {
                 atomicExch(&gs->count, 0u);
                 __threadfence();
                 st_release_u32(&gs->gen, g + 1u);
@@ -82,6 +84,8 @@ MT_DEV bool grid_sync(GridSync* gs, int where)
     __syncthreads();
     return s_ok != 0;
 }
+
+MT_DEV bool grid_sync(GridSync* gs, int where) { return group_sync(gs, gridDim.x, where); }
 
 // Block-wide reductions; the result is returned to every thread.  scratch must
 // hold 32 doubles.  Deterministic (fixed tree).

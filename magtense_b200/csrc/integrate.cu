@@ -49,6 +49,7 @@ struct Ctx {
     int rcount;
     long long budget_end;       // stop when f_total reaches this
     bool abort;
+    int grank, gsize;           // this CTA's rank in the instance's CTA group, and the group size
 };
 
 // ---- own-element iteration ---------------------------------------------
@@ -63,16 +64,16 @@ template <bool IsMax, int K>
 MT_DEV bool grid_reduce(Ctx& X, double (&v)[K], int where)
 {
     for (int k = 0; k < K; ++k) v[k] = block_reduce<IsMax>(v[k], X.sm_scr);
-    double* buf = X.B.partials + (size_t)(X.rcount & 1) * gridDim.x * kRed;
+    double* buf = X.B.partials + (size_t)(X.rcount & 1) * X.gsize * kRed;
     X.rcount++;
     if (threadIdx.x == 0)
-        for (int k = 0; k < K; ++k) buf[blockIdx.x * kRed + k] = v[k];
-    if (!grid_sync(X.B.gs, where)) { X.abort = true; return false; }
+        for (int k = 0; k < K; ++k) buf[X.grank * kRed + k] = v[k];
+    if (!group_sync(X.B.gs, X.gsize, where)) { X.abort = true; return false; }
     if (threadIdx.x < 32) {
         for (int k = 0; k < K; ++k) {
             double r = IsMax ? 0.0 : 0.0;
             bool have = false;
-            for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) {
+            for (int b = threadIdx.x; b < X.gsize; b += 32) {
                 double x = ldcg(&buf[b * kRed + k]);
                 if (IsMax) r = have ? fmax(r, x) : x; else r += x;
                 have = true;
@@ -90,7 +91,7 @@ MT_DEV bool grid_reduce(Ctx& X, double (&v)[K], int where)
 
 MT_DEV bool barrier(Ctx& X, int where)
 {
-    if (!grid_sync(X.B.gs, where)) { X.abort = true; return false; }
+    if (!group_sync(X.B.gs, X.gsize, where)) { X.abort = true; return false; }
     return true;
 }
 
@@ -629,15 +630,15 @@ MT_DEV int rk_range_integrate(Ctx& X, RKS& s, double t_want, double* y_got, doub
     return flag;
 }
 
-__global__ void __launch_bounds__(kIntegThreads, 1)
-integrate_kernel(DevProb P, IntegBufs B, IntegParams Q)
+// The integrator of one instance on its CTA group (X.P, X.B, X.Q, X.grank, X.gsize set).
+MT_DEV void integrate_body(Ctx& X, unsigned char* smem)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
-    Ctx X;
-    X.P = P; X.B = B; X.Q = Q;
-    const int G = gridDim.x;
-    X.c0 = (int)(((long long)P.n * blockIdx.x) / G);
-    X.nc = (int)(((long long)P.n * (blockIdx.x + 1)) / G) - X.c0;
+    const DevProb& P = X.P;
+    const IntegBufs& B = X.B;
+    const IntegParams& Q = X.Q;
+    const int G = X.gsize;
+    X.c0 = (int)(((long long)P.n * X.grank) / G);
+    X.nc = (int)(((long long)P.n * (X.grank + 1)) / G) - X.c0;
     const int ncmax = (P.n + G - 1) / G;
     const int JC = P.ldk < kDemagJC ? P.ldk : kDemagJC;
     X.sm_m = reinterpret_cast<float*>(smem);
@@ -677,7 +678,7 @@ integrate_kernel(DevProb P, IntegBufs B, IntegParams Q)
                         FOR_OWN(X, q, q32) slot[q] = ldcg(&dst[q]);
                         __syncthreads();
                     }
-                    if (blockIdx.x == 0 && threadIdx.x == 0) { Q.t_out[s.ko] = t_got; Q.flags_out[s.ko] = flag; }
+                    if (X.grank == 0 && threadIdx.x == 0) { Q.t_out[s.ko] = t_got; Q.flags_out[s.ko] = flag; }
                 }
                 s.converged_at = s.ko;
                 s.finished = 1;
@@ -688,15 +689,42 @@ integrate_kernel(DevProb P, IntegBufs B, IntegParams Q)
             __syncthreads();
         }
         if (save) {
-            if (blockIdx.x == 0 && threadIdx.x == 0) { Q.t_out[s.ko] = t_got; Q.flags_out[s.ko] = flag; }
+            if (X.grank == 0 && threadIdx.x == 0) { Q.t_out[s.ko] = t_got; Q.flags_out[s.ko] = flag; }
             s.ko++;
         }
         s.ci++;
         if (s.status) { s.finished = 1; break; }
         if (s.full_f_count + s.f_count >= X.budget_end) break;
     }
-    // every CTA holds the same state; CTA 0 publishes it
-    if (blockIdx.x == 0 && threadIdx.x == 0 && !X.abort) *B.state = s;
+    // every CTA holds the same state; the group's first CTA publishes it
+    if (X.grank == 0 && threadIdx.x == 0 && !X.abort) *B.state = s;
+}
+
+__global__ void __launch_bounds__(kIntegThreads, 1)
+integrate_kernel(DevProb P, IntegBufs B, IntegParams Q)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    Ctx X;
+    X.P = P; X.B = B; X.Q = Q;
+    X.grank = blockIdx.x;
+    X.gsize = gridDim.x;
+    integrate_body(X, smem);
+}
+
+// Ragged batch: instances of different grids in one launch.  Instance k owns the
+// CTAs [inst[k].cta0, inst[k].cta0 + inst[k].ncta) and runs the single-instance
+// integrator on them with its own barrier, buffers and budget; the groups never
+// wait for each other, so a group whose instance finishes simply returns.
+__global__ void __launch_bounds__(kIntegThreads, 1)
+integrate_ragged_kernel(const RaggedInst* __restrict__ inst, const int* __restrict__ cta_inst)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int k = cta_inst[blockIdx.x];
+    Ctx X;
+    X.P = inst[k].P; X.B = inst[k].B; X.Q = inst[k].Q;
+    X.grank = blockIdx.x - inst[k].cta0;
+    X.gsize = inst[k].ncta;
+    integrate_body(X, smem);
 }
 
 }  // namespace
@@ -786,6 +814,19 @@ size_t integrate_smem_bytes(int n, int ldk, int grid)
 {
     const int ncmax = (n + grid - 1) / grid;
     return demag_smem_bytes(ldk, ncmax) + 16 + sizeof(double) * (32 + kRed + 2);
+}
+
+cudaError_t launch_integrate_ragged(const RaggedInst* inst_dev, const int* cta_inst_dev, int grid, size_t smem,
+                                    cudaStream_t stream)
+{
+    cudaError_t e = cudaFuncSetAttribute(integrate_ragged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    const RaggedInst* a = inst_dev;
+    const int* b = cta_inst_dev;
+    void* args[] = {&a, &b};
+    return cudaLaunchCooperativeKernel((const void*)integrate_ragged_kernel, dim3(grid), dim3(kIntegThreads), args, smem,
+                                       stream);
 }
 
 cudaError_t launch_integrate(const DevProb& P, const IntegBufs& B, const IntegParams& Q, int grid,

@@ -50,8 +50,18 @@ struct IntegParams {
     int renorm;
 };
 
+// one instance of a ragged launch and its CTA group
+struct RaggedInst {
+    DevProb P;
+    IntegBufs B;
+    IntegParams Q;
+    int cta0, ncta;
+};
+
 cudaError_t integrate_upload_tables();
 int integrate_grid_size(int n, int num_sms);
 size_t integrate_smem_bytes(int n, int ldk, int grid);
 cudaError_t launch_integrate(const DevProb& P, const IntegBufs& B, const IntegParams& Q, int grid,
                              cudaStream_t stream);
+cudaError_t launch_integrate_ragged(const RaggedInst* inst_dev, const int* cta_inst_dev, int grid, size_t smem,
+                                    cudaStream_t stream);

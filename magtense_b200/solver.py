@@ -187,6 +187,35 @@ class Solver:
             pass
 
 
+def integrate_ragged(solvers, t, m0s, *, tol=1e-4, thres=1e-6, graph=True, stream=None):
+    """Integrate several independent single-instance problems (each its own ``Solver``:
+    grid, tensor, material and dynamics set) over the same output times in one
+    persistent launch, each on its own group of SMs with its own adaptive steps.
+
+    m0s: one (3 n_k,) state per solver.  Returns (t_out (K, nt), [y_k (nt, 3 n_k)],
+    flags (K, nt), stats list).  graph: replay the launch sequence from a CUDA graph."""
+    K = len(solvers)
+    t = _np_d(t).reshape(-1)
+    nt = t.shape[0]
+    dev = solvers[0].device
+    m0t = [torch.as_tensor(m, dtype=torch.float64, device=dev).reshape(-1).contiguous() for m in m0s]
+    ys = [torch.zeros((nt, 3 * sv.n), dtype=torch.float64, device=dev) for sv in solvers]
+    hs = (VPA * K)(*[sv._h.value for sv in solvers])
+    m0p = (VPA * K)(*[m.data_ptr() for m in m0t])
+    yp = (VPA * K)(*[y.data_ptr() for y in ys])
+    t_out = np.zeros((K, nt))
+    flags = np.zeros((K, nt), dtype=np.int32)
+    st = (_lib.Stats * K)()
+    with torch.cuda.device(dev):
+        rc = _lib.lib().mt_integrate_ragged(hs, K, t.ctypes.data_as(_lib.D), nt, m0p, float(tol), float(thres),
+                                            t_out.ctypes.data_as(_lib.D), yp, flags.ctypes.data_as(_lib.I), st,
+                                            1 if graph else 0, _stream(stream))
+    check(rc, "mt_integrate_ragged")
+    return t_out, ys, flags, [x.as_dict() for x in st]
+
+
+VPA = C.c_void_p
+
 PRECISIONS = {"fp32": 0, "bf16x3": 1, "bf16x2": 2, "fp16s": 3, "int8": 4}
 
 
