@@ -13,14 +13,16 @@ for the std-problem-4 dataset workflow.  One step = every instance of the
 rank integrated over the window.
 
 Other workloads: "film-plain" (the same film, single-instance FP32 path) and
-"adjoint" (the differentiation configuration: forward and adjoint backward of
+"ragged" (64 films of seeded sizes nx in 20..120, ny = nx/4, each with its own
+tensor, field and adaptive steps, in one persistent launch on per-instance SM
+groups, replayed from a CUDA graph), "adjoint" (the differentiation configuration: forward and adjoint backward of
 a 2 ns fixed-step RK4 trajectory of the film with 200 piecewise-constant field
 segments and per-cell Ms) and
 "large-plain" (64x64x8 cubes of 5 nm, n = 32768, 25.8 GB FP32 tensor, the
 HBM-bound demag matvec).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload film-batch|film-plain|large-plain|adjoint]
+                  [--workload film-batch|film-plain|large-plain|adjoint|ragged]
 
 Multi-GPU: one process per GPU (torchrun); instances are sharded across ranks
 with no data-path collective ("scaling": "weak"); the step time is the max over
@@ -58,7 +60,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="film-batch", choices=["film-batch", "film-plain", "large-plain", "adjoint"])
+    ap.add_argument("--workload", default="film-batch", choices=["film-batch", "film-plain", "large-plain", "adjoint", "ragged"])
     ap.add_argument("--instances", type=int, default=256, help="instances per rank (film-batch)")
     ap.add_argument("--precision", default="int8", choices=["int8", "fp16s", "bf16x3", "bf16x2", "fp32"])
     ap.add_argument("--plain-sample", type=int, default=4,
@@ -240,12 +242,18 @@ def run_ours(args):
         line = bench_film_batch(torch, args, ws, rank, local, dist, hbm, bf16_sus, src)
     elif args.workload == "adjoint":
         line = bench_adjoint(torch, args, ws, rank, local, dist, hbm, src)
+    elif args.workload == "ragged":
+        line = bench_ragged(torch, args, ws, rank, local, dist, hbm, src)
     else:
         line = bench_plain(torch, args, ws, rank, local, dist, hbm, src)
     if rank == 0 and line is not None:
         if not args.no_cpu:
-            line["cpu_baseline"] = (cpu_adjoint_sample(args.cpu_window) if args.workload == "adjoint" else
-                                    cpu_reference_sample(args.cpu_window, args.workload))
+            if args.workload == "adjoint":
+                line["cpu_baseline"] = cpu_adjoint_sample(args.cpu_window)
+            elif args.workload == "ragged":
+                line["cpu_baseline"] = cpu_ragged_sample(args.cpu_window)
+            else:
+                line["cpu_baseline"] = cpu_reference_sample(args.cpu_window, args.workload)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -494,6 +502,111 @@ def bench_adjoint(torch, args, ws, rank, local, dist, hbm, src):
         "e2e": {"value": sim_ns / (e2e_ms / 1e3), "unit": "simulated ns/s",
                 "h2d_bytes_per_step": (hseg.size + Ms.size) * 8, "d2h_bytes_per_step": (hseg.size + Ms.size) * 8},
         "gpu_launches": int(steps * (4 * 2 + 4 * 2 + 4 * 2)),
+        "clocks": clocks,
+    }
+
+
+def ragged_sizes(seed, count=64):
+    """Seeded film sizes of the ragged batch: nx ~ U{20..120}, ny = nx // 4, nz = 1, cells of
+    6.25 x 6.25 x 3 nm (100 to 3600 cells)."""
+    rng = np.random.default_rng(seed)
+    nxs = rng.integers(20, 121, count)
+    return [((int(nx), int(nx) // 4, 1), (nx * 6.25e-9, (nx // 4) * 6.25e-9, 3e-9)) for nx in nxs]
+
+
+def cpu_ragged_sample(window_ns):
+    """The oracle (FP32 restatement, all host cores) on one mid-sized film of the ragged set."""
+    from oracle import oracle as O
+    res, L = ragged_sizes(2)[0]
+    n = int(np.prod(res))
+    h = instance_fields(1000, 1)[0]
+    win = window_ns * 1e-9
+    P = O.Problem(res, L, mode=0, gamma=GAMMA, alpha=GAMMA * 0.02, hext=np.array([[0.0, *h], [win, *h]]))
+    t0 = time.perf_counter()
+    _, _, _, st = P.solve(np.linspace(0, win, max(2, int(round(window_ns / 1e-3)) + 1)), start_state(n), tol=1e-6)
+    dt = time.perf_counter() - t0
+    return {"value": window_ns / dt, "unit": "simulated ns/s", "cores": O.threads(), "kind": "port",
+            "sample": f"{window_ns} ns of one {res[0]}x{res[1]}x1 film of the ragged set ({st['f_evals']} RHS evals, "
+                      f"{dt:.1f} s); per-instance rate on the host"}
+
+
+def bench_ragged(torch, args, ws, rank, local, dist, hbm, src):
+    from magtense_b200 import Solver, integrate_ragged
+    from magtense_b200.shard import shard_range
+    sizes = ragged_sizes(2, 64 * ws)
+    a0, a1 = shard_range(len(sizes), ws, rank)
+    sizes = sizes[a0:a1]
+    fields = instance_fields(1000, 64 * ws)[a0:a1]
+    window = 0.05 if args.window is None else args.window
+    win = window * 1e-9
+    nt = int(round(window / 1e-3)) + 1
+    t = np.linspace(0, win, nt)
+    solvers, m0s = [], []
+    for (res, L), h in zip(sizes, fields):
+        s = Solver(res, L)
+        s.assemble()
+        s.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.02, hext=np.array([[0.0, *h], [win, *h]]))
+        solvers.append(s)
+        m0s.append(torch.as_tensor(start_state(int(np.prod(res))), device="cuda"))
+    out = {}
+
+    def step():
+        _, _, _, st = integrate_ragged(solvers, t, m0s, tol=1e-6, graph=True)
+        out["st"] = st
+        return st
+
+    times, stats, clocks, flush = timed_steps(torch, step, args.steps, args.warmup, dist, local)
+    # end to end: host states in, host trajectories out
+    m0_host = [m.cpu() for m in m0s]
+    e2e = []
+    for _ in range(max(1, args.steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dev = [m.to("cuda") for m in m0_host]
+        _, ys, _, _ = integrate_ragged(solvers, t, dev, tol=1e-6, graph=True)
+        host = [y.cpu() for y in ys]
+        torch.cuda.synchronize()
+        e2e.append((time.perf_counter() - t0) * 1e3)
+        del ys, host
+    # the same instances one after another through the single-instance path
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s, m in zip(solvers, m0s):
+        s.integrate(t, m, tol=1e-6)
+    torch.cuda.synchronize()
+    seq_s = time.perf_counter() - t0
+    step_ms, e2e_ms = max_over_ranks(torch, dist, [max(times), statistics.median(e2e)])
+    if rank != 0:
+        return None
+    K = len(solvers)
+    st = stats[-1]
+    evals = [x["f_evals"] for x in st]
+    bytes_ = sum(24.0 * s.n * s.n * e for s, e in zip(solvers, evals))
+    kms = st[0]["kernel_ms"]
+    achieved = bytes_ / (kms / 1e3) / 1e9
+    sim_ns = ws * K * window
+    ns = [s.n for s in solvers]
+    return {
+        "metric": "simulated ns/s", "value": sim_ns / (step_ms / 1e3), "unit": "simulated ns/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"ragged: {K} films/rank, nx ~ U{{20..120}}, ny = nx/4, 6.25x6.25x3 nm cells "
+                               f"(n {min(ns)}..{max(ns)}, {sum(24 * x * x for x in ns) / 1e9:.2f} GB of FP32 "
+                               f"tensors), seeded in-plane fields, {window} ns each at alpha_G = 0.02, tol 1e-6, "
+                               "output every 1 ps; one cooperative launch on per-instance SM groups, replayed from "
+                               "a CUDA graph",
+                   "instances_per_rank": K, "window_ns": window, "parallelism": f"instances sharded over {ws} rank(s)",
+                   "l2": "flushed (256 MB write) before every timed step"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None,
+                     "note": f"integrate_ragged_kernel: sum over instances of 24*n_k^2 tensor bytes x evaluations "
+                             f"({sum(evals)} evaluations) over {kms:.1f} ms of device time; peak {src} HBM copy"},
+        "sequential_single_instance": {"value": ws * K * window / seq_s, "unit": "simulated ns/s",
+                                       "note": "the same instances one after another through mt_integrate"},
+        "e2e": {"value": sim_ns / (e2e_ms / 1e3), "unit": "simulated ns/s",
+                "h2d_bytes_per_step": sum(3 * x * 8 for x in ns), "d2h_bytes_per_step": sum(nt * 3 * x * 8 for x in ns)},
+        "rhs_evals_per_instance": {"min": int(min(evals)), "median": float(np.median(evals)), "max": int(max(evals))},
+        "gpu_launches": int(st[0]["launches"]),
         "clocks": clocks,
     }
 
