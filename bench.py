@@ -352,7 +352,7 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
                      "note": f"batch_kernel (the whole persistent integrator, GEMM and RKSUITE coroutines): 18*n^2 "
                              f"useful flops per instance RHS evaluation x {evals} evaluations over {kms:.1f} ms of "
                              f"device time; peak = sustained cuBLAS bf16 ({src})"
-                             + ("; the int8 product executes 12 int8 limb products per useful product" if
+                             + ("; the int8 product executes 16 int8 limb products per useful product" if
                                 args.precision == "int8" else "")},
         "rhs_evals_per_instance": {"min": int(min(x["f_evals"] for x in stats[-1])),
                                    "median": float(np.median([x["f_evals"] for x in stats[-1]])),
