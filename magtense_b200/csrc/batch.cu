@@ -136,6 +136,105 @@ MT_DEV void put_arg(const BCtx& X, int argi, int b, int q, double v)
     }
 }
 
+// Where the stage argument of instance b goes: its FP64 copy and the GEMM
+// operand of the precision, as plain pointers and strides.
+struct ArgDst {
+    double* pool;          // FP64 argument (3n)
+    int prec, n, np, ldk;
+    float* m32;            // fp32: [3][ldk] of instance b
+    uint16_t* mhi;         // 16-bit splits: column b*Kd
+    uint16_t* mlo;
+    int8_t* mlimb;         // int8: column b*Kd of limb 0
+    size_t limb_stride;
+    GridSync* gs;
+};
+
+MT_DEV ArgDst arg_dst(const BCtx& X, int argi, int b)
+{
+    ArgDst d;
+    d.pool = VPOOL(X, argi, b);
+    d.prec = X.Q.prec; d.n = X.P.n; d.np = X.Q.np; d.ldk = X.P.ldk;
+    d.m32 = X.F.m32 ? X.F.m32 + (size_t)b * 3 * X.P.ldk : nullptr;
+    d.mhi = X.F.mhi ? X.F.mhi + (size_t)b * X.Q.Kd : nullptr;
+    d.mlo = X.F.mlo ? X.F.mlo + (size_t)b * X.Q.Kd : nullptr;
+    d.mlimb = X.F.mlimb ? X.F.mlimb + (size_t)b * X.Q.Kd : nullptr;
+    d.limb_stride = (size_t)X.Q.Bp * X.Q.Kd;
+    d.gs = X.F.gs;
+    return d;
+}
+
+MT_DEV void put_arg_d(const ArgDst& d, int q, double v)
+{
+    d.pool[q] = v;
+    const int a = q / d.n, i = q - a * d.n;
+    if (d.prec == kPrecI8) {
+        i8_store_m(v, d.mlimb + (size_t)a * d.np + i, d.limb_stride, d.gs);
+    } else if (d.prec == kPrecFP32) {
+        d.m32[(size_t)a * d.ldk + i] = (float)v;
+    } else {
+        const size_t col = (size_t)a * d.np + i;
+        split_store((float)v, d.prec, d.mhi + col, d.mlo + col);
+    }
+}
+
+struct StgPtrs { const double* s[8]; };
+
+// The stage argument y + h sum_j a_ij k_j of stage i on the lane's owned elements,
+// with the stepb error estimate at stage 7 (returned: the lane's max) and the
+// combination kept for the error estimate at stage 8.  Non-inlined and fed plain
+// pointers, so its loop runs from registers.
+__device__ __noinline__ double stage_args(int i, const double* __restrict__ y, const double* __restrict__ yp,
+                                          StgPtrs st, double* __restrict__ es, ArgDst d, double htry, double thr,
+                                          int lane, int c0, int nc)
+{
+    constexpr int U = 3;   // elements per lane in flight
+    double lm = 0.0;
+    const int n = d.n, tot = 3 * nc;
+    for (int e0 = lane; e0 < tot; e0 += 32 * U) {
+        int q[U];
+        bool on[U];
+        double kv[U][8], ypq[U], yq[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int e = e0 + 32 * u;
+            on[u] = e < tot;
+            const int ee = on[u] ? e : e0;
+            const int a = ee / nc;
+            q[u] = a * n + c0 + (ee - a * nc);
+#pragma unroll
+            for (int j = 2; j <= 7; ++j) kv[u][j] = (j <= i - 1) ? ldcg(&st.s[j][q[u]]) : 0.0;
+            ypq[u] = ldcg(&yp[q[u]]);
+            yq[u] = ldcg(&y[q[u]]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (!on[u]) continue;
+            double e = xmul(cB.a[i][1], ypq[u]);
+#pragma unroll
+            for (int j = 2; j <= 7; ++j) {
+                if (j > i - 1) break;
+                const double aij = cB.a[i][j];
+                if (aij == 0.0) continue;
+                e = xadd(e, xmul(aij, kv[u][j]));
+            }
+            const double yn = xadd(yq[u], xmul(htry, e));
+            put_arg_d(d, q[u], yn);
+            if (i == 8) es[q[u]] = e;
+            if (i == 7) {
+                double v = xmul(cB.e[1], ypq[u]);
+                v = xadd(v, xmul(cB.e[3], kv[u][3]));
+                v = xadd(v, xmul(cB.e[4], kv[u][4]));
+                v = xadd(v, xmul(cB.e[5], kv[u][5]));
+                v = xadd(v, xmul(cB.e[6], kv[u][6]));
+                const double wq = fmax(xmul(0.5, xadd(fabs(yq[u]), fabs(yn))), thr);
+                lm = fmax(lm, fabs(v) / wq);
+            }
+        }
+    }
+    __syncwarp();
+    return lm;
+}
+
 MT_DEV double warp_red(double v, bool is_max)
 {
     return is_max ? warp_max(v) : warp_sum(v);
@@ -238,12 +337,18 @@ MT_DEV void advance(BCtx& X, BInst& I, int b)
                             const double* k1 = VDER(X, s.dypold, b);
                             const double* k8 = VDER(X, s.dyp, b);
                             FOR_OWN_W(X, q) {
-                                double e = xmul(cB.a[i][1], ldcg(&k1[q]));
-                                for (int j = 2; j <= i - 1; ++j) {
-                                    const double* sj = (j == 8) ? k8 : VSTG(X, j, b);
-                                    e = xadd(e, xmul(cB.a[i][j], ldcg(&sj[q])));
+                                double kv[11];
+#pragma unroll
+                                for (int j = 2; j <= 10; ++j)
+                                    kv[j] = (j <= i - 1) ? ldcg(&((j == 8) ? k8 : VSTG(X, j, b))[q]) : 0.0;
+                                const double k1q = ldcg(&k1[q]), yoq = ldcg(&yold[q]);
+                                double e = xmul(cB.a[i][1], k1q);
+#pragma unroll
+                                for (int j = 2; j <= 10; ++j) {
+                                    if (j > i - 1) break;
+                                    e = xadd(e, xmul(cB.a[i][j], kv[j]));
                                 }
-                                put_arg(X, argi, b, q, xadd(ldcg(&yold[q]), xmul(s.h_old, e)));
+                                put_arg(X, argi, b, q, xadd(yoq, xmul(s.h_old, e)));
                             }
                             __syncwarp();
                             I.tstg = xadd(s.t_old, xmul(cB.c[i], s.h_old));
@@ -628,28 +733,11 @@ MT_DEV void advance(BCtx& X, BInst& I, int b)
                                 const double* yp = VDER(X, s.dyp, b);
                                 double* es = X.F.errest + (size_t)b * X.n3;
                                 double lm = 0.0;
-                                FOR_OWN_W(X, q) {
-                                    double e = xmul(cB.a[i][1], ldcg(&yp[q]));
-                                    for (int j = 2; j <= i - 1; ++j) {
-                                        const double aij = cB.a[i][j];
-                                        if (aij == 0.0) continue;
-                                        e = xadd(e, xmul(aij, ldcg(&VSTG(X, j, b)[q])));
-                                    }
-                                    const double yq = ldcg(&y[q]);
-                                    const double yn = xadd(yq, xmul(I.htry, e));
-                                    put_arg(X, argi, b, q, yn);
-                                    if (i == 8) es[q] = e;
-                                    if (i == 7) {
-                                        double v = xmul(cB.e[1], ldcg(&yp[q]));
-                                        v = xadd(v, xmul(cB.e[3], ldcg(&VSTG(X, 3, b)[q])));
-                                        v = xadd(v, xmul(cB.e[4], ldcg(&VSTG(X, 4, b)[q])));
-                                        v = xadd(v, xmul(cB.e[5], ldcg(&VSTG(X, 5, b)[q])));
-                                        v = xadd(v, xmul(cB.e[6], ldcg(&VSTG(X, 6, b)[q])));
-                                        const double wq = fmax(xmul(0.5, xadd(fabs(yq), fabs(yn))), thr);
-                                        lm = fmax(lm, fabs(v) / wq);
-                                    }
-                                }
-                                __syncwarp();
+                                const uint64_t tv0 = (X.F.prof && blockIdx.x == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0;
+                                StgPtrs sp;
+                                for (int j = 0; j < 8; ++j) sp.s[j] = (j >= 2) ? VSTG(X, j, b) : nullptr;
+                                lm = stage_args(i, y, yp, sp, es, arg_dst(X, argi, b), I.htry, thr, X.lane, X.c0, X.nc);
+                                if (tv0) { atomicAdd(&X.F.prof[25], globaltimer_ns() - tv0); atomicAdd(&X.F.prof[26], 1ull); }
                                 if (i == 7) post_reduce(X, I, b, &lm, 1, true);
                                 I.tstg = xadd(s.t, xmul(cB.c[i], I.htry));
                                 if (s.at_t_end && cB.c[i] == 1.0) I.tstg = s.t_end;
@@ -719,13 +807,18 @@ MT_DEV void advance(BCtx& X, BInst& I, int b)
                             double* w = X.F.weights + (size_t)b * X.n3;
                             double lm = 0.0;
                             FOR_OWN_W(X, q) {
-                                double v = ldcg(&es[q]);
-                                v = xsub(v, xmul(cB.b[1], ldcg(&yp[q])));
+                                double kv[8];
+#pragma unroll
+                                for (int i = 2; i <= 7; ++i) kv[i] = ldcg(&VSTG(X, i, b)[q]);
+                                const double esq = ldcg(&es[q]), ypq = ldcg(&yp[q]), k8q = ldcg(&k8[q]);
+                                double v = esq;
+                                v = xsub(v, xmul(cB.b[1], ypq));
+#pragma unroll
                                 for (int i = 2; i <= 7; ++i) {
                                     if (cB.b[i] == 0.0) continue;
-                                    v = xsub(v, xmul(cB.b[i], ldcg(&VSTG(X, i, b)[q])));
+                                    v = xsub(v, xmul(cB.b[i], kv[i]));
                                 }
-                                v = xsub(v, xmul(cB.b[8], ldcg(&k8[q])));
+                                v = xsub(v, xmul(cB.b[8], k8q));
                                 v = xmul(I.htry, v);
                                 es[q] = v;
                                 const double wq = fmax(xmul(0.5, xadd(fabs(ldcg(&y[q])), fabs(ldcg(&yn[q])))), thr);
@@ -1123,7 +1216,11 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
             const int b = X.i0 + X.warp + k * X.nwarps;
             if (b >= Q.B) continue;
             if (I.req == 2) resolve_reduce(X, I, b);
-            if (I.req == 0) advance(X, I, b);
+            if (I.req == 0) {
+                const uint64_t ta = (F.prof && t == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0;
+                advance(X, I, b);
+                if (ta) { atomicAdd(&F.prof[27], globaltimer_ns() - ta); atomicAdd(&F.prof[28], 1ull); }
+            }
             if (I.req != 3 && I.req != 4) my_active++;
             if (I.req == 1) { my_rhs++; rhs_tile[(b / kI8N - X.jb0) & 1]++; }
         }
@@ -1203,7 +1300,9 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
             const int b = X.i0 + X.warp + k * X.nwarps;
             if (b >= Q.B || I.req != 1) continue;
             I.req = 0;
+            const uint64_t ta = (F.prof && t == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0;
             advance(X, I, b);
+            if (ta) { atomicAdd(&F.prof[27], globaltimer_ns() - ta); atomicAdd(&F.prof[28], 1ull); }
         }
         __syncthreads();
         PROF_MARK(4);

@@ -1198,6 +1198,9 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
                     "full %.2f tfree %.2f; epilogue waits %.2f drains %.2f; producer waits %.2f; units %.1f segments %.2f\n",
                     pr[23] / tk / 1e3, pr[24] / tk / 1e3, pr[16] / tk / 1e3, pr[17] / tk / 1e3, pr[18] / tk / 1e3,
                     pr[19] / tk / 1e3, pr[20] / tk / 1e3, pr[21] / tk, pr[22] / tk);
+        fprintf(stderr, "[batch profile] CTA 0 warp 0: advance %.2f us per call (%llu calls), stage-argument loop "
+                "%.2f us per call (%llu calls)\n", pr[28] ? pr[27] / 1e3 / pr[28] : 0.0, pr[28],
+                pr[26] ? pr[25] / 1e3 / pr[26] : 0.0, pr[26]);
     }
     if (worst) return fail(MT_ERR_SOLVER, "an instance stopped with RKSUITE flag %d", worst);
     return MT_OK;
