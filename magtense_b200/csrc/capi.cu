@@ -778,7 +778,7 @@ int make_tmap(CUtensorMap* m, const void* base, uint64_t inner, uint64_t outer, 
     return MT_OK;
 }
 
-// 3-D int8 tensor [limbs][outer][inner] (inner contiguous), box {64, box_outer, 1}, 64-byte swizzle
+// 3-D int8 tensor [limbs][outer][inner] (inner contiguous), box {128, box_outer, 1}, 128-byte swizzle
 int make_tmap_i8(CUtensorMap* m, const void* base, uint64_t inner, uint64_t outer, uint64_t limbs, uint32_t box_outer)
 {
     int rc = get_encoder();
@@ -788,7 +788,7 @@ int make_tmap_i8(CUtensorMap* m, const void* base, uint64_t inner, uint64_t oute
     cuuint32_t box[3] = {(cuuint32_t)kI8KB, box_outer, 1};
     cuuint32_t es[3] = {1, 1, 1};
     CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, es,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(MT_ERR_CUDA, "cuTensorMapEncodeTiled (int8) failed (%d)", (int)r);
     return MT_OK;

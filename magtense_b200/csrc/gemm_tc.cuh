@@ -309,19 +309,32 @@ MT_DEV bool tc_gemm_tile_impl(unsigned char* smem, const QT& Q, const FT& F, con
 // is the same bit pattern on every run.
 //
 // Work split (Stream-K): tile = 128 tensor rows x 64 instances, unit = one
-// 64-wide k step of a tile; the units of all active tiles are split into
+// 128-wide k step of a tile; the units of all active tiles are split into
 // contiguous non-empty ranges, one per CTA, so every SM gets the same number of
 // MMAs.  A CTA's range covers pieces ("segments") of one or more tiles; each
 // segment's exact int64 partials go to its own slot [CTA][segment][part][inst][row],
 // and the reader sums the slots of the CTAs that cover the tile.
 // ---------------------------------------------------------------------------
-constexpr int kI8Stages = 4;
-constexpr int kI8KB = 64;                                    // int8 sources per stage (64-byte rows)
+constexpr int kI8Stages = 2;
+constexpr int kI8KB = 128;                                   // int8 sources per stage (128-byte rows, 128-byte swizzle)
 constexpr int kI8N = 64;                                     // instances per tile (MMA N)
-constexpr int kI8ATile = 128 * kI8KB;                        // one 128-row K limb tile, 8 KB
-constexpr int kI8BTile = kI8N * kI8KB;                       // one 64-row m limb tile, 4 KB
+constexpr int kI8ATile = 128 * kI8KB;                        // one 128-row K limb tile, 16 KB
+constexpr int kI8BTile = kI8N * kI8KB;                       // one 64-row m limb tile, 8 KB
 constexpr int kI8KLimbs = 4, kI8MLimbs = 4, kI8Acc = 7;
-constexpr int kI8StageBytes = kI8KLimbs * kI8ATile + kI8MLimbs * kI8BTile;   // 48 KB
+constexpr int kI8StageBytes = kI8KLimbs * kI8ATile + kI8MLimbs * kI8BTile;   // 96 KB
+
+// shared-memory matrix descriptor: K-major tile of 128-byte rows with the
+// 128-byte swizzle, 8-row groups 1024 bytes apart (SBO), version 1 (tcgen05)
+MT_DEV uint64_t sdesc_sw128(uint32_t saddr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;                  // LBO (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;         // SBO
+    d |= (uint64_t)1 << 46;                   // descriptor version
+    d |= (uint64_t)2 << 61;                   // SWIZZLE_128B
+    return d;
+}
 constexpr int kI8SlotElems = 2 * kI8N * 128;                 // int64 per segment slot (hi and lo parts)
 // D S32 (2 at bit 4), A and B signed 8-bit (1 at bits 7 and 10), N = 64, M = 128
 constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | (((uint32_t)kI8N >> 3) << 17) | ((128u >> 4) << 24);
@@ -511,10 +524,10 @@ MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int
                 for (int kk = 0; kk < kI8KB / 32; ++kk) {
 #pragma unroll
                     for (int a = 0; a < kI8KLimbs; ++a) {
-                        const uint64_t ad = sdesc_sw64(base + a * kI8ATile + kk * 32);
+                        const uint64_t ad = sdesc_sw128(base + a * kI8ATile + kk * 32);
 #pragma unroll
                         for (int b = 0; b < kI8MLimbs; ++b) {
-                            const uint64_t bd = sdesc_sw64(base + kI8KLimbs * kI8ATile + b * kI8BTile + kk * 32);
+                            const uint64_t bd = sdesc_sw128(base + kI8KLimbs * kI8ATile + b * kI8BTile + kk * 32);
                             // the first product into each accumulator of the segment overwrites it:
                             // (0,b) opens s = 0..3, (1,3), (2,3), (3,3) open s = 4, 5, 6
                             const bool first = ks == ks0 && kk == 0 && (a == 0 || b == kI8MLimbs - 1);
