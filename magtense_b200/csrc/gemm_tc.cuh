@@ -616,8 +616,17 @@ MT_DEV double i8_tile_sum(const long long* part, int maxseg, const SkCover& cv, 
 {
     const size_t off = (size_t)lj * 128 + (size_t)lr, lo = (size_t)kI8N * 128;
     const long long* p0 = part + ((size_t)cv.first * maxseg + (size_t)cv.jf) * kI8SlotElems + off;
-    long long hi_s = __ldcg(p0), lo_s = __ldcg(p0 + lo);
-    for (int c = cv.first + 1; c <= cv.last; ++c) {
+    // the first three covering slots are loaded together (most tiles have at most three)
+    const int c1 = cv.first + 1 <= cv.last ? cv.first + 1 : cv.first;
+    const int c2 = cv.first + 2 <= cv.last ? cv.first + 2 : cv.first;
+    const long long* p1 = (c1 != cv.first) ? part + (size_t)c1 * maxseg * kI8SlotElems + off : p0;
+    const long long* p2 = (c2 != cv.first) ? part + (size_t)c2 * maxseg * kI8SlotElems + off : p0;
+    const long long h0 = __ldcg(p0), l0 = __ldcg(p0 + lo), h1 = __ldcg(p1), l1 = __ldcg(p1 + lo);
+    const long long h2 = __ldcg(p2), l2 = __ldcg(p2 + lo);
+    long long hi_s = h0, lo_s = l0;
+    if (c1 != cv.first) { hi_s += h1; lo_s += l1; }
+    if (c2 != cv.first) { hi_s += h2; lo_s += l2; }
+    for (int c = cv.first + 3; c <= cv.last; ++c) {
         const long long* pc = part + (size_t)c * maxseg * kI8SlotElems + off;
         hi_s += __ldcg(pc);
         lo_s += __ldcg(pc + lo);

@@ -83,6 +83,14 @@ MT_DEV double lap_cell_dev(const DevProb& P, const double* v, int i)
     double dgz = (nz > 1) ? ((iz == 0 || iz == nz - 1) ? P.diag_b[2] : P.diag_i[2]) : 0.0;
     double diag = xadd(dgx, dgy);
     if (nz > 1) diag = xadd(diag, dgz);
+    // which neighbours exist; every value is loaded up front (an absent neighbour
+    // loads the cell itself and is not used), so the loads are in flight together
+    const bool hz0 = nz > 1 && iz > 0, hy0 = ny > 1 && iy > 0, hx0 = nx > 1 && ix > 0;
+    const bool hx1 = nx > 1 && ix < nx - 1, hy1 = ny > 1 && iy < ny - 1, hz1 = nz > 1 && iz < nz - 1;
+    const double vz0 = ldcg(&v[hz0 ? i - nx * ny : i]), vy0 = ldcg(&v[hy0 ? i - nx : i]);
+    const double vx0 = ldcg(&v[hx0 ? i - 1 : i]), vc = ldcg(&v[i]);
+    const double vx1 = ldcg(&v[hx1 ? i + 1 : i]), vy1 = ldcg(&v[hy1 ? i + nx : i]);
+    const double vz1 = ldcg(&v[hz1 ? i + nx * ny : i]);
     double s = 0.0;
     bool first = true;
 #define MT_ACC(term)                              \
@@ -91,13 +99,13 @@ MT_DEV double lap_cell_dev(const DevProb& P, const double* v, int i)
         if (first) { s = _t; first = false; }     \
         else s = xadd(s, _t);                     \
     } while (0)
-    if (nz > 1 && iz > 0) MT_ACC(xmul(P.lapc[2], ldcg(&v[i - nx * ny])));
-    if (ny > 1 && iy > 0) MT_ACC(xmul(P.lapc[1], ldcg(&v[i - nx])));
-    if (nx > 1 && ix > 0) MT_ACC(xmul(P.lapc[0], ldcg(&v[i - 1])));
-    MT_ACC(xmul(diag, ldcg(&v[i])));
-    if (nx > 1 && ix < nx - 1) MT_ACC(xmul(P.lapc[0], ldcg(&v[i + 1])));
-    if (ny > 1 && iy < ny - 1) MT_ACC(xmul(P.lapc[1], ldcg(&v[i + nx])));
-    if (nz > 1 && iz < nz - 1) MT_ACC(xmul(P.lapc[2], ldcg(&v[i + nx * ny])));
+    if (hz0) MT_ACC(xmul(P.lapc[2], vz0));
+    if (hy0) MT_ACC(xmul(P.lapc[1], vy0));
+    if (hx0) MT_ACC(xmul(P.lapc[0], vx0));
+    MT_ACC(xmul(diag, vc));
+    if (hx1) MT_ACC(xmul(P.lapc[0], vx1));
+    if (hy1) MT_ACC(xmul(P.lapc[1], vy1));
+    if (hz1) MT_ACC(xmul(P.lapc[2], vz1));
 #undef MT_ACC
     return s;
 }
