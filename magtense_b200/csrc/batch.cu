@@ -54,9 +54,20 @@ struct BCtx {
     int nact;
     long long U;
     const int* act_pos;     // [2 IB] position of a 64-instance tile in the active list, -1 if idle
-    int jb0;
-    const SkCover* cov;     // [3][2]
+    int jb0;                // first tile of this CTA's instances (compact positions when packed)
+    const SkCover* cov;     // [3][3]
+    bool packed;            // instances sit at their compact positions (integration) or at b (demag only)
+    const unsigned* bits;   // [Bp / 32] request bits of this tick (packed)
+    const int* pre;         // [Bp / 32] requests before each word (packed)
 };
+
+// compact position of requesting instance b: requests with a smaller index
+MT_DEV int compact_pos(const BCtx& X, int b)
+{
+    if (!X.packed) return b;
+    const int w = b >> 5;
+    return X.pre[w] + __popc(X.bits[w] & ((1u << (b & 31)) - 1u));
+}
 
 // per-instance vector addressing
 MT_DEV double* VPOOL(const BCtx& X, int k, int b) { return X.F.pool + ((size_t)k * X.Q.Bp + b) * X.n3; }
@@ -967,26 +978,52 @@ MT_DEV void advance(BCtx& X, BInst& I, int b)
 MT_DEV void i8_cell_field(const BCtx& X, int b, int i, double hm[3])
 {
     const double ms = (double)__ldg(&X.P.Mfact[i]);
-    const int jl = b / kI8N - X.jb0;
+    const int k = compact_pos(X, b);
+    const int jl = k / kI8N - X.jb0;
     for (int a = 0; a < 3; ++a) {
         const int r = a * X.Q.np + i;
-        const double h = i8_tile_sum(X.F.part, X.Q.maxseg, X.cov[a * 2 + jl], r & 127, b % kI8N);
+        const double h = i8_tile_sum(X.F.part, X.Q.maxseg, X.cov[a * 3 + jl], r & 127, k % kI8N);
         hm[a] = xmul(-ms, xmul(h, __ldg(&X.Q.row_scale[r])));
     }
 }
 
-// covers of this CTA's tiles for the current active list (threads 0..5)
+// covers of this CTA's tiles (3 components x 3 tiles from jb0; threads 0..8).
+// Packed: tile j of the compact list is active tile j; otherwise act_pos maps tiles.
 MT_DEV void i8_fill_cover(BCtx& X, SkCover* cov)
 {
     const int k = threadIdx.x;
-    if (k < 6 && X.nc > 0) {
-        const int a = k / 2, jb = X.jb0 + (k & 1);
+    if (k < 9 && X.nc > 0) {
+        const int a = k / 3, jb = X.jb0 + k % 3;
         SkCover cv = {0, -1, 0};
-        if (jb < 2 * X.Q.IB && X.act_pos[jb] >= 0) {
-            const long long t = (long long)X.act_pos[jb] * X.Q.RB + (a * X.Q.np + X.c0) / 128;
+        const int pos = X.packed ? (jb < X.nact ? jb : -1) : (jb < 2 * X.Q.IB ? X.act_pos[jb] : -1);
+        if (pos >= 0) {
+            const long long t = (long long)pos * X.Q.RB + (a * X.Q.np + X.c0) / 128;
             cv = sk_cover(t, X.Q.nks, X.U);
         }
         cov[k] = cv;
+    }
+}
+
+// copy the limbs of this CTA's share of the requesting instances to their compact rows
+MT_DEV void i8_pack(const BCtx& X, int nreq, const unsigned* bits, const int* pre, int W)
+{
+    const int G = gridDim.x, c = blockIdx.x;
+    const int k0 = (int)((long long)nreq * c / G), k1 = (int)((long long)nreq * (c + 1) / G);
+    const size_t plane = (size_t)X.Q.Bp * X.Q.Kd;
+    const int v16 = X.Q.Kd / 16;   // Kd is a multiple of 384
+    for (int k = k0; k < k1; ++k) {
+        // instance of compact position k: the word that holds it, then the bit
+        int w = 0;
+        while (w + 1 < W && pre[w + 1] <= k) ++w;
+        unsigned m = bits[w];
+        for (int r = k - pre[w]; r > 0; --r) m &= m - 1u;
+        const int b = (w << 5) + (__ffs(m) - 1);
+        for (int e = threadIdx.x; e < 4 * v16; e += blockDim.x) {
+            const int l = e / v16, v = e - l * v16;
+            const uint4* src = reinterpret_cast<const uint4*>(X.F.mlimb + l * plane + (size_t)b * X.Q.Kd) + v;
+            uint4* dst = reinterpret_cast<uint4*>(X.F.mcomp + l * plane + (size_t)k * X.Q.Kd) + v;
+            *dst = __ldcg(src);
+        }
     }
 }
 
@@ -1125,10 +1162,16 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
     X.nact = 0;
     X.U = 0;
     __shared__ int s_act[2 * kMaxIB], s_actpos[2 * kMaxIB], s_nact;
-    __shared__ SkCover s_cov[6];
+    __shared__ SkCover s_cov[9];
+    __shared__ unsigned s_bits[4 * kMaxIB];
+    __shared__ int s_pre[4 * kMaxIB + 1];
     X.act_pos = s_actpos;
     X.jb0 = X.i0 / kI8N;
     X.cov = s_cov;
+    X.packed = false;
+    X.bits = s_bits;
+    X.pre = s_pre;
+    const int W = Q.Bp / 32;
     X.n3 = 3 * (size_t)P.n;
     X.lane = threadIdx.x & 31;
     X.warp = threadIdx.x >> 5;
@@ -1162,7 +1205,7 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
             X.nact = JB;
             X.U = (long long)JB * Q.RB * Q.nks;
             i8_fill_cover(X, s_cov);
-            ok = tc_i8_streamk(X.smem, F, F.part, Q.maxseg, maps, X.nact, s_act, Q.RB, Q.nks, tcs);
+            ok = tc_i8_streamk(X.smem, F, F.part, Q.maxseg, maps, &maps.bhi, X.nact, s_act, Q.RB, Q.nks, tcs);
         } else if (!tc) {
             gemm_tile_simt(X);
         } else {
@@ -1179,7 +1222,7 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
                 double h;
                 if (i8) {
                     const int r = a * Q.np + i;
-                    const double v = i8_tile_sum(F.part, Q.maxseg, s_cov[a * 2 + b / kI8N - X.jb0], r & 127, b % kI8N);
+                    const double v = i8_tile_sum(F.part, Q.maxseg, s_cov[a * 3 + b / kI8N - X.jb0], r & 127, b % kI8N);
                     h = xmul(-(double)__ldg(&P.Mfact[i]), xmul(v, __ldg(&Q.row_scale[r])));
                 } else {
                     float acc = 0.f;
@@ -1222,14 +1265,18 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
                 if (ta) { atomicAdd(&F.prof[27], globaltimer_ns() - ta); atomicAdd(&F.prof[28], 1ull); }
             }
             if (I.req != 3 && I.req != 4) my_active++;
-            if (I.req == 1) { my_rhs++; rhs_tile[(b / kI8N - X.jb0) & 1]++; }
+            if (I.req == 1) {
+                my_rhs++;
+                rhs_tile[(b / kI8N - X.i0 / kI8N) & 1]++;
+                if (i8 && X.cb == 0 && X.lane == 0) atomicOr(&F.reqbits[(tick % 3) * W + (b >> 5)], 1u << (b & 31));
+            }
         }
         asm volatile("fence.proxy.async.global;" ::: "memory");   // operand stores -> TMA reads
         if (X.lane == 0 && X.cb == 0 && (my_active | my_rhs)) {
             atomicAdd(&ctr[0], (unsigned)my_active);
             atomicAdd(&ctr[1], (unsigned)my_rhs);
             for (int h = 0; h < 2; ++h)
-                if (rhs_tile[h]) atomicAdd(&F.ibreq[(tick % 3) * 2 * Q.IB + X.jb0 + h], (unsigned)rhs_tile[h]);
+                if (rhs_tile[h]) atomicAdd(&F.ibreq[(tick % 3) * 2 * Q.IB + X.i0 / kI8N + h], (unsigned)rhs_tile[h]);
         }
         __syncthreads();
         PROF_MARK(0);
@@ -1243,24 +1290,43 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
             unsigned* nxt = F.counters + 2 * ((tick + 1) % 3);
             nxt[0] = 0; nxt[1] = 0;
             for (int k = 0; k < 2 * Q.IB; ++k) F.ibreq[((tick + 1) % 3) * 2 * Q.IB + k] = 0;
+            if (i8) for (int w = 0; w < W; ++w) F.reqbits[((tick + 1) % 3) * W + w] = 0u;
         }
         if (active == 0) break;
         if (i8) {
-            // 64-instance tiles with requests, in order; every CTA builds the same list
+            // requesting instances, packed in index order: every CTA builds the same prefix table,
+            // copies its share of their operand rows to the compact buffer, then the GEMM runs
+            // over ceil(requests / 64) tiles of that buffer
+            for (int w = threadIdx.x; w < W; w += blockDim.x) s_bits[w] = __ldcg(&F.reqbits[(tick % 3) * W + w]);
+            __syncthreads();
             if (threadIdx.x == 0) {
-                int na = 0;
-                for (int k = 0; k < 2 * Q.IB; ++k) {
-                    const bool on = __ldcg(&F.ibreq[(tick % 3) * 2 * Q.IB + k]) > 0;
-                    s_actpos[k] = on ? na : -1;
-                    if (on) s_act[na++] = k;
-                }
-                s_nact = na;
+                int acc = 0;
+                for (int w = 0; w < W; ++w) { s_pre[w] = acc; acc += __popc(s_bits[w]); }
+                s_pre[W] = acc;
             }
             __syncthreads();
-            X.nact = s_nact;
+            const int nr = s_pre[W];
+            X.packed = true;
+            X.nact = (nr + kI8N - 1) / kI8N;
             X.U = (long long)X.nact * Q.RB * Q.nks;
+            // first compact position among this CTA's requesting instances
+            {
+                int first = 1 << 30;
+                for (int li = 0; li < X.ni; ++li) {
+                    const int b = X.i0 + li;
+                    if (b < Q.B && ((s_bits[b >> 5] >> (b & 31)) & 1u)) { first = compact_pos(X, b); break; }
+                }
+                X.jb0 = first < (1 << 30) ? first / kI8N : 0;
+            }
             i8_fill_cover(X, s_cov);   // read in P1, after the barriers that follow the GEMM
-            if (X.nact > 0 && !tc_i8_streamk(X.smem, F, F.part, Q.maxseg, maps, X.nact, s_act, Q.RB, Q.nks, tcs))
+            i8_pack(X, nr, s_bits, s_pre, W);
+            asm volatile("fence.proxy.async.global;" ::: "memory");   // packed rows -> TMA reads
+            __syncthreads();
+            if (!grid_sync(F.gs, 6)) { ok = false; break; }
+            for (int k = threadIdx.x; k < X.nact; k += blockDim.x) s_act[k] = k;
+            __syncthreads();
+            if (X.nact > 0 && !tc_i8_streamk(X.smem, F, F.part, Q.maxseg, maps, &maps.blo, X.nact, s_act, Q.RB, Q.nks,
+                                             tcs))
                 ok = false;
         } else if (nreq > 0) {
             if (!tc) gemm_tile_simt(X);

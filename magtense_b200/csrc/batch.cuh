@@ -52,6 +52,8 @@ struct BatchBufs {
     uint16_t* mhi;     // [Bp][Kd] BF16 argument, K-major (tcgen05 backends)
     uint16_t* mlo;
     int8_t* mlimb;     // [4][Bp][Kd] int8 limbs of the argument (int8 backend)
+    int8_t* mcomp;     // [4][Bp][Kd] the limbs of this tick's requesting instances, packed (int8 backend)
+    unsigned* reqbits; // [3][Bp / 32] instances that request a right-hand side (int8 backend)
     float* hpart;      // [S][Bp][3][np] partial demag sums
     long long* part;   // [G][maxseg][64][128] exact int64 segment sums (int8 backend)
     double* partials;  // [Bp][kRedSlots][CB] reduction partials

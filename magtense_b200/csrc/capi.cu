@@ -937,6 +937,10 @@ int batch_alloc(mt_batch* bt, BatchRun& R, int nt, cudaStream_t s)
     } else if (bt->prec == MT_PREC_INT8) {
         CUDA_TRY(R.A.get(&F.mlimb, 4 * (size_t)Bp * bt->Kd));
         CUDA_TRY(cudaMemsetAsync(F.mlimb, 0, 4 * (size_t)Bp * bt->Kd, s));
+        CUDA_TRY(R.A.get(&F.mcomp, 4 * (size_t)Bp * bt->Kd));
+        CUDA_TRY(cudaMemsetAsync(F.mcomp, 0, 4 * (size_t)Bp * bt->Kd, s));
+        CUDA_TRY(R.A.get(&F.reqbits, 3 * (size_t)(Bp / 32)));
+        CUDA_TRY(cudaMemsetAsync(F.reqbits, 0, sizeof(unsigned) * 3 * (Bp / 32), s));
     } else {
         CUDA_TRY(R.A.get(&F.mhi, (size_t)Bp * bt->Kd));
         CUDA_TRY(R.A.get(&F.mlo, (size_t)Bp * bt->Kd));
@@ -974,6 +978,7 @@ int batch_alloc(mt_batch* bt, BatchRun& R, int nt, cudaStream_t s)
         int rc;
         if ((rc = make_tmap_i8(&R.maps.ahi, bt->klimb, bt->Kd, bt->Kd, 4, 128))) return rc;
         if ((rc = make_tmap_i8(&R.maps.bhi, F.mlimb, bt->Kd, Bp, 4, kI8N))) return rc;
+        if ((rc = make_tmap_i8(&R.maps.blo, F.mcomp, bt->Kd, Bp, 4, kI8N))) return rc;
     } else if (bt->prec != MT_PREC_FP32) {
         int rc;
         if ((rc = make_tmap(&R.maps.ahi, bt->khi, bt->Kd, bt->Kd, 128))) return rc;
@@ -1132,6 +1137,7 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
         CUDA_TRY(cudaMemsetAsync(F.gs, 0, sizeof(GridSync), s));
         CUDA_TRY(cudaMemsetAsync(F.counters, 0, sizeof(unsigned) * 6, s));
         CUDA_TRY(cudaMemsetAsync(F.ibreq, 0, sizeof(unsigned) * 6 * bt->IB, s));
+        if (F.reqbits) CUDA_TRY(cudaMemsetAsync(F.reqbits, 0, sizeof(unsigned) * 3 * (Q.Bp / 32), s));
         CUDA_TRY(cudaEventRecord(ev0, s));
         CUDA_TRY(launch_batch(P, F, Q, bt->grid, bt->prec != MT_PREC_FP32 ? &R.maps : nullptr, s,
                               l2_bytes ? (bt->prec == MT_PREC_INT8 ? (const void*)bt->klimb : (const void*)bt->khi)

@@ -458,7 +458,7 @@ MT_DEV void i8_prof_add(unsigned long long* prof, int slot, unsigned long long v
 // part: int64 slots [gridDim.x][maxseg][64][128].  Returns a CTA-uniform ok flag.
 template <typename FT>
 MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int maxseg, const TcMaps& maps,
-                          int nact, const int* act_jb, int RB, int nks, TcState& st)
+                          const CUtensorMap* bmap, int nact, const int* act_jb, int RB, int nks, TcState& st)
 {
     I8Smem L = i8_layout(smem);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -489,7 +489,7 @@ MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int
                 for (int a = 0; a < kI8KLimbs; ++a)
                     tma_load_3d(smem_u32(base + a * kI8ATile), &maps.ahi, x, rb * 128, a, fb);
                 for (int b = 0; b < kI8MLimbs; ++b)
-                    tma_load_3d(smem_u32(base + kI8KLimbs * kI8ATile + b * kI8BTile), &maps.bhi, x, jb * kI8N, b, fb);
+                    tma_load_3d(smem_u32(base + kI8KLimbs * kI8ATile + b * kI8BTile), bmap, x, jb * kI8N, b, fb);
             }
             u = ue;
         }
