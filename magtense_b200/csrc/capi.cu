@@ -70,6 +70,7 @@ struct mt_handle {
     // dynamics
     int solver = 2; double gamma = 0.0, alpha0 = 0.0; int hext_row = 0; int renorm = 0;
     double* hext = nullptr; int nt_hext = 0; double* alpha_tab = nullptr; int nt_alpha = 0;
+    int cap_hext = 0, cap_alpha = 0;   // allocated rows: tables of the same size keep their device address
     bool have_dynamics = false;
     // tensor
     float* K = nullptr; bool have_K = false;
@@ -216,10 +217,16 @@ int mt_set_dynamics(mt_handle* h, int solver, double gamma, double alpha0, const
     if (nt_alpha > 0 && !alpha_tab) return fail(MT_ERR_ARG, "null alpha table");
     if (solver == 1 && (hext_row < 0 || hext_row >= nt_hext))
         return fail(MT_ERR_ARG, "hext_row %d outside the table (%d rows)", hext_row, nt_hext);
-    free_ptr(h->hext); h->hext = nullptr;
-    free_ptr(h->alpha_tab); h->alpha_tab = nullptr;
-    CUDA_TRY(dalloc(&h->hext, 4 * (size_t)std::max(nt_hext, 1)));
-    CUDA_TRY(dalloc(&h->alpha_tab, 2 * (size_t)std::max(nt_alpha, 1)));
+    if (!h->hext || h->cap_hext < std::max(nt_hext, 1)) {
+        free_ptr(h->hext); h->hext = nullptr;
+        CUDA_TRY(dalloc(&h->hext, 4 * (size_t)std::max(nt_hext, 1)));
+        h->cap_hext = std::max(nt_hext, 1);
+    }
+    if (!h->alpha_tab || h->cap_alpha < std::max(nt_alpha, 1)) {
+        free_ptr(h->alpha_tab); h->alpha_tab = nullptr;
+        CUDA_TRY(dalloc(&h->alpha_tab, 2 * (size_t)std::max(nt_alpha, 1)));
+        h->cap_alpha = std::max(nt_alpha, 1);
+    }
     CUDA_TRY(cudaMemset(h->hext, 0, sizeof(double) * 4 * std::max(nt_hext, 1)));
     CUDA_TRY(cudaMemset(h->alpha_tab, 0, sizeof(double) * 2 * std::max(nt_alpha, 1)));
     if (nt_hext > 0) CUDA_TRY(cudaMemcpy(h->hext, hext, sizeof(double) * 4 * nt_hext, cudaMemcpyHostToDevice));

@@ -171,11 +171,22 @@ cudaError_t launch_field(int mode, const DevProb& P, const double* m, const floa
     const int grid = (P.n + cpc - 1) / cpc;
     const size_t smem = demag_smem_bytes(P.ldk, cpc);
     cudaError_t e = cudaSuccess;
-#define MT_LAUNCH(M)                                                                                       \
-    do {                                                                                                   \
-        e = cudaFuncSetAttribute(field_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-        if (e != cudaSuccess) return e;                                                                    \
-        field_kernel<M><<<grid, kFieldThreads, smem, s>>>(P, m, m32, t, cpc, o0, o1, o2, o3, h32, pref);   \
+    // the shared-memory limit is raised only when it grows (once per mode and size in practice),
+    // so repeated launches, for example inside a stream capture, make no attribute calls
+    constexpr int kMaxDev = 64;
+    static size_t smem_set[kMaxDev][6] = {};
+    int dev = 0;
+    e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    size_t* set = (dev >= 0 && dev < kMaxDev) ? smem_set[dev] : nullptr;
+#define MT_LAUNCH(M)                                                                                           \
+    do {                                                                                                       \
+        if (!set || smem > set[M]) {                                                                           \
+            e = cudaFuncSetAttribute(field_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+            if (e != cudaSuccess) return e;                                                                    \
+            if (set) set[M] = smem;                                                                            \
+        }                                                                                                      \
+        field_kernel<M><<<grid, kFieldThreads, smem, s>>>(P, m, m32, t, cpc, o0, o1, o2, o3, h32, pref);       \
     } while (0)
     switch (mode) {
         case 0: MT_LAUNCH(0); break;
