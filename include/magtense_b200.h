@@ -133,6 +133,45 @@ int mt_integrate_ragged(mt_handle* const* hs, int ninst, const double* t, int nt
                         double tol, double thres, double* t_out, double* const* y_out_dev, int* flags,
                         mt_stats* stats, int options, void* stream);
 
+/* Row shards of ONE instance over `world` ranks, one GPU each (1 < world <= 8).
+ * Rank r keeps the tensor rows of the receiver cells
+ * [n*r/world, n*(r+1)/world) only (24 n^2 / world bytes), and integrates those
+ * cells; each stage argument is all-gathered by peer stores into every rank's
+ * exchange region, and the error norms are combined over all ranks, so every
+ * rank takes the same adaptive steps as the whole instance.  No counterpart in
+ * the reference, which holds the whole tensor in one process
+ * (LandauLifshitzEquationSolver.f90:881-986, MagTenseCudaBlas.cu:29-92).
+ *
+ * Order on each rank: mt_create, mt_set_row_shard, mt_set_material,
+ * mt_set_dynamics, mt_assemble_demag (own rows), mt_shard_region, then the
+ * peers' regions through mt_shard_open_peers (IPC handles from
+ * mt_shard_ipc_handle, one process per GPU) or mt_shard_set_peers (pointers
+ * the caller has mapped), then mt_integrate on every rank at the same time:
+ * each rank fills its own cells' rows of y_out (and the whole first sample).
+ * A sharded handle serves no other compute entry point (MT_ERR_UNSUPPORTED).
+ * A wait for the other ranks gives up after 10 s (environment variable
+ * MAGTENSE_B200_SHARD_TIMEOUT_S, read by mt_integrate, sets another bound) with
+ * MT_ERR_TIMEOUT; the ranks' barrier epochs then differ: destroy the handles. */
+int mt_set_row_shard(mt_handle* h, int rank, int world);
+/* This rank's exchange region (device memory, allocated on the first call). */
+int mt_shard_region(mt_handle* h, void** region_dev, size_t* bytes);
+/* cudaIpcMemHandle_t of the region (64 bytes into handle_out). */
+int mt_shard_ipc_handle(mt_handle* h, void* handle_out);
+/* Map the peers' regions from their IPC handles (world * 64 bytes, rank order;
+ * this rank's entry is ignored). */
+int mt_shard_open_peers(mt_handle* h, const void* handles);
+/* Peer regions given as device pointers valid in this process (world entries,
+ * rank order; this rank's entry must be its own region). */
+int mt_shard_set_peers(mt_handle* h, void* const* regions_dev);
+/* All `world` ranks of a row-sharded instance on ONE device, as CTA groups of one
+ * cooperative launch (the multi-GPU code path, with peer stores into local
+ * memory).  hs: the ranks' handles in rank order, peers set with
+ * mt_shard_set_peers; y_out_dev (nt * 3n) is shared, each rank writing its own
+ * rows; other arguments as mt_integrate, statistics of rank 0. */
+int mt_integrate_shards_local(mt_handle* const* hs, int world, const double* t, int nt, const double* m0_dev,
+                              double tol, double thres, const double* t_conv, int nt_conv, double conv_tol,
+                              double* t_out, double* y_out_dev, int* flags, mt_stats* stats, void* stream);
+
 /* Allocation-free dm/dt.  No counterpart in the reference: it exists for
  * callers that may not allocate device memory (for example code running while
  * a CUDA graph is captured, or a host framework that owns all device memory

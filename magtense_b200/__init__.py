@@ -15,7 +15,8 @@ def __getattr__(name):
     if name in ("MicromagProblem", "load_demag_tensor", "save_demag_tensor"):
         from . import micromag
         return getattr(micromag, name)
-    if name in ("Solver", "BatchSolver", "grid_points", "integrate_ragged"):
+    if name in ("Solver", "BatchSolver", "grid_points", "integrate_ragged", "shard_rows", "link_shards_local",
+                "integrate_shards_local"):
         from . import solver
         return getattr(solver, name)
     if name in ("TrajectoryProblem", "mean_m_trajectory", "LLTrajectory"):

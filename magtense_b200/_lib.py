@@ -72,6 +72,13 @@ SIGNATURES = {
                             C.POINTER(VP), I, C.POINTER(Stats), C.c_int, VP],
     "mt_integrate": [VP, D, C.c_int, VP, C.c_double, C.c_double, D, C.c_int, C.c_double, D, VP, I,
                      C.POINTER(Stats), VP],
+    "mt_set_row_shard": [VP, C.c_int, C.c_int],
+    "mt_shard_region": [VP, C.POINTER(VP), C.POINTER(C.c_size_t)],
+    "mt_shard_ipc_handle": [VP, VP],
+    "mt_shard_open_peers": [VP, VP],
+    "mt_shard_set_peers": [VP, C.POINTER(VP)],
+    "mt_integrate_shards_local": [C.POINTER(VP), C.c_int, D, C.c_int, VP, C.c_double, C.c_double, D, C.c_int,
+                                  C.c_double, D, VP, I, C.POINTER(Stats), VP],
     "mt_batch_create": [C.POINTER(Grid), C.c_int, C.c_int, C.POINTER(VP)],
     "mt_batch_destroy": [VP],
     "mt_batch_set_material": [VP, C.c_double, D, D, D],

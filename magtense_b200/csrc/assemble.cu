@@ -135,13 +135,13 @@ __device__ double axis_coord(int i, int nn, double L, double d)
 
 struct GridDesc { int nx, ny, nz; double L[3], d[3]; };
 
-// One thread per (receiver i, source j); blockIdx.y = receiver.
-__global__ void __launch_bounds__(128) assemble_kernel(GridDesc g, int n, int ldk, float* __restrict__ K)
+// One thread per (receiver i, source j); blockIdx.y = receiver - row0.
+__global__ void __launch_bounds__(128) assemble_kernel(GridDesc g, int n, int ldk, int row0, float* __restrict__ K)
 {
-    const int i = blockIdx.y;
+    const int i = row0 + blockIdx.y;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= ldk) return;
-    float* rowbase = K + ((size_t)i * 6) * ldk + j;
+    float* rowbase = K + ((size_t)blockIdx.y * 6) * ldk + j;
     if (j >= n) {
         for (int c = 0; c < 6; ++c) rowbase[(size_t)c * ldk] = 0.0f;
         return;
@@ -192,15 +192,16 @@ __global__ void rows_to_colmajor(const float* __restrict__ K, int c, int n, int 
 }  // namespace
 
 // Host launchers (called from capi.cu)
-cudaError_t launch_assemble(int nx, int ny, int nz, const double L[3], const double d[3], int n, int ldk, float* K,
-                            cudaStream_t s)
+cudaError_t launch_assemble(int nx, int ny, int nz, const double L[3], const double d[3], int n, int ldk, int row0,
+                            int nrows, float* K, cudaStream_t s)
 {
+    if (row0 < 0 || nrows < 1 || row0 + nrows > n) return cudaErrorInvalidValue;
     GridDesc g;
     g.nx = nx; g.ny = ny; g.nz = nz;
     for (int a = 0; a < 3; ++a) { g.L[a] = L[a]; g.d[a] = d[a]; }
     dim3 block(128);
-    dim3 grid((ldk + 127) / 128, n);
-    assemble_kernel<<<grid, block, 0, s>>>(g, n, ldk, K);
+    dim3 grid((ldk + 127) / 128, nrows);
+    assemble_kernel<<<grid, block, 0, s>>>(g, n, ldk, row0, K);
     return cudaGetLastError();
 }
 

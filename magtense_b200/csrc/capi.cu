@@ -79,6 +79,14 @@ struct mt_handle {
     double* vjp_buf = nullptr;   // [lam (3n) | g_Ms (n)]
     double* vjp_z = nullptr;     // Jfact g_he (3n)
     float* vjp_v32 = nullptr;    // Ms g_he, FP32 [3][ldk] (padding stays 0)
+    // row shards of one instance (shard_world > 1): this rank's cells and tensor rows only
+    int shard_rank = 0, shard_world = 1, shard_cell0 = 0, shard_ncell = 0;
+    unsigned char* shard_region = nullptr;          // this rank's exchange region
+    void* shard_peer[kMaxShards] = {};              // every rank's region, this rank's included
+    bool shard_ipc[kMaxShards] = {};                // mapped here by cudaIpcOpenMemHandle
+    bool shard_peers_set = false, shard_broken = false;
+    ShardLink* shard_link = nullptr;                // device copy of the link
+    long long shard_xseq = 0, shard_rseq = 0;       // barrier and reduction counts after the last run
 };
 
 namespace {
@@ -99,6 +107,7 @@ DevProb make_prob(const mt_handle* h)
     memset(&P, 0, sizeof(P));
     P.n = h->n; P.nx = h->nx; P.ny = h->ny; P.nz = h->nz; P.ldk = h->ldk;
     P.K = h->K;
+    P.krow0 = h->shard_cell0;
     const int nn[3] = {h->nx, h->ny, h->nz};
     for (int a = 0; a < 3; ++a) {
         const double d2 = h->d[a] * h->d[a];
@@ -122,10 +131,21 @@ int check_ready(const mt_handle* h, bool need_material, bool need_dynamics)
     return MT_OK;
 }
 
+bool sharded(const mt_handle* h) { return h && h->shard_world > 1; }
+
+int refuse_sharded(const mt_handle* h, const char* what)
+{
+    if (sharded(h)) return fail(MT_ERR_UNSUPPORTED, "%s: the handle is a row shard (only mt_integrate runs it)", what);
+    return MT_OK;
+}
+
+// tensor rows the handle holds
+int tensor_rows(const mt_handle* h) { return sharded(h) ? h->shard_ncell : h->n; }
+
 int ensure_tensor(mt_handle* h)
 {
     if (h->K) return MT_OK;
-    const size_t cnt = (size_t)h->n * 6 * (size_t)h->ldk;
+    const size_t cnt = (size_t)tensor_rows(h) * 6 * (size_t)h->ldk;
     CUDA_TRY(dalloc(&h->K, cnt));
     return MT_OK;
 }
@@ -176,6 +196,9 @@ int mt_destroy(mt_handle* h)
     free_ptr(h->Jfact); free_ptr(h->Kfact); free_ptr(h->Mfact); free_ptr(h->A6);
     free_ptr(h->hext); free_ptr(h->alpha_tab); free_ptr(h->K); free_ptr(h->m32);
     free_ptr(h->vjp_buf); free_ptr(h->vjp_z); free_ptr(h->vjp_v32);
+    for (int p = 0; p < kMaxShards; ++p)
+        if (h->shard_ipc[p]) cudaIpcCloseMemHandle(h->shard_peer[p]);
+    free_ptr(h->shard_region); free_ptr(h->shard_link);
     delete h;
     return MT_OK;
 }
@@ -242,7 +265,8 @@ int mt_assemble_demag(mt_handle* h, void* stream)
     if (!h) return fail(MT_ERR_ARG, "null handle");
     int rc = ensure_tensor(h);
     if (rc) return rc;
-    CUDA_TRY(launch_assemble(h->nx, h->ny, h->nz, h->L, h->d, h->n, h->ldk, h->K, (cudaStream_t)stream));
+    CUDA_TRY(launch_assemble(h->nx, h->ny, h->nz, h->L, h->d, h->n, h->ldk, h->shard_cell0, tensor_rows(h), h->K,
+                             (cudaStream_t)stream));
     h->have_K = true;
     return MT_OK;
 }
@@ -251,6 +275,7 @@ int mt_load_demag_colmajor(mt_handle* h, const float* Kxx, const float* Kxy, con
                            const float* Kyz, const float* Kzz)
 {
     if (!h || !Kxx || !Kxy || !Kxz || !Kyy || !Kyz || !Kzz) return fail(MT_ERR_ARG, "null argument");
+    if (int rc = refuse_sharded(h, "mt_load_demag_colmajor")) return rc;
     int rc = ensure_tensor(h);
     if (rc) return rc;
     const float* blocks[6] = {Kxx, Kxy, Kxz, Kyy, Kyz, Kzz};
@@ -271,6 +296,7 @@ int mt_load_demag_colmajor(mt_handle* h, const float* Kxx, const float* Kxy, con
 int mt_get_demag_colmajor(mt_handle* h, float* Kxx, float* Kxy, float* Kxz, float* Kyy, float* Kyz, float* Kzz)
 {
     if (!h || !Kxx || !Kxy || !Kxz || !Kyy || !Kyz || !Kzz) return fail(MT_ERR_ARG, "null argument");
+    if (int rc = refuse_sharded(h, "mt_get_demag_colmajor")) return rc;
     if (!h->have_K) return fail(MT_ERR_STATE, "no demag tensor");
     float* blocks[6] = {Kxx, Kxy, Kxz, Kyy, Kyz, Kzz};
     float* tmp = nullptr;
@@ -289,6 +315,7 @@ int mt_demag_field(mt_handle* h, const double* m_dev, double* H_dev, void* strea
 {
     int rc = check_ready(h, true, false);
     if (rc) return rc;
+    if ((rc = refuse_sharded(h, "mt_demag_field"))) return rc;
     if (!m_dev || !H_dev) return fail(MT_ERR_ARG, "null device pointer");
     if ((rc = ensure_m32(h))) return rc;
     cudaStream_t s = (cudaStream_t)stream;
@@ -302,6 +329,7 @@ int mt_fields(mt_handle* h, double t, const double* m_dev, double* Hj, double* H
 {
     int rc = check_ready(h, true, true);
     if (rc) return rc;
+    if ((rc = refuse_sharded(h, "mt_fields"))) return rc;
     if (!m_dev || !Hj || !Hh || !Hk || !Hm) return fail(MT_ERR_ARG, "null device pointer");
     if ((rc = ensure_m32(h))) return rc;
     cudaStream_t s = (cudaStream_t)stream;
@@ -315,6 +343,7 @@ int mt_rhs(mt_handle* h, double t, const double* m_dev, double* dmdt_dev, void* 
 {
     int rc = check_ready(h, true, true);
     if (rc) return rc;
+    if ((rc = refuse_sharded(h, "mt_rhs"))) return rc;
     if (!m_dev || !dmdt_dev) return fail(MT_ERR_ARG, "null device pointer");
     if ((rc = ensure_m32(h))) return rc;
     cudaStream_t s = (cudaStream_t)stream;
@@ -329,6 +358,7 @@ int mt_rhs_vjp(mt_handle* h, double t, const double* m_dev, const double* lam_de
 {
     int rc = check_ready(h, true, true);
     if (rc) return rc;
+    if ((rc = refuse_sharded(h, "mt_rhs_vjp"))) return rc;
     if (!m_dev || !lam_dev || !gm_dev || !ghe_dev || !gms_dev) return fail(MT_ERR_ARG, "null device pointer");
     if ((rc = ensure_m32(h))) return rc;
     const size_t n = (size_t)h->n;
@@ -433,10 +463,21 @@ int integ_prepare(mt_handle* h, const double* t, int nt, const double* m0_dev, d
     IntegAlloc& A = R.A;
     IntegBufs& B = R.B;
     memset(&B, 0, sizeof(B));
-    for (int k = 0; k < 4; ++k) {
-        CUDA_TRY(A.get(&B.pool[k], n3));
-        CUDA_TRY(A.get(&B.pool32[k], 3 * (size_t)h->ldk));
-        CUDA_TRY(cudaMemsetAsync(B.pool32[k], 0, sizeof(float) * 3 * h->ldk, s));
+    if (sharded(h)) {   // stage arguments and partials in the exchange region, which peers write into
+        const ShardLayout lay = shard_layout(n, h->ldk, h->shard_world);
+        for (int k = 0; k < 4; ++k) {
+            B.pool[k] = reinterpret_cast<double*>(h->shard_region + lay.pool) + (size_t)k * n3;
+            B.pool32[k] = reinterpret_cast<float*>(h->shard_region + lay.pool32) + (size_t)k * 3 * h->ldk;
+        }
+        CUDA_TRY(cudaMemsetAsync(B.pool32[0], 0, sizeof(float) * 4 * 3 * (size_t)h->ldk, s));
+        B.partials = reinterpret_cast<double*>(h->shard_region + lay.partials);
+        B.link = h->shard_link;
+    } else {
+        for (int k = 0; k < 4; ++k) {
+            CUDA_TRY(A.get(&B.pool[k], n3));
+            CUDA_TRY(A.get(&B.pool32[k], 3 * (size_t)h->ldk));
+            CUDA_TRY(cudaMemsetAsync(B.pool32[k], 0, sizeof(float) * 3 * h->ldk, s));
+        }
     }
     for (int k = 0; k < 3; ++k) CUDA_TRY(A.get(&B.deriv[k], n3));
     for (int k = 2; k <= 11; ++k) if (k != 8) CUDA_TRY(A.get(&B.stg[k], n3));
@@ -446,7 +487,7 @@ int integ_prepare(mt_handle* h, const double* t, int nt, const double* m0_dev, d
     CUDA_TRY(A.get(&B.ylast, n3));
     CUDA_TRY(A.get(&B.ystep, n3));
     B.y_out = y_out_dev;
-    CUDA_TRY(A.get(&B.partials, 2 * (size_t)grid * 4));
+    if (!sharded(h)) CUDA_TRY(A.get(&B.partials, 2 * (size_t)grid * 4));
     CUDA_TRY(A.get(&B.gs, 1));
     CUDA_TRY(A.get(&B.state, 1));
     double* d_comb = nullptr; int* d_cflags = nullptr;
@@ -478,6 +519,7 @@ int integ_prepare(mt_handle* h, const double* t, int nt, const double* m0_dev, d
     st.dyp = 0; st.dypold = 1; st.d8 = 2;
     st.ci = 1; st.ko = 1;
     st.converged_at = -1;
+    st.xseq = h->shard_xseq; st.rseq = h->shard_rseq;
     CUDA_TRY(cudaMemcpyAsync(B.state, &st, sizeof(st), cudaMemcpyHostToDevice, s));
 
     IntegParams& Q = R.Q;
@@ -487,14 +529,17 @@ int integ_prepare(mt_handle* h, const double* t, int nt, const double* m0_dev, d
     Q.comb_t = d_comb; Q.comb_flags = d_cflags; Q.ncomb = (int)comb.size(); Q.nt = nt;
     Q.t_out = d_tout; Q.flags_out = d_flags;
     Q.renorm = h->renorm;
+    // cells the grid's CTAs share; for row shards the largest rank's, so that every
+    // rank gets the same evaluation budget per launch and they stop together
+    const int cells = sharded(h) ? (n + h->shard_world - 1) / h->shard_world : n;
     {   // about 0.25 s of work per launch
-        const double bytes = 24.0 * (double)n * (double)h->ldk;
+        const double bytes = 24.0 * (double)cells * (double)h->ldk;
         const double t_eval = bytes / 3.0e12 + 15e-6;
         long long b = (long long)(0.25 / t_eval);
         Q.evals_per_launch = std::min(100000LL, std::max(64LL, b));
     }
     // co-residency of the persistent grid
-    const size_t smem = integrate_smem_bytes(n, h->ldk, grid);
+    const size_t smem = integrate_smem_bytes(cells, h->ldk, grid);
     R.smem = smem;
     if (smem > 227 * 1024) return fail(MT_ERR_UNSUPPORTED, "integrator shared memory %zu exceeds 227 KB", smem);
     R.P = make_prob(h);
@@ -525,6 +570,158 @@ int integ_finish(IntegRun& R, const RKS& hs, const double* t, int nt, double* t_
     return MT_OK;
 }
 
+// ---- row shards ----
+
+int shard_ready(const mt_handle* h)
+{
+    if (!h->shard_region) return fail(MT_ERR_STATE, "row shard: call mt_shard_region first");
+    if (!h->shard_peers_set) return fail(MT_ERR_STATE, "row shard: the peers' regions are not set");
+    if (h->shard_broken) return fail(MT_ERR_STATE, "row shard: an earlier run gave up; destroy the ranks' handles");
+    return MT_OK;
+}
+
+// CTAs per rank: the same on every rank (from the largest rank's cells)
+int shard_grid(const mt_handle* h, int sms)
+{
+    return std::min(kShardMaxCtas, integrate_grid_size((h->n + h->shard_world - 1) / h->shard_world, sms));
+}
+
+// the device link of this rank for a launch of `grid` CTAs per rank
+int build_link(mt_handle* h, int grid)
+{
+    const ShardLayout lay = shard_layout(h->n, h->ldk, h->shard_world);
+    ShardLink L;
+    memset(&L, 0, sizeof(L));
+    L.rank = h->shard_rank; L.world = h->shard_world;
+    L.cell0 = h->shard_cell0; L.ncell = h->shard_ncell;
+    L.cta_base = h->shard_rank * grid; L.cta_total = h->shard_world * grid;
+    // ranks may enter a run some time apart: 10 s by default, MAGTENSE_B200_SHARD_TIMEOUT_S overrides
+    double tmo_s = 10.0;
+    if (const char* e = getenv("MAGTENSE_B200_SHARD_TIMEOUT_S")) {
+        const double v = atof(e);
+        if (v > 0.0 && v <= 600.0) tmo_s = v;
+    }
+    L.timeout_ns = (unsigned long long)(tmo_s * 1e9);
+    for (int p = 0; p < h->shard_world; ++p) {
+        unsigned char* base = static_cast<unsigned char*>(h->shard_peer[p]);
+        for (int k = 0; k < 4; ++k) {
+            L.pool[p][k] = reinterpret_cast<double*>(base + lay.pool) + (size_t)k * 3 * h->n;
+            L.pool32[p][k] = reinterpret_cast<float*>(base + lay.pool32) + (size_t)k * 3 * h->ldk;
+        }
+        L.partials[p] = reinterpret_cast<double*>(base + lay.partials);
+        L.flags[p] = reinterpret_cast<unsigned*>(base + lay.flags);
+    }
+    if (!h->shard_link) CUDA_TRY(dalloc(&h->shard_link, 1));
+    CUDA_TRY(cudaMemcpy(h->shard_link, &L, sizeof(L), cudaMemcpyHostToDevice));
+    return MT_OK;
+}
+
+// Barrier and RKSUITE state of a CTA group after a launch.
+struct GroupBack { GridSync gs; RKS st; };
+
+// Integrates prepared runs as CTA groups of one cooperative launch on one device,
+// relaunched until every group has finished (replayed from a CUDA graph when
+// `graph`).  runs[k]->grid CTAs go to group k.  back receives each group's final
+// barrier and state.
+int run_groups(const std::vector<IntegRun*>& runs, bool graph, cudaStream_t cs, std::vector<GroupBack>& back_out,
+               long long& launches, double& kernel_ms)
+{
+    const int ninst = (int)runs.size();
+    size_t smem = 0;
+    int used = 0;
+    for (IntegRun* r : runs) { smem = std::max(smem, r->smem); used += r->grid; }
+    std::vector<RaggedInst> tab(ninst);
+    std::vector<int> cta_inst(used);
+    for (int k = 0, c0 = 0; k < ninst; ++k) {
+        tab[k].P = runs[k]->P; tab[k].B = runs[k]->B; tab[k].Q = runs[k]->Q;
+        tab[k].cta0 = c0; tab[k].ncta = runs[k]->grid;
+        for (int j = 0; j < runs[k]->grid; ++j) cta_inst[c0 + j] = k;
+        c0 += runs[k]->grid;
+    }
+    IntegAlloc A;
+    RaggedInst* d_tab = nullptr;
+    int* d_cta = nullptr;
+    CUDA_TRY(A.get(&d_tab, (size_t)ninst));
+    CUDA_TRY(A.get(&d_cta, (size_t)used));
+    CUDA_TRY(cudaMemcpyAsync(d_tab, tab.data(), sizeof(RaggedInst) * ninst, cudaMemcpyHostToDevice, cs));
+    CUDA_TRY(cudaMemcpyAsync(d_cta, cta_inst.data(), sizeof(int) * used, cudaMemcpyHostToDevice, cs));
+    // pinned read-back of every group's barrier and RKSUITE state after a launch
+    GroupBack* back = nullptr;
+    CUDA_TRY(cudaMallocHost((void**)&back, sizeof(GroupBack) * ninst));
+    struct HostFree { void* p; ~HostFree() { cudaFreeHost(p); } } hf{back};
+    // private stream (the caller's may be the legacy default stream, which cannot be captured)
+    cudaStream_t s = nullptr;
+    CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamDestroy(s); } } sg{s};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evc = nullptr;
+    CUDA_TRY(cudaEventCreate(&ev0));
+    CUDA_TRY(cudaEventCreate(&ev1));
+    CUDA_TRY(cudaEventCreateWithFlags(&evc, cudaEventDisableTiming));
+    struct EvGuard { cudaEvent_t a, b, c; ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); cudaEventDestroy(c); } }
+        evg{ev0, ev1, evc};
+    CUDA_TRY(cudaEventRecord(evc, cs));
+    CUDA_TRY(cudaStreamWaitEvent(s, evc, 0));
+    auto enqueue = [&]() -> cudaError_t {
+        cudaError_t e = cudaSuccess;
+        for (int k = 0; k < ninst && e == cudaSuccess; ++k) e = cudaMemsetAsync(runs[k]->B.gs, 0, sizeof(GridSync), s);
+        if (e == cudaSuccess) e = launch_integrate_ragged(d_tab, d_cta, used, smem, s);
+        for (int k = 0; k < ninst && e == cudaSuccess; ++k) {
+            e = cudaMemcpyAsync(&back[k].gs, runs[k]->B.gs, sizeof(GridSync), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(&back[k].st, runs[k]->B.state, sizeof(RKS), cudaMemcpyDeviceToHost, s);
+        }
+        return e;
+    };
+    cudaGraphExec_t gexec = nullptr;
+    struct GraphGuard { cudaGraphExec_t g; ~GraphGuard() { if (g) cudaGraphExecDestroy(g); } } gg{nullptr};
+    if (graph) {
+        cudaGraph_t gr = nullptr;
+        CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = enqueue();
+        cudaError_t e2 = cudaStreamEndCapture(s, &gr);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (gr) cudaGraphDestroy(gr);
+            cudaGetLastError();
+            return fail(MT_ERR_CUDA, "capturing the group launch: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+        }
+        e = cudaGraphInstantiate(&gexec, gr, 0);
+        cudaGraphDestroy(gr);
+        if (e != cudaSuccess) return fail(MT_ERR_CUDA, "instantiating the group launch: %s", cudaGetErrorString(e));
+        gg.g = gexec;
+    }
+    kernel_ms = 0.0;
+    launches = 0;
+    std::vector<long long> last(ninst, -1);
+    back_out.assign(ninst, GroupBack());
+    for (;;) {
+        CUDA_TRY(cudaEventRecord(ev0, s));
+        if (gexec) CUDA_TRY(cudaGraphLaunch(gexec, s));
+        else CUDA_TRY(enqueue());
+        CUDA_TRY(cudaEventRecord(ev1, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        float ms = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, ev0, ev1));
+        kernel_ms += ms;
+        launches++;
+        bool all = true, progress = false;
+        for (int k = 0; k < ninst; ++k) {
+            const GroupBack& bk = back[k];
+            back_out[k] = bk;
+            if (bk.gs.err != 0 || bk.gs.abort)
+                return fail(MT_ERR_TIMEOUT, "group %d: barrier gave up (code %d at %d)", k, bk.gs.err, bk.gs.err_where);
+            if (!bk.st.finished) all = false;
+            const long long sig = bk.st.full_f_count + bk.st.f_count + bk.st.ci;
+            if (sig != last[k]) progress = true;
+            last[k] = sig;
+        }
+        if (all) break;
+        if (!progress) return fail(MT_ERR_SOLVER, "grouped integrator made no progress");
+    }
+    CUDA_TRY(cudaEventRecord(evc, s));
+    CUDA_TRY(cudaStreamWaitEvent(cs, evc, 0));
+    return MT_OK;
+}
+
 
 
 }  // namespace
@@ -540,9 +737,14 @@ int mt_integrate(mt_handle* h, const double* t, int nt, const double* m0_dev, do
     if (!t || nt < 2 || !m0_dev || !t_out || !y_out_dev || !stats) return fail(MT_ERR_ARG, "bad argument (nt >= 2 required)");
     if (nt_conv < 0 || (nt_conv > 0 && !t_conv)) return fail(MT_ERR_ARG, "bad convergence-time list");
     cudaStream_t s = (cudaStream_t)stream;
+    int grid0 = integrate_grid_size(h->n, h->num_sms);
+    if (sharded(h)) {   // this rank's part of a row-sharded instance; the peers run theirs at the same time
+        if ((rc = shard_ready(h))) return rc;
+        grid0 = shard_grid(h, h->num_sms);
+        if ((rc = build_link(h, grid0))) return rc;
+    }
     IntegRun R;
-    int prc = integ_prepare(h, t, nt, m0_dev, tol, thres, t_conv, nt_conv, conv_tol, y_out_dev,
-                            integrate_grid_size(h->n, h->num_sms), R, stats, s);
+    int prc = integ_prepare(h, t, nt, m0_dev, tol, thres, t_conv, nt_conv, conv_tol, y_out_dev, grid0, R, stats, s);
     if (prc) return prc;
     DevProb P = R.P;
     IntegBufs& B = R.B;
@@ -572,14 +774,22 @@ int mt_integrate(mt_handle* h, const double* t, int nt, const double* m0_dev, do
         launches++;
         stats->launches = launches;
         stats->kernel_ms = kernel_ms;
-        if (gs_h.err != 0 || gs_h.abort)
-            return fail(MT_ERR_TIMEOUT, "integrator grid barrier gave up (code %d at %d)", gs_h.err, gs_h.err_where);
+        if (gs_h.err != 0 || gs_h.abort) {
+            h->shard_broken = sharded(h);
+            return fail(MT_ERR_TIMEOUT, "integrator %s barrier gave up (code %d at %d)",
+                        gs_h.err == KERR_PEER_TIMEOUT ? "cross-rank" : "grid", gs_h.err, gs_h.err_where);
+        }
         if (hs.finished) break;
         const long long evals = hs.full_f_count + hs.f_count;
-        if (evals == last_evals && hs.ci == last_ci) return fail(MT_ERR_SOLVER, "integrator made no progress");
+        if (evals == last_evals && hs.ci == last_ci) {
+            h->shard_broken = sharded(h);
+            return fail(MT_ERR_SOLVER, "integrator made no progress");
+        }
         last_evals = evals;
         last_ci = hs.ci;
     }
+    h->shard_xseq = hs.xseq;
+    h->shard_rseq = hs.rseq;
     return integ_finish(R, hs, t, nt, t_out, flags, stats);
 }
 
@@ -594,6 +804,7 @@ int mt_integrate_ragged(mt_handle* const* hs, int ninst, const double* t, int nt
     for (int k = 0; k < ninst; ++k) {
         if (!hs[k] || !m0_dev[k] || !y_out_dev[k]) return fail(MT_ERR_ARG, "null handle or buffer of instance %d", k);
         if ((rc = check_ready(hs[k], true, true))) return rc;
+        if ((rc = refuse_sharded(hs[k], "mt_integrate_ragged"))) return rc;
         if (hs[k]->device != hs[0]->device) return fail(MT_ERR_ARG, "all instances must live on one device");
     }
     const int G = hs[0]->num_sms;
@@ -623,105 +834,21 @@ int mt_integrate_ragged(mt_handle* const* hs, int ninst, const double* t, int nt
     }
     cudaStream_t cs = (cudaStream_t)stream;
     std::vector<std::unique_ptr<IntegRun>> runs(ninst);
-    size_t smem = 0;
-    std::vector<RaggedInst> tab(ninst);
-    std::vector<int> cta_inst(used);
-    int c0 = 0;
+    std::vector<IntegRun*> rp(ninst);
     for (int k = 0; k < ninst; ++k) {
         runs[k].reset(new IntegRun());
+        rp[k] = runs[k].get();
         if ((rc = integ_prepare(hs[k], t, nt, m0_dev[k], tol, thres, nullptr, 0, 0.0, y_out_dev[k], ncta[k], *runs[k],
                                 &stats[k], cs)))
             return rc;
-        smem = std::max(smem, runs[k]->smem);
         // about 0.25 s per launch for this group: 24 n^2 bytes per evaluation over ncta SMs
         const double t_eval = 24.0 * (double)hs[k]->n * (double)hs[k]->ldk / (ncta[k] * 30.0e9) + 15e-6;
         runs[k]->Q.evals_per_launch = std::min(100000LL, std::max(64LL, (long long)(0.25 / t_eval)));
-        tab[k].P = runs[k]->P; tab[k].B = runs[k]->B; tab[k].Q = runs[k]->Q;
-        tab[k].cta0 = c0; tab[k].ncta = ncta[k];
-        for (int j = 0; j < ncta[k]; ++j) cta_inst[c0 + j] = k;
-        c0 += ncta[k];
     }
-    IntegAlloc A;
-    RaggedInst* d_tab = nullptr;
-    int* d_cta = nullptr;
-    CUDA_TRY(A.get(&d_tab, (size_t)ninst));
-    CUDA_TRY(A.get(&d_cta, (size_t)used));
-    CUDA_TRY(cudaMemcpyAsync(d_tab, tab.data(), sizeof(RaggedInst) * ninst, cudaMemcpyHostToDevice, cs));
-    CUDA_TRY(cudaMemcpyAsync(d_cta, cta_inst.data(), sizeof(int) * used, cudaMemcpyHostToDevice, cs));
-    // pinned read-back of every instance's barrier and RKSUITE state after a launch
-    struct Back { GridSync gs; RKS st; };
-    Back* back = nullptr;
-    CUDA_TRY(cudaMallocHost((void**)&back, sizeof(Back) * ninst));
-    struct HostFree { void* p; ~HostFree() { cudaFreeHost(p); } } hf{back};
-    // private stream (the caller's may be the legacy default stream, which cannot be captured)
-    cudaStream_t s = nullptr;
-    CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamDestroy(s); } } sg{s};
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evc = nullptr;
-    CUDA_TRY(cudaEventCreate(&ev0));
-    CUDA_TRY(cudaEventCreate(&ev1));
-    CUDA_TRY(cudaEventCreateWithFlags(&evc, cudaEventDisableTiming));
-    struct EvGuard { cudaEvent_t a, b, c; ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); cudaEventDestroy(c); } }
-        evg{ev0, ev1, evc};
-    CUDA_TRY(cudaEventRecord(evc, cs));
-    CUDA_TRY(cudaStreamWaitEvent(s, evc, 0));
-    auto enqueue = [&]() -> cudaError_t {
-        cudaError_t e = cudaSuccess;
-        for (int k = 0; k < ninst && e == cudaSuccess; ++k) e = cudaMemsetAsync(runs[k]->B.gs, 0, sizeof(GridSync), s);
-        if (e == cudaSuccess) e = launch_integrate_ragged(d_tab, d_cta, used, smem, s);
-        for (int k = 0; k < ninst && e == cudaSuccess; ++k) {
-            e = cudaMemcpyAsync(&back[k].gs, runs[k]->B.gs, sizeof(GridSync), cudaMemcpyDeviceToHost, s);
-            if (e == cudaSuccess)
-                e = cudaMemcpyAsync(&back[k].st, runs[k]->B.state, sizeof(RKS), cudaMemcpyDeviceToHost, s);
-        }
-        return e;
-    };
-    cudaGraphExec_t gexec = nullptr;
-    struct GraphGuard { cudaGraphExec_t g; ~GraphGuard() { if (g) cudaGraphExecDestroy(g); } } gg{nullptr};
-    if (options & MT_RAGGED_GRAPH) {
-        cudaGraph_t graph = nullptr;
-        CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        cudaError_t e = enqueue();
-        cudaError_t e2 = cudaStreamEndCapture(s, &graph);
-        if (e != cudaSuccess || e2 != cudaSuccess) {
-            if (graph) cudaGraphDestroy(graph);
-            cudaGetLastError();
-            return fail(MT_ERR_CUDA, "capturing the ragged launch: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
-        }
-        e = cudaGraphInstantiate(&gexec, graph, 0);
-        cudaGraphDestroy(graph);
-        if (e != cudaSuccess) return fail(MT_ERR_CUDA, "instantiating the ragged launch: %s", cudaGetErrorString(e));
-        gg.g = gexec;
-    }
-    double kernel_ms = 0.0;
+    std::vector<GroupBack> back;
     long long launches = 0;
-    std::vector<long long> last(ninst, -1);
-    for (;;) {
-        CUDA_TRY(cudaEventRecord(ev0, s));
-        if (gexec) CUDA_TRY(cudaGraphLaunch(gexec, s));
-        else CUDA_TRY(enqueue());
-        CUDA_TRY(cudaEventRecord(ev1, s));
-        CUDA_TRY(cudaStreamSynchronize(s));
-        float ms = 0.f;
-        CUDA_TRY(cudaEventElapsedTime(&ms, ev0, ev1));
-        kernel_ms += ms;
-        launches++;
-        bool all = true, progress = false;
-        for (int k = 0; k < ninst; ++k) {
-            const Back& bk = back[k];
-            if (bk.gs.err != 0 || bk.gs.abort)
-                return fail(MT_ERR_TIMEOUT, "instance %d: group barrier gave up (code %d at %d)", k, bk.gs.err,
-                            bk.gs.err_where);
-            if (!bk.st.finished) all = false;
-            const long long sig = bk.st.full_f_count + bk.st.f_count + bk.st.ci;
-            if (sig != last[k]) progress = true;
-            last[k] = sig;
-        }
-        if (all) break;
-        if (!progress) return fail(MT_ERR_SOLVER, "ragged integrator made no progress");
-    }
-    CUDA_TRY(cudaEventRecord(evc, s));
-    CUDA_TRY(cudaStreamWaitEvent(cs, evc, 0));
+    double kernel_ms = 0.0;
+    if ((rc = run_groups(rp, (options & MT_RAGGED_GRAPH) != 0, cs, back, launches, kernel_ms))) return rc;
     int worst = MT_OK;
     for (int k = 0; k < ninst; ++k) {
         const int r = integ_finish(*runs[k], back[k].st, t, nt, t_out + (size_t)k * nt, flags ? flags + (size_t)k * nt : nullptr,
@@ -731,6 +858,136 @@ int mt_integrate_ragged(mt_handle* const* hs, int ninst, const double* t, int nt
     stats[0].launches = launches;
     stats[0].kernel_ms = kernel_ms;
     return worst;
+}
+
+int mt_set_row_shard(mt_handle* h, int rank, int world)
+{
+    if (!h) return fail(MT_ERR_ARG, "null handle");
+    if (world < 2 || world > kMaxShards) return fail(MT_ERR_ARG, "world %d outside [2, %d]", world, kMaxShards);
+    if (rank < 0 || rank >= world) return fail(MT_ERR_ARG, "rank %d outside [0, %d)", rank, world);
+    if (h->n < world) return fail(MT_ERR_ARG, "%d cells cannot be split over %d ranks", h->n, world);
+    if (h->K || h->shard_region) return fail(MT_ERR_STATE, "mt_set_row_shard must come before the tensor and the region");
+    h->shard_rank = rank;
+    h->shard_world = world;
+    h->shard_cell0 = (int)(((long long)h->n * rank) / world);
+    h->shard_ncell = (int)(((long long)h->n * (rank + 1)) / world) - h->shard_cell0;
+    return MT_OK;
+}
+
+int mt_shard_region(mt_handle* h, void** region_dev, size_t* bytes)
+{
+    if (!h || !region_dev || !bytes) return fail(MT_ERR_ARG, "null argument");
+    if (!sharded(h)) return fail(MT_ERR_STATE, "not a row shard: call mt_set_row_shard first");
+    const ShardLayout lay = shard_layout(h->n, h->ldk, h->shard_world);
+    if (!h->shard_region) {
+        CUDA_TRY(dalloc(&h->shard_region, lay.bytes));
+        CUDA_TRY(cudaMemset(h->shard_region, 0, lay.bytes));
+        CUDA_TRY(cudaDeviceSynchronize());
+        h->shard_peer[h->shard_rank] = h->shard_region;
+    }
+    *region_dev = h->shard_region;
+    *bytes = lay.bytes;
+    return MT_OK;
+}
+
+int mt_shard_ipc_handle(mt_handle* h, void* handle_out)
+{
+    if (!h || !handle_out) return fail(MT_ERR_ARG, "null argument");
+    if (!h->shard_region) return fail(MT_ERR_STATE, "call mt_shard_region first");
+    static_assert(sizeof(cudaIpcMemHandle_t) == 64, "IPC handle size");
+    cudaIpcMemHandle_t ih;
+    CUDA_TRY(cudaIpcGetMemHandle(&ih, h->shard_region));
+    memcpy(handle_out, &ih, sizeof(ih));
+    return MT_OK;
+}
+
+int mt_shard_open_peers(mt_handle* h, const void* handles)
+{
+    if (!h || !handles) return fail(MT_ERR_ARG, "null argument");
+    if (!h->shard_region) return fail(MT_ERR_STATE, "call mt_shard_region first");
+    if (h->shard_peers_set) return fail(MT_ERR_STATE, "the peers' regions are already set");
+    const unsigned char* hb = static_cast<const unsigned char*>(handles);
+    for (int p = 0; p < h->shard_world; ++p) {
+        if (p == h->shard_rank) continue;
+        cudaIpcMemHandle_t ih;
+        memcpy(&ih, hb + (size_t)p * sizeof(ih), sizeof(ih));
+        void* ptr = nullptr;
+        CUDA_TRY(cudaIpcOpenMemHandle(&ptr, ih, cudaIpcMemLazyEnablePeerAccess));
+        h->shard_peer[p] = ptr;
+        h->shard_ipc[p] = true;
+    }
+    h->shard_peers_set = true;
+    return MT_OK;
+}
+
+int mt_shard_set_peers(mt_handle* h, void* const* regions_dev)
+{
+    if (!h || !regions_dev) return fail(MT_ERR_ARG, "null argument");
+    if (!h->shard_region) return fail(MT_ERR_STATE, "call mt_shard_region first");
+    if (h->shard_peers_set) return fail(MT_ERR_STATE, "the peers' regions are already set");
+    if (regions_dev[h->shard_rank] != h->shard_region)
+        return fail(MT_ERR_ARG, "entry %d must be this rank's own region", h->shard_rank);
+    for (int p = 0; p < h->shard_world; ++p)
+        if (!regions_dev[p]) return fail(MT_ERR_ARG, "null region of rank %d", p);
+    for (int p = 0; p < h->shard_world; ++p) h->shard_peer[p] = regions_dev[p];
+    h->shard_peers_set = true;
+    return MT_OK;
+}
+
+int mt_integrate_shards_local(mt_handle* const* hs, int world, const double* t, int nt, const double* m0_dev,
+                              double tol, double thres, const double* t_conv, int nt_conv, double conv_tol,
+                              double* t_out, double* y_out_dev, int* flags, mt_stats* stats, void* stream)
+{
+    if (!hs || world < 2 || world > kMaxShards || !t || nt < 2 || !m0_dev || !t_out || !y_out_dev || !stats)
+        return fail(MT_ERR_ARG, "bad argument (2 <= world <= %d, nt >= 2 required)", kMaxShards);
+    if (nt_conv < 0 || (nt_conv > 0 && !t_conv)) return fail(MT_ERR_ARG, "bad convergence-time list");
+    int rc;
+    for (int r = 0; r < world; ++r) {
+        if (!hs[r]) return fail(MT_ERR_ARG, "null handle of rank %d", r);
+        if ((rc = check_ready(hs[r], true, true))) return rc;
+        if (!sharded(hs[r]) || hs[r]->shard_rank != r || hs[r]->shard_world != world)
+            return fail(MT_ERR_ARG, "handle %d is not rank %d of %d row shards", r, r, world);
+        if (hs[r]->n != hs[0]->n || hs[r]->device != hs[0]->device)
+            return fail(MT_ERR_ARG, "the shards must share one grid and one device");
+        if ((rc = shard_ready(hs[r]))) return rc;
+    }
+    const int grid = shard_grid(hs[0], hs[0]->num_sms / world);
+    if (grid < 1) return fail(MT_ERR_UNSUPPORTED, "%d ranks exceed the %d SMs of one launch", world, hs[0]->num_sms);
+    cudaStream_t cs = (cudaStream_t)stream;
+    std::vector<std::unique_ptr<IntegRun>> runs(world);
+    std::vector<IntegRun*> rp(world);
+    std::vector<mt_stats> st(world);
+    for (int r = 0; r < world; ++r) {
+        if ((rc = build_link(hs[r], grid))) return rc;
+        runs[r].reset(new IntegRun());
+        rp[r] = runs[r].get();
+        if ((rc = integ_prepare(hs[r], t, nt, m0_dev, tol, thres, t_conv, nt_conv, conv_tol, y_out_dev, grid, *runs[r],
+                                &st[r], cs)))
+            return rc;
+    }
+    std::vector<GroupBack> back;
+    long long launches = 0;
+    double kernel_ms = 0.0;
+    rc = run_groups(rp, false, cs, back, launches, kernel_ms);
+    if (rc) {
+        for (int r = 0; r < world; ++r) hs[r]->shard_broken = true;
+        return rc;
+    }
+    for (int r = 0; r < world; ++r) {
+        const RKS& a = back[r].st;
+        const RKS& b = back[0].st;
+        if (a.full_f_count + a.f_count != b.full_f_count + b.f_count || a.step_count != b.step_count ||
+            a.ko != b.ko || a.t != b.t || a.xseq != b.xseq) {
+            for (int q = 0; q < world; ++q) hs[q]->shard_broken = true;
+            return fail(MT_ERR_SOLVER, "row shard %d took different steps from rank 0", r);
+        }
+        hs[r]->shard_xseq = a.xseq;
+        hs[r]->shard_rseq = a.rseq;
+    }
+    rc = integ_finish(*runs[0], back[0].st, t, nt, t_out, flags, stats);
+    stats->launches = launches;
+    stats->kernel_ms = kernel_ms;
+    return rc;
 }
 
 // ---------------------------------------------------------------------------
@@ -1320,6 +1577,7 @@ int noalloc_scratch(int dev, float** out)
 extern "C" int mt_rhs_noalloc(mt_handle* h, double t, const double* m_dev, double* dmdt_dev, void* stream)
 {
     if (!h) return fail(MT_ERR_ARG, "null handle");
+    if (int rc = refuse_sharded(h, "mt_rhs_noalloc")) return rc;
     if (h->n > MT_NOALLOC_MAX_CELLS)
         return fail(MT_ERR_ARG, "n = %d cells exceeds the %d-cell limit of mt_rhs_noalloc (use mt_rhs)", h->n,
                     MT_NOALLOC_MAX_CELLS);

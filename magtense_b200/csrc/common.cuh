@@ -7,7 +7,7 @@
 #define MT_DEV __device__ __forceinline__
 
 // Error codes recorded by kernels in GridSync::err (host maps them to MT_ERR_*).
-enum { KERR_NONE = 0, KERR_BARRIER_TIMEOUT = 1, KERR_BAD_CONFIG = 2, KERR_RANGE = 3 };
+enum { KERR_NONE = 0, KERR_BARRIER_TIMEOUT = 1, KERR_BAD_CONFIG = 2, KERR_RANGE = 3, KERR_PEER_TIMEOUT = 4 };
 
 // Grid-wide barrier state for the persistent cooperative kernels.  count is
 // reset to 0 by the host before every launch.
@@ -29,6 +29,16 @@ MT_DEV unsigned ld_acquire_u32(const unsigned* p)
 MT_DEV void st_release_u32(unsigned* p, unsigned v)
 {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+MT_DEV unsigned ld_acquire_sys_u32(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+MT_DEV void st_release_sys_u32(unsigned* p, unsigned v)
+{
+    asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 MT_DEV int ld_volatile_i32(const int* p) { return *(volatile const int*)p; }
 MT_DEV uint64_t globaltimer_ns()

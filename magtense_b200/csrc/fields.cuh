@@ -13,7 +13,9 @@ int field_cells_per_cta(int n, int num_sms);
 cudaError_t launch_field(int mode, const DevProb& P, const double* m, const float* m32, double t, double* o0,
                          double* o1, double* o2, double* o3, float* h32, float pref, int num_sms, cudaStream_t s);
 
-cudaError_t launch_assemble(int nx, int ny, int nz, const double L[3], const double d[3], int n, int ldk, float* K,
+// tensor rows of the receiver cells [row0, row0 + nrows) into K (nrows * 6 * ldk floats)
+cudaError_t launch_assemble(int nx, int ny, int nz, const double L[3], const double d[3], int n, int ldk, int row0,
+                            int nrows, float* K,
                             cudaStream_t s);
 cudaError_t launch_colmajor_to_rows(const float* blk, int c, int n, int ldk, float* K, cudaStream_t s);
 cudaError_t launch_rows_to_colmajor(const float* K, int c, int n, int ldk, float* blk, cudaStream_t s);

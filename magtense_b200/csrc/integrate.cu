@@ -22,7 +22,10 @@
 //     fixed-order combine done identically by every CTA.
 // Stage arguments alternate between two buffers so that a fast CTA never
 // overwrites an argument a slow CTA is still reading.  All waits are bounded
-// (grid_sync in common.cuh).  The kernel returns after a budget of
+// (grid_sync in common.cuh).  A row-sharded instance (ShardLink in
+// integrate.cuh) runs the same code on every rank with each rank's CTAs owning
+// that rank's cells; its argument stores and reduction partials go to every
+// rank and its barriers span all ranks (sync_all).  The kernel returns after a budget of
 // right-hand-side evaluations with its full state saved, and is relaunched by
 // the host until the run ends.
 #include "common.cuh"
@@ -50,6 +53,10 @@ struct Ctx {
     long long budget_end;       // stop when f_total reaches this
     bool abort;
     int grank, gsize;           // this CTA's rank in the instance's CTA group, and the group size
+    const ShardLink* L;         // row shards, or nullptr
+    int srank, sworld;          // shard rank and count (0, 1 without shards)
+    int slot0, nslots;          // this group's first reduction slot, and the slots over all ranks
+    long long xseq;             // cross-rank barriers passed
 };
 
 // ---- own-element iteration ---------------------------------------------
@@ -60,20 +67,70 @@ struct Ctx {
         if ([[maybe_unused]] const int _a = _e / (X).nc, _i = (X).c0 + (_e - _a * (X).nc), \
                       q = _a * (X).P.n + _i, q32 = _a * (X).P.ldk + _i; true)
 
+// Barrier of all CTAs of the instance.  Row shards: the rank's CTAs meet, the
+// rank's first CTA raises its epoch flag in every rank's region (release at
+// system scope), and every CTA of every rank waits until all ranks' flags carry
+// the epoch (acquire at system scope; bounded by the link's timeout, after which
+// KERR_PEER_TIMEOUT is recorded and the instance aborts).  Each thread fences its
+// peer stores at system scope before it arrives.
+MT_DEV bool sync_all(Ctx& X, int where)
+{
+    if (!X.L) {
+        if (!group_sync(X.B.gs, X.gsize, where)) { X.abort = true; return false; }
+        return true;
+    }
+    __threadfence_system();
+    if (!group_sync(X.B.gs, X.gsize, where)) { X.abort = true; return false; }
+    X.xseq++;
+    const unsigned ep = (unsigned)X.xseq;
+    __shared__ int s_xok;
+    if (threadIdx.x == 0) s_xok = 1;
+    __syncthreads();
+    if (threadIdx.x < X.sworld) {
+        const int p = threadIdx.x;
+        if (X.grank == 0) st_release_sys_u32(X.L->flags[p] + X.srank, ep);
+        const unsigned* f = X.L->flags[X.srank] + p;
+        const unsigned long long tmo = X.L->timeout_ns;
+        long long it = 0;
+        const uint64_t t0 = globaltimer_ns();
+        while ((int)(ld_acquire_sys_u32(f) - ep) < 0) {
+            if (ld_volatile_i32(&X.B.gs->abort)) { s_xok = 0; break; }
+            if ((unsigned long long)(++it) > tmo / 8 || ((it & 1023) == 0 && globaltimer_ns() - t0 > tmo)) {
+                if (atomicCAS(&X.B.gs->err, 0, KERR_PEER_TIMEOUT) == 0) X.B.gs->err_where = where;
+                atomicExch(&X.B.gs->abort, 1);
+                s_xok = 0;
+                break;
+            }
+            __nanosleep(64);
+        }
+    }
+    __syncthreads();
+    if (!s_xok) { X.abort = true; return false; }
+    return true;
+}
+
 template <bool IsMax, int K>
 MT_DEV bool grid_reduce(Ctx& X, double (&v)[K], int where)
 {
     for (int k = 0; k < K; ++k) v[k] = block_reduce<IsMax>(v[k], X.sm_scr);
-    double* buf = X.B.partials + (size_t)(X.rcount & 1) * X.gsize * kRed;
+    const size_t half = (size_t)(X.rcount & 1) * X.nslots * kRed;
+    double* buf = X.B.partials + half;
     X.rcount++;
-    if (threadIdx.x == 0)
-        for (int k = 0; k < K; ++k) buf[X.grank * kRed + k] = v[k];
-    if (!group_sync(X.B.gs, X.gsize, where)) { X.abort = true; return false; }
+    if (threadIdx.x == 0) {
+        const int slot = (X.slot0 + X.grank) * kRed;
+        if (X.L) {
+            for (int p = 0; p < X.sworld; ++p)
+                for (int k = 0; k < K; ++k) X.L->partials[p][half + slot + k] = v[k];
+        } else {
+            for (int k = 0; k < K; ++k) buf[slot + k] = v[k];
+        }
+    }
+    if (!sync_all(X, where)) return false;
     if (threadIdx.x < 32) {
         for (int k = 0; k < K; ++k) {
             double r = IsMax ? 0.0 : 0.0;
             bool have = false;
-            for (int b = threadIdx.x; b < X.gsize; b += 32) {
+            for (int b = threadIdx.x; b < X.nslots; b += 32) {
                 double x = ldcg(&buf[b * kRed + k]);
                 if (IsMax) r = have ? fmax(r, x) : x; else r += x;
                 have = true;
@@ -89,11 +146,7 @@ MT_DEV bool grid_reduce(Ctx& X, double (&v)[K], int where)
     return true;
 }
 
-MT_DEV bool barrier(Ctx& X, int where)
-{
-    if (!group_sync(X.B.gs, X.gsize, where)) { X.abort = true; return false; }
-    return true;
-}
+MT_DEV bool barrier(Ctx& X, int where) { return sync_all(X, where); }
 
 // right-hand side of the LL equation at (t, arg) for the owned cells
 MT_DEV void feval(Ctx& X, RKS& s, double t, int argi, double* out)
@@ -115,6 +168,14 @@ MT_DEV void feval(Ctx& X, RKS& s, double t, int argi, double* out)
 
 MT_DEV void write_arg(Ctx& X, int argi, int q, int q32, double v)
 {
+    if (X.L) {   // every rank's copy, this rank's included
+        const float f = (float)v;
+        for (int p = 0; p < X.sworld; ++p) {
+            X.L->pool[p][argi][q] = v;
+            X.L->pool32[p][argi][q32] = f;
+        }
+        return;
+    }
     X.B.pool[argi][q] = v;
     X.B.pool32[argi][q32] = (float)v;
 }
@@ -408,8 +469,14 @@ MT_DEV void renorm_own(Ctx& X, int pi)
         const double r = sqrt(xadd(xadd(xmul(x, x), xmul(y, y)), xmul(z, z)));
         if (r > 0.0) {
             const double a = x / r, b = y / r, c = z / r;
-            v[i] = a; v[n + i] = b; v[2 * n + i] = c;
-            v32[i] = (float)a; v32[ldk + i] = (float)b; v32[2 * ldk + i] = (float)c;
+            if (X.L) {
+                write_arg(X, pi, i, i, a);
+                write_arg(X, pi, n + i, ldk + i, b);
+                write_arg(X, pi, 2 * n + i, 2 * ldk + i, c);
+            } else {
+                v[i] = a; v[n + i] = b; v[2 * n + i] = c;
+                v32[i] = (float)a; v32[ldk + i] = (float)b; v32[2 * ldk + i] = (float)c;
+            }
         }
     }
     __syncthreads();
@@ -637,19 +704,28 @@ MT_DEV void integrate_body(Ctx& X, unsigned char* smem)
     const IntegBufs& B = X.B;
     const IntegParams& Q = X.Q;
     const int G = X.gsize;
-    X.c0 = (int)(((long long)P.n * X.grank) / G);
-    X.nc = (int)(((long long)P.n * (X.grank + 1)) / G) - X.c0;
-    const int ncmax = (P.n + G - 1) / G;
+    X.L = B.link;
+    int cell0 = 0, ncell = P.n;
+    X.srank = 0; X.sworld = 1; X.slot0 = 0; X.nslots = G;
+    if (X.L) {
+        X.srank = X.L->rank; X.sworld = X.L->world;
+        cell0 = X.L->cell0; ncell = X.L->ncell;
+        X.slot0 = X.L->cta_base; X.nslots = X.L->cta_total;
+    }
+    X.c0 = cell0 + (int)(((long long)ncell * X.grank) / G);
+    X.nc = cell0 + (int)(((long long)ncell * (X.grank + 1)) / G) - X.c0;
+    const int ncmax = (ncell + G - 1) / G;
     const int JC = P.ldk < kDemagJC ? P.ldk : kDemagJC;
     X.sm_m = reinterpret_cast<float*>(smem);
     X.sm_part = X.sm_m + 3 * JC;
     X.sm_S = X.sm_part + 3 * kDemagMaxUnits;
     X.sm_scr = reinterpret_cast<double*>(X.sm_S + ((3 * ncmax + 3) & ~3));
     X.sm_red = X.sm_scr + 32;
-    X.rcount = 0;
     X.abort = false;
 
     RKS s = *B.state;                  // identical copy in every thread
+    X.rcount = (int)(s.rseq & 1);
+    X.xseq = s.xseq;
     X.budget_end = s.full_f_count + s.f_count + Q.evals_per_launch;
     const int n3 = 3 * P.n;
     while (!s.finished && !X.abort) {
@@ -697,6 +773,8 @@ MT_DEV void integrate_body(Ctx& X, unsigned char* smem)
         if (s.full_f_count + s.f_count >= X.budget_end) break;
     }
     // every CTA holds the same state; the group's first CTA publishes it
+    s.rseq = X.rcount;
+    s.xseq = X.xseq;
     if (X.grank == 0 && threadIdx.x == 0 && !X.abort) *B.state = s;
 }
 
@@ -812,6 +890,7 @@ int integrate_grid_size(int n, int num_sms)
 
 size_t integrate_smem_bytes(int n, int ldk, int grid)
 {
+    // n: the cells the grid's CTAs share (a rank's cells for a row-sharded instance)
     const int ncmax = (n + grid - 1) / grid;
     return demag_smem_bytes(ldk, ncmax) + 16 + sizeof(double) * (32 + kRed + 2);
 }

@@ -19,7 +19,46 @@ struct RKS {
     int ci;                        // next entry of the merged output-time list
     int ko;                        // next output slot
     int finished, status, converged_at;
+    long long xseq;                // row shards: cross-rank barriers passed since the exchange region was made
+    long long rseq;                // reductions since then (parity of the partials buffer)
 };
+
+// Row shards of one instance (one rank per GPU).  Rank r owns the receiver cells
+// [cell0, cell0 + ncell) and the tensor rows of those cells only.  Every rank keeps a
+// full copy of the stage arguments: a rank writes its own cells' values into all
+// ranks' exchange regions (peer stores), and the group barrier becomes local barrier,
+// release/acquire flags between ranks at system scope.  Reductions
+// write each CTA's partial into every region and combine all ranks' partials in the
+// same order everywhere, so all ranks take identical steps.
+constexpr int kMaxShards = 8;
+constexpr int kShardMaxCtas = 256;   // per rank, for the partials slots
+
+struct ShardLink {
+    int rank, world;
+    int cell0, ncell;              // this rank's receiver cells
+    int cta_base, cta_total;       // this rank's first global CTA index; CTAs over all ranks
+    double* pool[kMaxShards][4];   // each rank's stage-argument buffers (3n FP64)
+    float* pool32[kMaxShards][4];  // each rank's FP32 shadows [3][ldk]
+    double* partials[kMaxShards];  // each rank's reduction slots [2][cta_total][4]
+    unsigned* flags[kMaxShards];   // each rank's barrier flags: slot p is written by rank p
+    unsigned long long timeout_ns; // bound on one wait for the other ranks
+};
+
+// Byte offsets inside one rank's exchange region (identical on every rank).
+struct ShardLayout {
+    size_t pool, pool32, partials, flags, bytes;
+};
+inline ShardLayout shard_layout(int n, int ldk, int world)
+{
+    auto up = [](size_t v) { return (v + 255) & ~(size_t)255; };
+    ShardLayout L;
+    L.pool = 0;
+    L.pool32 = up(L.pool + sizeof(double) * 4 * 3 * (size_t)n);
+    L.partials = up(L.pool32 + sizeof(float) * 4 * 3 * (size_t)ldk);
+    L.flags = up(L.partials + sizeof(double) * 2 * (size_t)world * kShardMaxCtas * 4);
+    L.bytes = up(L.flags + sizeof(unsigned) * kMaxShards);
+    return L;
+}
 
 struct IntegBufs {
     double* pool[4];       // 3n FP64: y, y_old and two stage-argument buffers (rotating)
@@ -35,6 +74,7 @@ struct IntegBufs {
     double* partials;      // 2 * grid * 4 reduction partials
     GridSync* gs;
     RKS* state;
+    const ShardLink* link;  // row shards (device memory), nullptr for a whole instance
 };
 
 struct IntegParams {

@@ -12,7 +12,8 @@
 
 struct DevProb {
     int n, nx, ny, nz, ldk;
-    const float* K;
+    const float* K;          // tensor rows of cells [krow0, ...): K[((i - krow0)*6 + c)*ldk + j]
+    int krow0;               // first cell whose rows K holds (0 unless the instance is row-sharded)
     double lapc[3];          // 1/(d*d) per axis
     double diag_b[3];        // boundary-row diagonal -1/(d*d), 0 when the axis has one cell
     double diag_i[3];        // interior-row diagonal -2/(d*d), 0 when the axis has one cell
@@ -235,7 +236,7 @@ MT_DEV void demag_cta(const DevProb& P, const float* __restrict__ m32, int c0, i
             const int cell = u / nseg, seg = u - cell * nseg;
             const int js4 = (seg * seglen) >> 2;
             const int je4 = min(seg * seglen + seglen, len) >> 2;
-            const float* row = P.K + ((size_t)(c0 + cell) * 6) * ldk + ch0;
+            const float* row = P.K + ((size_t)(c0 + cell - P.krow0) * 6) * ldk + ch0;
             float sx = 0.f, sy = 0.f, sz = 0.f;
 #pragma unroll 2
             for (int j4 = js4 + lane; j4 < je4; j4 += 32) {

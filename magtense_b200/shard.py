@@ -8,6 +8,13 @@ the max over ranks of a timing, and an optional final gather of per-instance
 results (for example <m>(t)) to rank 0.  They run on whatever process group is
 initialised (NCCL on GPUs, gloo on CPUs); without one they act on the single
 local rank.
+
+One instance too large for one GPU is split by receiver rows instead
+(``Solver(shard=(rank, world))``): each rank holds the tensor rows of its own
+cells, and the integrator exchanges stage arguments and error norms between the
+ranks' kernels through peer memory (CUDA IPC of each rank's exchange region).
+``link_row_shard`` sets that up over the process group; ``gather_rows`` collects
+the ranks' rows of the trajectory.
 """
 from __future__ import annotations
 
@@ -73,3 +80,49 @@ def gather_to_root(local: np.ndarray, total: int):
     if rank != 0:
         return None
     return np.concatenate([parts[r][: b - a].cpu().numpy() for r, (a, b) in enumerate(sizes)], axis=0)
+
+
+def exchange_bytes(blob: bytes) -> list[bytes]:
+    """Every rank's ``blob`` in rank order (all ranks must call it)."""
+    d = _dist()
+    if not d:
+        return [bytes(blob)]
+    out = [None] * d.get_world_size()
+    d.all_gather_object(out, bytes(blob))
+    return out
+
+
+def link_row_shard(solver) -> None:
+    """Map every other rank's exchange region into this rank's row shard: each rank
+    publishes the CUDA IPC handle of its region and opens the others'.  The
+    solver's shard must be (rank, world) of the initialised process group."""
+    ws, rank = world()
+    if solver.shard != (rank, ws):
+        raise ValueError(f"solver shard {solver.shard} is not (rank, world) = {(rank, ws)}")
+    handles = exchange_bytes(solver.shard_ipc_handle())
+    solver.shard_open_peers(handles)
+
+
+def gather_rows(y_local, n: int):
+    """Whole-instance trajectory from the row shards' outputs: ``y_local`` (nt, 3n)
+    holds valid values in this rank's cells [c0, c0 + nc) of each component (the
+    first sample everywhere); every rank gets the (nt, 3n) array with each rank's
+    cells taken from that rank.  All ranks must call it."""
+    d = _dist()
+    y = torch.as_tensor(y_local)
+    if not d:
+        return y
+    ws, rank = d.get_world_size(), d.get_rank()
+    nt = y.shape[0]
+    rows = [((n * r) // ws, (n * (r + 1)) // ws - (n * r) // ws) for r in range(ws)]
+    width = max(nc for _, nc in rows)
+    dev = _device()
+    c0, nc = rows[rank]
+    buf = torch.zeros((nt, 3, width), dtype=torch.float64, device=dev)
+    buf[:, :, :nc] = y.reshape(nt, 3, n)[:, :, c0:c0 + nc].to(dev)
+    parts = [torch.empty_like(buf) for _ in range(ws)]
+    d.all_gather(parts, buf)
+    full = torch.empty((nt, 3, n), dtype=torch.float64, device=dev)
+    for r, (a, k) in enumerate(rows):
+        full[:, :, a:a + k] = parts[r][:, :, :k]
+    return full.reshape(nt, 3 * n).to(y.device)

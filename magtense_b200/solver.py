@@ -47,10 +47,22 @@ def grid_points(res, grid_L) -> np.ndarray:
     return X.reshape(nx * ny * nz, 3)
 
 
-class Solver:
-    """Uniform-grid micromagnetic problem resident on one GPU."""
+def shard_rows(n, rank, world):
+    """Receiver cells [c0, c0 + nc) of row shard `rank` of `world` (as mt_set_row_shard)."""
+    c0 = (n * rank) // world
+    return c0, (n * (rank + 1)) // world - c0
 
-    def __init__(self, res, grid_L, *, A0=1.3e-11, Ms=8e5, K0=0.0, u_ea=None, device=None):
+
+class Solver:
+    """Uniform-grid micromagnetic problem resident on one GPU.
+
+    shard=(rank, world): this object is one row shard of the instance; it holds the
+    tensor rows of its cells only (``shard_rows``), and only ``integrate`` runs it,
+    at the same time as the other ranks' (see ``magtense_b200.shard.open_row_shard``
+    for one process per GPU, ``link_shards_local`` and ``integrate_shards_local`` for
+    all ranks on one device)."""
+
+    def __init__(self, res, grid_L, *, A0=1.3e-11, Ms=8e5, K0=0.0, u_ea=None, device=None, shard=None):
         if not torch.cuda.is_available():
             raise RuntimeError("magtense_b200 needs a CUDA device (no CPU path exists)")
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
@@ -64,6 +76,11 @@ class Solver:
         with torch.cuda.device(self.device):
             check(L.mt_create(C.byref(g), C.byref(h)), "mt_create")
         self._h = h
+        self.shard = None
+        if shard is not None:
+            rank, world = (int(v) for v in shard)
+            check(L.mt_set_row_shard(self._h, rank, world), "mt_set_row_shard")
+            self.shard = (rank, world)
         self.set_material(A0, Ms, K0, u_ea)
         self._have_tensor = False
 
@@ -174,6 +191,42 @@ class Solver:
         check(rc, "mt_integrate")
         return t_out, y_out, flags, st.as_dict()
 
+    # ---------------------------------------------------------------- row shards
+    @property
+    def shard_cells(self):
+        """(c0, nc): the receiver cells this shard owns (the whole grid without shards)."""
+        return (0, self.n) if self.shard is None else shard_rows(self.n, *self.shard)
+
+    def shard_region(self):
+        """(device address, bytes) of this rank's exchange region, allocated on first use."""
+        p = C.c_void_p()
+        nb = C.c_size_t()
+        with torch.cuda.device(self.device):
+            check(_lib.lib().mt_shard_region(self._h, C.byref(p), C.byref(nb)), "mt_shard_region")
+        return p.value, nb.value
+
+    def shard_ipc_handle(self) -> bytes:
+        """The CUDA IPC handle (64 bytes) of this rank's exchange region."""
+        self.shard_region()
+        buf = C.create_string_buffer(64)
+        with torch.cuda.device(self.device):
+            check(_lib.lib().mt_shard_ipc_handle(self._h, buf), "mt_shard_ipc_handle")
+        return buf.raw
+
+    def shard_open_peers(self, handles):
+        """Map the other ranks' regions from their IPC handles (one per rank, rank order)."""
+        blob = b"".join(bytes(hd) for hd in handles)
+        if len(blob) != 64 * self.shard[1]:
+            raise ValueError("need one 64-byte handle per rank")
+        buf = C.create_string_buffer(blob, len(blob))
+        with torch.cuda.device(self.device):
+            check(_lib.lib().mt_shard_open_peers(self._h, buf), "mt_shard_open_peers")
+
+    def shard_set_peers(self, regions):
+        """The ranks' regions as device addresses valid in this process (rank order)."""
+        arr = (C.c_void_p * len(regions))(*[int(r) for r in regions])
+        check(_lib.lib().mt_shard_set_peers(self._h, arr), "mt_shard_set_peers")
+
     def close(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
@@ -212,6 +265,38 @@ def integrate_ragged(solvers, t, m0s, *, tol=1e-4, thres=1e-6, graph=True, strea
                                             1 if graph else 0, _stream(stream))
     check(rc, "mt_integrate_ragged")
     return t_out, ys, flags, [x.as_dict() for x in st]
+
+
+def link_shards_local(shards):
+    """Give every row shard of one instance on ONE device the other ranks' regions."""
+    regions = [sv.shard_region()[0] for sv in shards]
+    for sv in shards:
+        sv.shard_set_peers(regions)
+
+
+def integrate_shards_local(shards, t, m0, *, tol=1e-4, thres=1e-6, t_conv=None, conv_tol=1e-4, stream=None):
+    """All row shards of one instance (``Solver(shard=(r, W))`` for r < W, linked with
+    ``link_shards_local``) integrated on one device as CTA groups of one launch: the
+    multi-GPU code path with its peer stores landing in local memory.  Returns what
+    ``Solver.integrate`` returns, for the whole instance."""
+    W = len(shards)
+    sv0 = shards[0]
+    t = _np_d(t).reshape(-1)
+    nt = t.shape[0]
+    m0 = sv0._vec(m0)
+    tc = np.zeros(1) if t_conv is None else _np_d(t_conv).reshape(-1)
+    y_out = torch.zeros((nt, 3 * sv0.n), dtype=torch.float64, device=sv0.device)
+    t_out = np.zeros(nt)
+    flags = np.zeros(nt, dtype=np.int32)
+    st = _lib.Stats()
+    hs = (VPA * W)(*[sv._h.value for sv in shards])
+    with torch.cuda.device(sv0.device):
+        rc = _lib.lib().mt_integrate_shards_local(hs, W, t.ctypes.data_as(_lib.D), nt, _dptr(m0), float(tol),
+                                                  float(thres), tc.ctypes.data_as(_lib.D), tc.shape[0],
+                                                  float(conv_tol), t_out.ctypes.data_as(_lib.D), _dptr(y_out),
+                                                  flags.ctypes.data_as(_lib.I), C.byref(st), _stream(stream))
+    check(rc, "mt_integrate_shards_local")
+    return t_out, y_out, flags, st.as_dict()
 
 
 VPA = C.c_void_p

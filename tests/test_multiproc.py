@@ -1,6 +1,8 @@
 """Instance sharding over ranks (magtense_b200/shard.py) with world_size-2
 gloo process groups on the CPU: the slices partition the instance list, the
-max over ranks and the gather to rank 0 are exact and in rank order, and a
+max over ranks and the gather to rank 0 are exact and in rank order, the row
+shards of one instance gather their rows and swap their IPC handles in rank
+order, and a
 rank that leaves before a collective makes the other rank's collective fail
 within the process-group timeout instead of hanging."""
 import datetime
@@ -38,6 +40,28 @@ def _worker_collectives(rank, world, port, total, out):
     if rank == 0:
         out.put(("gather", full))
     out.put(("max", rank, mx))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def _worker_rows(rank, world, port, n, out):
+    """Row shards' host side: every rank fills only its own cells of a (nt, 3n)
+    trajectory (NaN elsewhere, the first sample everywhere) and exchanges a
+    64-byte blob standing in for its IPC handle."""
+    dist = _init(rank, world, port)
+    import torch
+    from magtense_b200.shard import exchange_bytes, gather_rows
+    from magtense_b200.solver import shard_rows
+    nt = 4
+    ref = torch.arange(nt * 3 * n, dtype=torch.float64).reshape(nt, 3 * n)
+    y = torch.full_like(ref, float("nan"))
+    y[0] = ref[0]
+    c0, nc = shard_rows(n, rank, world)
+    for a in range(3):
+        y[1:, a * n + c0:a * n + c0 + nc] = ref[1:, a * n + c0:a * n + c0 + nc]
+    full = gather_rows(y, n)
+    blobs = exchange_bytes(bytes([rank]) * 64)
+    out.put((rank, bool(torch.equal(full, ref)), blobs))
     dist.barrier()
     dist.destroy_process_group()
 
@@ -99,3 +123,36 @@ def test_gloo_rank_that_leaves_is_detected():
     for p in procs:
         p.join(timeout=60)
     assert kind == "error", info
+
+
+@pytest.mark.parametrize("world,n", [(2, 640), (3, 814)])
+def test_gloo_row_shards_gather_rows_and_handles(world, n):
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker_rows, args=(r, world, port, n, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    msgs = sorted(out.get(timeout=120) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, ok, blobs in msgs:
+        assert ok, rank
+        assert blobs == [bytes([r]) * 64 for r in range(world)]
+
+
+def test_row_partition_matches_the_library():
+    """shard_rows restates mt_set_row_shard's split: contiguous, covering, sizes
+    differing by at most one."""
+    from magtense_b200.solver import shard_rows
+    for n in (2, 7, 640, 814, 32768):
+        for w in range(2, 9):
+            if n < w:
+                continue
+            cells = []
+            for r in range(w):
+                c0, nc = shard_rows(n, r, w)
+                assert nc in (n // w, n // w + 1)
+                cells.extend(range(c0, c0 + nc))
+            assert cells == list(range(n))
