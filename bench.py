@@ -19,10 +19,15 @@ groups, replayed from a CUDA graph), "adjoint" (the differentiation configuratio
 a 2 ns fixed-step RK4 trajectory of the film with 200 piecewise-constant field
 segments and per-cell Ms) and
 "large-plain" (64x64x8 cubes of 5 nm, n = 32768, 25.8 GB FP32 tensor, the
-HBM-bound demag matvec).
+HBM-bound demag matvec).  large-plain --shards W splits that one instance by
+receiver rows: on one GPU into W shards run as CTA groups of one launch (the
+multi-GPU code path, its peer stores landing in local memory); under torchrun
+with W = --gpus over the ranks, each GPU holding 25.8/W GB of tensor rows and
+exchanging stage arguments and error norms with its peers through CUDA IPC
+regions ("scaling": "strong").
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload film-batch|film-plain|large-plain|adjoint|ragged]
+                  [--workload film-batch|film-plain|large-plain|adjoint|ragged] [--shards W]
 
 Multi-GPU: one process per GPU (torchrun); instances are sharded across ranks
 with no data-path collective ("scaling": "weak"); the step time is the max over
@@ -69,6 +74,8 @@ def parse():
     ap.add_argument("--cpu-window", type=float, default=0.3, help="simulated ns of the bounded CPU sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--shards", type=int, default=1,
+                    help="large-plain: row shards of the one instance (over the ranks when --gpus > 1)")
     ap.add_argument("--res", type=int, nargs=3, default=None,
                     help="large-plain: override the grid (cubes of 5 nm), e.g. a small case for profiling")
     return ap.parse_args()
@@ -325,7 +332,7 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
         plain_evals += pst["f_evals"]
         del yp
     plain_rate = len(pick) * window / plain_s
-    step_ms = max(times)
+    step_ms = sum(times) / len(times)   # the K timed steps as one bracket, L2 flushes excluded
     step_ms, e2e_red = max_over_ranks(torch, dist, [step_ms, e2e_ms or 0.0])
     if rank != 0:
         return None
@@ -476,7 +483,7 @@ def bench_adjoint(torch, args, ws, rank, local, dist, hbm, src):
         gh, gm = out["g"][0].cpu(), out["g"][1].cpu()
         torch.cuda.synchronize()
         e2e.append((time.perf_counter() - t0) * 1e3)
-    step_ms, e2e_ms = max_over_ranks(torch, dist, [max(times), statistics.median(e2e)])
+    step_ms, e2e_ms = max_over_ranks(torch, dist, [sum(times) / len(times), statistics.median(e2e)])
     if rank != 0:
         return None
     # right-hand sides per step: forward 4 RK4 stages; backward 4 recomputed stages plus 4
@@ -575,7 +582,7 @@ def bench_ragged(torch, args, ws, rank, local, dist, hbm, src):
         s.integrate(t, m, tol=1e-6)
     torch.cuda.synchronize()
     seq_s = time.perf_counter() - t0
-    step_ms, e2e_ms = max_over_ranks(torch, dist, [max(times), statistics.median(e2e)])
+    step_ms, e2e_ms = max_over_ranks(torch, dist, [sum(times) / len(times), statistics.median(e2e)])
     if rank != 0:
         return None
     K = len(solvers)
@@ -612,8 +619,15 @@ def bench_ragged(torch, args, ws, rank, local, dist, hbm, src):
 
 
 def bench_plain(torch, args, ws, rank, local, dist, hbm, src):
-    from magtense_b200 import Solver
+    from magtense_b200 import Solver, integrate_shards_local, link_shards_local
+    from magtense_b200.shard import gather_rows, link_row_shard
     large = args.workload == "large-plain"
+    W = args.shards
+    mode = None if W <= 1 else ("ranks" if ws > 1 else "local")
+    if mode and not large:
+        raise SystemExit("--shards applies to large-plain")
+    if mode == "ranks" and W != ws:
+        raise SystemExit("--shards must equal --gpus for row shards over ranks")
     res, L = (LARGE_RES, LARGE_L) if large else (FILM_RES, FILM_L)
     if large and args.res:
         res = tuple(args.res)
@@ -627,20 +641,35 @@ def bench_plain(torch, args, ws, rank, local, dist, hbm, src):
         rng = np.random.default_rng(1)
         axis = rng.standard_normal(3)
         axis /= np.linalg.norm(axis)
-        s = Solver(res, L, K0=5e3, u_ea=np.tile(axis, (n, 1)))
-        s.assemble()
         m = rng.standard_normal((3, n))
         m_s = torch.as_tensor((m / np.linalg.norm(m, axis=0)).reshape(-1), device="cuda")
         h = np.array([10e-3 / MU0, 0.0, 0.0])
-        s.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.1, hext=np.array([[0.0, *h], [win, *h]]))
+
+        def make(shard=None):
+            sv = Solver(res, L, K0=5e3, u_ea=np.tile(axis, (n, 1)), shard=shard)
+            sv.assemble()
+            sv.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.1, hext=np.array([[0.0, *h], [win, *h]]))
+            return sv
+
+        if mode == "local":
+            shards = [make((r, W)) for r in range(W)]
+            link_shards_local(shards)
+        else:
+            s = make((rank, ws) if mode == "ranks" else None)
+            if mode == "ranks":
+                link_row_shard(s)
     else:
         s, m_s = relaxed_state(torch, res, L)
         h = instance_fields(1000, ws)[rank]
         s.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.02, hext=np.array([[0.0, *h], [win, *h]]))
 
+    def run(m0):
+        if mode == "local":
+            return integrate_shards_local(shards, t, m0, tol=1e-6)
+        return s.integrate(t, m0, tol=1e-6)
+
     def step():
-        _, _, _, st = s.integrate(t, m_s, tol=1e-6)
-        return [st]
+        return [run(m_s)[3]]
 
     times, stats, clocks, flush = timed_steps(torch, step, args.steps, args.warmup, dist, local)
     m_host = m_s.cpu().numpy()
@@ -650,38 +679,51 @@ def bench_plain(torch, args, ws, rank, local, dist, hbm, src):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         m0 = torch.from_numpy(m_host).pin_memory().to("cuda", non_blocking=True)
-        _, y, _, _ = s.integrate(t, m0, tol=1e-6)
+        _, y, _, _ = run(m0)
+        if mode == "ranks":
+            y = gather_rows(y, n)
         y.cpu()
         torch.cuda.synchronize()
         e2e.append((time.perf_counter() - t0) * 1e3)
-    step_ms, e2e_ms = max_over_ranks(torch, dist, [max(times), statistics.median(e2e)])
+    step_ms, e2e_ms = max_over_ranks(torch, dist, [sum(times) / len(times), statistics.median(e2e)])
     if rank != 0:
         return None
     flat = [x for st in stats for x in st]
     evals = sum(x["f_evals"] for x in flat)
     kms = sum(x["kernel_ms"] for x in flat)
     launches = sum(x["launches"] for x in flat)
-    achieved = 24.0 * n * n * evals / (kms / 1e3) / 1e9
-    sim_ns = ws * window
+    # tensor bytes one GPU streams per evaluation: its rows only when the ranks share the instance
+    rows = -(-n // ws) if mode == "ranks" else n
+    achieved = 24.0 * n * rows * evals / (kms / 1e3) / 1e9
+    sim_ns = window if mode == "ranks" else ws * window
+    if mode == "local":
+        par = f"one instance as {W} row shards on one GPU (CTA groups of one launch, peer stores into local memory)"
+    elif mode == "ranks":
+        par = f"one instance as {ws} row shards, one per GPU (CUDA IPC exchange regions)"
+    else:
+        par = f"one instance per rank, {ws} rank(s)"
+    kern = "integrate_ragged_kernel (shard groups)" if mode == "local" else "integrate_kernel"
     return {
         "metric": "simulated ns/s", "value": sim_ns / (step_ms / 1e3), "unit": "simulated ns/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "scaling": "strong" if mode == "ranks" else "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": (f"large-plain: {res[0]}x{res[1]}x{res[2]} cubes of 5 nm (n={n}, "
                                 f"{24 * n * n / 1e9:.2f} GB FP32 tensor), K=5e3 J/m^3 "
                                 "along a seeded axis, 10 mT field, alpha_G=0.1" if large else
                                 "film-plain: 80x20x1 std-problem-4 film (n=1600), single instance") +
                                ", plain FP32 demag, persistent single-instance integrator, tol 1e-6",
-                   "window_ns": window, "outputs": nt, "parallelism": f"one instance per rank, {ws} rank(s)",
+                   "window_ns": window, "outputs": nt, "parallelism": par,
                    "l2": "flushed (256 MB write) before every timed step"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": None,
-                     "note": f"integrate_kernel: 24*n^2 tensor bytes per RHS evaluation x {evals} evaluations over "
-                             f"{kms:.2f} ms of device time; peak {src} HBM copy"},
+                     "note": f"{kern}: 24*n*{rows} tensor bytes per RHS evaluation per GPU x {evals} evaluations "
+                             f"over {kms:.2f} ms of device time; peak {src} HBM copy"},
         "e2e": {"value": sim_ns / (e2e_ms / 1e3), "unit": "simulated ns/s", "h2d_bytes_per_step": 3 * n * 8,
                 "d2h_bytes_per_step": nt * 3 * n * 8},
         "gpu_launches": int(launches),
         "rhs_evals_per_s": evals / (sum(times) / 1e3) * ws,
+        "step_ms_each": [round(x, 3) for x in times],
+        "kernel_ms_each": [round(sum(x["kernel_ms"] for x in st), 3) for st in stats],
         "clocks": clocks,
     }
 
