@@ -1248,9 +1248,11 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
         }                                                  \
     } while (0)
     long long ticks_run = 0;
+    unsigned long long hist_ns[5] = {0, 0, 0, 0, 0}, hist_n[5] = {0, 0, 0, 0, 0};   // ticks by active tiles
     for (long long tick = 0; tick < Q.ticks_per_launch && ok; ++tick) {
         unsigned* ctr = F.counters + 2 * (tick % 3);
         ticks_run++;
+        const uint64_t t_tick = prof ? globaltimer_ns() : 0;
         // P2: resolve reductions, advance
         int my_active = 0, my_rhs = 0;
         int rhs_tile[2] = {0, 0};   // requests per 64-instance tile, tiles jb0 and jb0 + 1
@@ -1374,11 +1376,17 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
         PROF_MARK(4);
         if (!grid_sync(F.gs, 3)) { ok = false; break; }
         PROF_MARK(5);
+        if (prof && i8) {
+            const int k = X.nact < 4 ? X.nact : 4;
+            hist_ns[k] += globaltimer_ns() - t_tick;
+            hist_n[k]++;
+        }
     }
     if (prof) {
         if (t == 0) {
             for (int k = 0; k < 7; ++k) atomicAdd(&F.prof[k], acc[k]);
             atomicAdd(&F.prof[7], (unsigned long long)ticks_run);
+            for (int k = 0; k < 5; ++k) { atomicAdd(&F.prof[32 + k], hist_ns[k]); atomicAdd(&F.prof[37 + k], hist_n[k]); }
         }
         // busiest CTA per work phase (P2, GEMM, P1): value and CTA index
         const int work[3] = {0, 2, 4};

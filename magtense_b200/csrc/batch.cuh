@@ -61,7 +61,7 @@ struct BatchBufs {
     GridSync* gs;
     unsigned* counters;  // [3][2]: active instances, right-hand-side requests
     unsigned* ibreq;     // [3][2 IB]: right-hand-side requests per 64-instance tile
-    unsigned long long* prof;  // [8] phase times (ns) seen by CTA 0, or nullptr
+    unsigned long long* prof;  // [48] phase times (ns) and counters seen by CTA 0, or nullptr
     // per-instance inputs
     const double* hext;    // [Bp][nt_hext][4]
     const double* alpha0;  // [Bp]

@@ -1225,8 +1225,8 @@ int batch_alloc(mt_batch* bt, BatchRun& R, int nt, cudaStream_t s)
     CUDA_TRY(R.A.get(&F.ibreq, 6 * (size_t)bt->IB));
     CUDA_TRY(cudaMemsetAsync(F.ibreq, 0, sizeof(unsigned) * 6 * bt->IB, s));
     if (getenv("MT_BATCH_PROFILE")) {
-        CUDA_TRY(R.A.get(&F.prof, 32));
-        CUDA_TRY(cudaMemsetAsync(F.prof, 0, sizeof(unsigned long long) * 32, s));
+        CUDA_TRY(R.A.get(&F.prof, 48));
+        CUDA_TRY(cudaMemsetAsync(F.prof, 0, sizeof(unsigned long long) * 48, s));
     }
     F.hext = bt->hext;
     F.alpha0 = bt->alpha0;
@@ -1454,8 +1454,15 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
     stats[0].launches = launches;
     stats[0].kernel_ms = kernel_ms;
     if (F.prof) {
-        unsigned long long pr[32];
+        unsigned long long pr[48];
         CUDA_TRY(cudaMemcpy(pr, F.prof, sizeof(pr), cudaMemcpyDeviceToHost));
+        if (bt->prec == MT_PREC_INT8) {
+            fprintf(stderr, "[batch profile] ticks by active 64-instance tiles (count, mean us):");
+            for (int k = 0; k < 5; ++k)
+                fprintf(stderr, " %d%s: %llu, %.1f;", k, k == 4 ? "+" : "", pr[37 + k],
+                        pr[37 + k] ? pr[32 + k] / 1e3 / pr[37 + k] : 0.0);
+            fprintf(stderr, "\n");
+        }
         const double tk = pr[7] ? (double)pr[7] : 1.0;
         fprintf(stderr, "[batch profile] ticks %llu  per tick (us) at CTA 0: P2 %.2f B1 %.2f GEMM %.2f Bh %.2f "
                 "P1 epilogue %.2f advance %.2f B2 %.2f  busiest CTA: P2 %.2f (cta %llu) GEMM %.2f (cta %llu) "
