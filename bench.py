@@ -55,6 +55,10 @@ MU0 = 4 * np.pi * 1e-7
 GAMMA = 2.211e5
 FILM_RES = (80, 20, 1)
 FILM_L = (500e-9, 125e-9, 3e-9)
+# DRAM bytes (read + write) per algorithmic tensor byte of the streaming integrator,
+# from an ncu capture of large-plain at 32x32x4 (43.906 GB read + 0.065 GB written
+# for 43.89 GB of tensor rows)
+TRAFFIC_PER_TENSOR_BYTE = (43.906 + 0.065) / 43.89
 LARGE_RES = (64, 64, 8)
 LARGE_L = (320e-9, 320e-9, 40e-9)
 
@@ -715,9 +719,12 @@ def bench_plain(torch, args, ws, rank, local, dist, hbm, src):
                    "window_ns": window, "outputs": nt, "parallelism": par,
                    "l2": "flushed (256 MB write) before every timed step"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None,
+                     # DRAM bytes per launch: an ncu capture of a 32x32x4 case read 1.0004 x the tensor bytes of
+                     # its evaluations (writes 0.15 %); scaled here by this run's evaluations per launch
+                     "traffic": (TRAFFIC_PER_TENSOR_BYTE * 24.0 * n * rows * evals / max(1, launches)) if large else None,
                      "note": f"{kern}: 24*n*{rows} tensor bytes per RHS evaluation per GPU x {evals} evaluations "
-                             f"over {kms:.2f} ms of device time; peak {src} HBM copy"},
+                             f"over {kms:.2f} ms of device time; peak {src} HBM copy"
+                             + ("; traffic in bytes per launch, scaled from the 32x32x4 ncu capture" if large else "")},
         "e2e": {"value": sim_ns / (e2e_ms / 1e3), "unit": "simulated ns/s", "h2d_bytes_per_step": 3 * n * 8,
                 "d2h_bytes_per_step": nt * 3 * n * 8},
         "gpu_launches": int(launches),
