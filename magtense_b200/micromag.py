@@ -231,6 +231,60 @@ class MicromagProblem:
             H = [np.zeros((nt, n, 1, 3)) for _ in range(4)]
         return t_out, M, pts, H[0], H[1], H[2], H[3]
 
+    def run_batch(self, t_end, nt, h_ext, *, m0=None, alpha=None, precision="int8", keep_trajectory=True):
+        """B instances of this problem in one call: one grid, material and demag
+        tensor, and per instance its own applied field, damping, initial state and
+        RKSUITE 'M' step control; every right-hand-side evaluation of all instances
+        shares one demag GEMM (``BatchSolver``).  The reference solves one problem
+        per call; its dataset workflow loops ``run_simulation`` over seeded fields
+        (python/scripts/database.py:19-87).
+
+        h_ext: (B, nt_h_ext, 3) fields in A/m at the times linspace(0, t_end,
+            nt_h_ext), or (B, 3) constant fields (the explicit solver takes (B, 3):
+            one quasi-static field per instance).
+        m0: None (this problem's m0 for every instance) or (B, n, 3).
+        alpha: None (this problem's alpha) or a scalar or (B,) array, as ``alpha``
+            of the constructor.
+        precision: "int8" (exact fixed-point product, the default), "fp32" (the
+            reference's FP32 product), "bf16x3", "bf16x2" or "fp16s".
+        Returns (t_out (B, nt), M (B, nt, n, 1, 3) or None without the trajectory,
+        pts (n, 3)); per-instance statistics go to ``self.last_stats``."""
+        from .solver import BatchSolver
+        self._check_supported()
+        if self.N_load > 2:
+            raise NotImplementedError("run_batch assembles its tensor; loading one from disk is run_simulation only")
+        if alpha is None and self.alpha_mm == 0.0:
+            raise NotImplementedError("the batched path takes a constant alpha per instance, not an alpha(t) table")
+        n = self.ntot
+        h = np.asarray(h_ext, dtype=np.float64)
+        if h.ndim == 2:
+            h = np.repeat(h[:, None, :], 2, axis=1)
+        if h.ndim != 3 or h.shape[2] != 3:
+            raise ValueError("h_ext must be (B, 3) or (B, nt_h_ext, 3)")
+        B, ntab = h.shape[0], h.shape[1]
+        tab = np.zeros((B, ntab, 4))
+        tab[:, :, 0] = np.linspace(0, t_end, ntab)[None, :]
+        tab[:, :, 1:] = h
+        al = np.broadcast_to(np.asarray(self.alpha_mm if alpha is None else alpha, dtype=np.float64), (B,))
+        if m0 is None:
+            base = np.concatenate((self.m0[:, 0], self.m0[:, 1], self.m0[:, 2]))
+            m0s = np.broadcast_to(base, (B, 3 * n)).copy()
+        else:
+            m0s = np.asarray(m0, dtype=np.float64).reshape(B, n, 3).transpose(0, 2, 1).reshape(B, 3 * n).copy()
+        bs = BatchSolver(self.grid_n, self.grid_L, B, precision=precision, A0=self.A0, Ms=self.Ms, K0=self.K0,
+                         u_ea=self.u_ea)
+        try:
+            bs.assemble()
+            bs.set_dynamics(hext=tab, alpha=al, solver=self._solver, gamma=self.gamma, renormalize=self.renormalize)
+            t = np.linspace(0, t_end, nt)
+            t_out, y, _, st = bs.integrate(t, m0s, tol=self.tol, thres=self.thres, t_conv=self.t_conv,
+                                           conv_tol=float(self.conv_tol[0]), keep_trajectory=keep_trajectory)
+            M = None if y is None else y.view(B, nt, 3, n).permute(0, 1, 3, 2).cpu().numpy()[:, :, :, None, :]
+        finally:
+            bs.close()
+        self.last_stats = st
+        return t_out, M, grid_points(self.grid_n, self.grid_L)
+
 
 def load_demag_tensor(filename: str, n: int):
     """Read the reference's raw demag-tensor file: six records of n*n FP32, column-major
