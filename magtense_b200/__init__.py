@@ -19,6 +19,9 @@ def __getattr__(name):
                 "integrate_shards_local"):
         from . import solver
         return getattr(solver, name)
+    if name == "dataset":
+        import importlib
+        return importlib.import_module(".dataset", __name__)
     if name in ("TrajectoryProblem", "mean_m_trajectory", "LLTrajectory"):
         from . import adjoint
         return getattr(adjoint, name)

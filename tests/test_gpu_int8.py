@@ -161,3 +161,32 @@ def test_micromag_run_batch_matches_oracle(torch_cuda, oracle):
         assert np.array_equal(t_out[b], to), b
         assert prob.last_stats[b]["f_evals"] == so["f_evals"], (b, prob.last_stats[b], so)
         assert np.array_equal(M[b, :, :, 0, :].transpose(0, 2, 1).reshape(nt, -1), yo), b
+
+
+def test_std_prob_4_dataset_sequences_match_oracle(torch_cuda, oracle, tmp_path):
+    """The dataset driver: a short relaxation from the reference's s-state recipe,
+    then three seeded sequences in one batched run; each sequence equals the
+    oracle's single-instance run of the same definition, bit for bit, in the
+    database layout."""
+    from magtense_b200 import dataset as D
+    res, L = (16, 8, 1), (100e-9, 50e-9, 3e-9)
+    n = 128
+    st = D.s_state(res, L, t_end=2e-9, nt=5, nt_h_ext=50)
+    assert st.shape == (n, 3) and np.all(np.isfinite(st))
+    fields = D.std_prob_4_fields(3, seed=5)
+    t_steps, dt = 8, 4e-12
+    seq, stats = D.std_prob_4_sequences(st, res, fields, L, t_steps, dt, precision="int8")
+    assert seq.shape == (3, t_steps, 3, 16, 8) and seq.dtype == np.float32
+    K32 = device_tensor(list(res), list(L))
+    t = np.linspace(0, dt * t_steps, t_steps)
+    m0 = np.concatenate((st[:, 0], st[:, 1], st[:, 2]))
+    for b in range(3):
+        h = fields[b] / 1000 / MU0
+        P = oracle.Problem(list(res), list(L), mode=2, gamma=D.GAMMA, alpha=D.ALPHA,
+                           hext=np.array([[0.0, *h], [dt * t_steps, *h]]), K32=K32)
+        _, yo, _, so = P.solve(t, m0, tol=1e-4)
+        want = D.sequence_layout(yo.reshape(t_steps, 3, n).transpose(0, 2, 1), res).astype(np.float32)
+        assert stats[b]["f_evals"] == so["f_evals"], (b, stats[b], so)
+        assert np.array_equal(seq[b], want), b
+    out = D.write_database(tmp_path / "db", seq, fields, (0, 3))
+    assert out.exists()
