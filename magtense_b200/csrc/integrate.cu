@@ -772,6 +772,10 @@ MT_DEV void integrate_body(Ctx& X, unsigned char* smem)
         if (s.status) { s.finished = 1; break; }
         if (s.full_f_count + s.f_count >= X.budget_end) break;
     }
+    // row shards: all ranks finish at the same point (their states are identical), so
+    // they meet once more; after it no rank stores into a peer's region for this run,
+    // whichever exit (output, convergence or an RKSUITE error flag) ended it
+    if (X.L && s.finished && !X.abort) sync_all(X, 140);
     // every CTA holds the same state; the group's first CTA publishes it
     s.rseq = X.rcount;
     s.xseq = X.xseq;
