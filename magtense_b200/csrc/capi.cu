@@ -11,6 +11,8 @@
 #include <stdlib.h>
 #include <string.h>
 #include <algorithm>
+#include <chrono>
+#include <thread>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -85,6 +87,8 @@ struct mt_handle {
     void* shard_peer[kMaxShards] = {};              // every rank's region, this rank's included
     bool shard_ipc[kMaxShards] = {};                // mapped here by cudaIpcOpenMemHandle
     bool shard_peers_set = false, shard_broken = false;
+    double shard_timeout_s = 10.0;                  // bound on one cross-rank wait (build_link)
+    std::chrono::steady_clock::time_point shard_broken_at;   // when a run of this rank gave up
     ShardLink* shard_link = nullptr;                // device copy of the link
     long long shard_xseq = 0, shard_rseq = 0;       // barrier and reduction counts after the last run
 };
@@ -132,6 +136,14 @@ int check_ready(const mt_handle* h, bool need_material, bool need_dynamics)
 }
 
 bool sharded(const mt_handle* h) { return h && h->shard_world > 1; }
+
+// a run of this row shard gave up: no further runs, and mt_destroy keeps the region a while
+void mark_broken(mt_handle* h)
+{
+    if (!sharded(h) || h->shard_broken) return;
+    h->shard_broken = true;
+    h->shard_broken_at = std::chrono::steady_clock::now();
+}
 
 int refuse_sharded(const mt_handle* h, const char* what)
 {
@@ -193,6 +205,19 @@ int mt_create(const mt_grid* g, mt_handle** out)
 int mt_destroy(mt_handle* h)
 {
     if (!h) return MT_OK;
+    if (h->shard_broken && h->shard_region) {
+        // A rank of another process may still store into this region after a run gave up:
+        // until its next cross-rank barrier sees the abort word, or, if it waits on this
+        // rank, until its own wait runs out and it raises the abort words.  Both end within
+        // two timeouts of the failure, so the region is freed no earlier than that.
+        bool remote = false;
+        for (int p = 0; p < kMaxShards; ++p) remote = remote || h->shard_ipc[p];
+        if (remote) {
+            const auto until = h->shard_broken_at + std::chrono::milliseconds(
+                                   (long long)(1000.0 * (2.0 * h->shard_timeout_s + 1.0)));
+            std::this_thread::sleep_until(until);
+        }
+    }
     free_ptr(h->Jfact); free_ptr(h->Kfact); free_ptr(h->Mfact); free_ptr(h->A6);
     free_ptr(h->hext); free_ptr(h->alpha_tab); free_ptr(h->K); free_ptr(h->m32);
     free_ptr(h->vjp_buf); free_ptr(h->vjp_z); free_ptr(h->vjp_v32);
@@ -602,6 +627,7 @@ int build_link(mt_handle* h, int grid)
         if (v > 0.0 && v <= 600.0) tmo_s = v;
     }
     L.timeout_ns = (unsigned long long)(tmo_s * 1e9);
+    h->shard_timeout_s = tmo_s;
     for (int p = 0; p < h->shard_world; ++p) {
         unsigned char* base = static_cast<unsigned char*>(h->shard_peer[p]);
         for (int k = 0; k < 4; ++k) {
@@ -728,9 +754,25 @@ int run_groups(const std::vector<IntegRun*>& runs, bool graph, cudaStream_t cs, 
 
 extern "C" {
 
+static int integrate_single(mt_handle* h, const double* t, int nt, const double* m0_dev, double tol, double thres,
+                            const double* t_conv, int nt_conv, double conv_tol, double* t_out, double* y_out_dev,
+                            int* flags, mt_stats* stats, void* stream);
+
 int mt_integrate(mt_handle* h, const double* t, int nt, const double* m0_dev, double tol, double thres,
                  const double* t_conv, int nt_conv, double conv_tol, double* t_out, double* y_out_dev, int* flags,
                  mt_stats* stats, void* stream)
+{
+    const int rc = integrate_single(h, t, nt, m0_dev, tol, thres, t_conv, nt_conv, conv_tol, t_out, y_out_dev, flags,
+                                    stats, stream);
+    // a row shard whose run failed past the argument checks (CUDA error, timeout, no progress)
+    // may have left peers mid-run: it takes no further runs
+    if (rc != MT_OK && rc != MT_ERR_ARG && rc != MT_ERR_STATE) mark_broken(h);
+    return rc;
+}
+
+static int integrate_single(mt_handle* h, const double* t, int nt, const double* m0_dev, double tol, double thres,
+                            const double* t_conv, int nt_conv, double conv_tol, double* t_out, double* y_out_dev,
+                            int* flags, mt_stats* stats, void* stream)
 {
     int rc = check_ready(h, true, true);
     if (rc) return rc;
@@ -775,14 +817,16 @@ int mt_integrate(mt_handle* h, const double* t, int nt, const double* m0_dev, do
         stats->launches = launches;
         stats->kernel_ms = kernel_ms;
         if (gs_h.err != 0 || gs_h.abort) {
-            h->shard_broken = sharded(h);
+            mark_broken(h);
             return fail(MT_ERR_TIMEOUT, "integrator %s barrier gave up (code %d at %d)",
-                        gs_h.err == KERR_PEER_TIMEOUT ? "cross-rank" : "grid", gs_h.err, gs_h.err_where);
+                        gs_h.err == KERR_PEER_TIMEOUT ? "cross-rank"
+                        : gs_h.err == KERR_PEER_ABORT ? "cross-rank (another rank gave up)" : "grid",
+                        gs_h.err, gs_h.err_where);
         }
         if (hs.finished) break;
         const long long evals = hs.full_f_count + hs.f_count;
         if (evals == last_evals && hs.ci == last_ci) {
-            h->shard_broken = sharded(h);
+            mark_broken(h);
             return fail(MT_ERR_SOLVER, "integrator made no progress");
         }
         last_evals = evals;
@@ -970,7 +1014,7 @@ int mt_integrate_shards_local(mt_handle* const* hs, int world, const double* t, 
     double kernel_ms = 0.0;
     rc = run_groups(rp, false, cs, back, launches, kernel_ms);
     if (rc) {
-        for (int r = 0; r < world; ++r) hs[r]->shard_broken = true;
+        for (int r = 0; r < world; ++r) mark_broken(hs[r]);
         return rc;
     }
     for (int r = 0; r < world; ++r) {
@@ -978,7 +1022,7 @@ int mt_integrate_shards_local(mt_handle* const* hs, int world, const double* t, 
         const RKS& b = back[0].st;
         if (a.full_f_count + a.f_count != b.full_f_count + b.f_count || a.step_count != b.step_count ||
             a.ko != b.ko || a.t != b.t || a.xseq != b.xseq) {
-            for (int q = 0; q < world; ++q) hs[q]->shard_broken = true;
+            for (int q = 0; q < world; ++q) mark_broken(hs[q]);
             return fail(MT_ERR_SOLVER, "row shard %d took different steps from rank 0", r);
         }
         hs[r]->shard_xseq = a.xseq;

@@ -7,7 +7,8 @@
 #define MT_DEV __device__ __forceinline__
 
 // Error codes recorded by kernels in GridSync::err (host maps them to MT_ERR_*).
-enum { KERR_NONE = 0, KERR_BARRIER_TIMEOUT = 1, KERR_BAD_CONFIG = 2, KERR_RANGE = 3, KERR_PEER_TIMEOUT = 4 };
+enum { KERR_NONE = 0, KERR_BARRIER_TIMEOUT = 1, KERR_BAD_CONFIG = 2, KERR_RANGE = 3, KERR_PEER_TIMEOUT = 4,
+       KERR_PEER_ABORT = 5 };
 
 // Grid-wide barrier state for the persistent cooperative kernels.  count is
 // reset to 0 by the host before every launch.

@@ -2,6 +2,8 @@
 // mt_rhs and icl_MVMult_GetH.  One CTA owns a few receiver cells and streams
 // their tensor records (demag_cta in llg.cuh), then applies the per-cell
 // epilogue.
+#include <mutex>
+
 #include "common.cuh"
 #include "llg.cuh"
 #include "fields.cuh"
@@ -172,19 +174,25 @@ cudaError_t launch_field(int mode, const DevProb& P, const double* m, const floa
     const size_t smem = demag_smem_bytes(P.ldk, cpc);
     cudaError_t e = cudaSuccess;
     // the shared-memory limit is raised only when it grows (once per mode and size in practice),
-    // so repeated launches, for example inside a stream capture, make no attribute calls
-    constexpr int kMaxDev = 64;
+    // so repeated launches, for example inside a stream capture, make no attribute calls.  The
+    // per-device record is shared by every host thread, hence the lock around check and update.
+    constexpr int kMaxDev = 256;
     static size_t smem_set[kMaxDev][6] = {};
+    static std::mutex smem_mu;
     int dev = 0;
     e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     size_t* set = (dev >= 0 && dev < kMaxDev) ? smem_set[dev] : nullptr;
 #define MT_LAUNCH(M)                                                                                           \
     do {                                                                                                       \
-        if (!set || smem > set[M]) {                                                                           \
-            e = cudaFuncSetAttribute(field_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-            if (e != cudaSuccess) return e;                                                                    \
-            if (set) set[M] = smem;                                                                            \
+        {                                                                                                      \
+            std::lock_guard<std::mutex> lock(smem_mu);                                                         \
+            if (!set || smem > set[M]) {                                                                       \
+                e = cudaFuncSetAttribute(field_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
+                                         (int)smem);                                                           \
+                if (e != cudaSuccess) return e;                                                                \
+                if (set) set[M] = smem;                                                                        \
+            }                                                                                                  \
         }                                                                                                      \
         field_kernel<M><<<grid, kFieldThreads, smem, s>>>(P, m, m32, t, cpc, o0, o1, o2, o3, h32, pref);       \
     } while (0)

@@ -73,6 +73,12 @@ struct Ctx {
 // the epoch (acquire at system scope; bounded by the link's timeout, after which
 // KERR_PEER_TIMEOUT is recorded and the instance aborts).  Each thread fences its
 // peer stores at system scope before it arrives.
+//
+// A rank that gives up raises the sticky abort word in every rank's region.  A
+// rank checks its own abort word before it raises its flag and while it waits,
+// so a peer that was between barriers when another rank gave up stops at its
+// next barrier (KERR_PEER_ABORT) instead of waiting out its own timeout: its
+// peer stores end one barrier interval after the abort.
 MT_DEV bool sync_all(Ctx& X, int where)
 {
     if (!X.L) {
@@ -83,26 +89,43 @@ MT_DEV bool sync_all(Ctx& X, int where)
     if (!group_sync(X.B.gs, X.gsize, where)) { X.abort = true; return false; }
     X.xseq++;
     const unsigned ep = (unsigned)X.xseq;
+    const unsigned* own_abort = X.L->flags[X.srank] + kMaxShards;
     __shared__ int s_xok;
     if (threadIdx.x == 0) s_xok = 1;
     __syncthreads();
     if (threadIdx.x < X.sworld) {
         const int p = threadIdx.x;
-        if (X.grank == 0) st_release_sys_u32(X.L->flags[p] + X.srank, ep);
-        const unsigned* f = X.L->flags[X.srank] + p;
-        const unsigned long long tmo = X.L->timeout_ns;
-        long long it = 0;
-        const uint64_t t0 = globaltimer_ns();
-        while ((int)(ld_acquire_sys_u32(f) - ep) < 0) {
-            if (ld_volatile_i32(&X.B.gs->abort)) { s_xok = 0; break; }
-            if ((unsigned long long)(++it) > tmo / 8 || ((it & 1023) == 0 && globaltimer_ns() - t0 > tmo)) {
-                if (atomicCAS(&X.B.gs->err, 0, KERR_PEER_TIMEOUT) == 0) X.B.gs->err_where = where;
-                atomicExch(&X.B.gs->abort, 1);
-                s_xok = 0;
-                break;
+        bool gave_up = false;
+        if (ld_acquire_sys_u32(own_abort) != 0u) {
+            if (atomicCAS(&X.B.gs->err, 0, KERR_PEER_ABORT) == 0) X.B.gs->err_where = where;
+            atomicExch(&X.B.gs->abort, 1);
+            s_xok = 0;
+        } else {
+            if (X.grank == 0) st_release_sys_u32(X.L->flags[p] + X.srank, ep);
+            const unsigned* f = X.L->flags[X.srank] + p;
+            const unsigned long long tmo = X.L->timeout_ns;
+            long long it = 0;
+            const uint64_t t0 = globaltimer_ns();
+            while ((int)(ld_acquire_sys_u32(f) - ep) < 0) {
+                if (ld_volatile_i32(&X.B.gs->abort)) { s_xok = 0; break; }
+                if (ld_acquire_sys_u32(own_abort) != 0u) {
+                    if (atomicCAS(&X.B.gs->err, 0, KERR_PEER_ABORT) == 0) X.B.gs->err_where = where;
+                    atomicExch(&X.B.gs->abort, 1);
+                    s_xok = 0;
+                    break;
+                }
+                if ((unsigned long long)(++it) > tmo / 8 || ((it & 1023) == 0 && globaltimer_ns() - t0 > tmo)) {
+                    if (atomicCAS(&X.B.gs->err, 0, KERR_PEER_TIMEOUT) == 0) X.B.gs->err_where = where;
+                    atomicExch(&X.B.gs->abort, 1);
+                    s_xok = 0;
+                    gave_up = true;
+                    break;
+                }
+                __nanosleep(64);
             }
-            __nanosleep(64);
         }
+        if (gave_up)   // tell every rank (this one included) to stop at its next barrier
+            for (int r = 0; r < X.sworld; ++r) st_release_sys_u32(X.L->flags[r] + kMaxShards, 1u);
     }
     __syncthreads();
     if (!s_xok) { X.abort = true; return false; }

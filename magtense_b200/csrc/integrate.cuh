@@ -40,7 +40,8 @@ struct ShardLink {
     double* pool[kMaxShards][4];   // each rank's stage-argument buffers (3n FP64)
     float* pool32[kMaxShards][4];  // each rank's FP32 shadows [3][ldk]
     double* partials[kMaxShards];  // each rank's reduction slots [2][cta_total][4]
-    unsigned* flags[kMaxShards];   // each rank's barrier flags: slot p is written by rank p
+    unsigned* flags[kMaxShards];   // each rank's barrier flags: slot p is written by rank p; slot
+                                   // kMaxShards is the rank's sticky abort word (any rank may raise it)
     unsigned long long timeout_ns; // bound on one wait for the other ranks
 };
 
@@ -56,7 +57,7 @@ inline ShardLayout shard_layout(int n, int ldk, int world)
     L.pool32 = up(L.pool + sizeof(double) * 4 * 3 * (size_t)n);
     L.partials = up(L.pool32 + sizeof(float) * 4 * 3 * (size_t)ldk);
     L.flags = up(L.partials + sizeof(double) * 2 * (size_t)world * kShardMaxCtas * 4);
-    L.bytes = up(L.flags + sizeof(unsigned) * kMaxShards);
+    L.bytes = up(L.flags + sizeof(unsigned) * (kMaxShards + 1));
     return L;
 }
 

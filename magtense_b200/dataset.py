@@ -23,8 +23,12 @@ GAMMA = 2.211e5
 
 
 def std_prob_4_fields(n_seq, h_ext_a=(0, 360), h_ext_n=(0, 50), seed=0, intv=None):
-    """(n, 3) applied fields in mT of sequences intv[0]..intv[1] (all by default),
-    drawn as the reference draws them (database.py:62-70)."""
+    """(n, 3) applied fields in mT of the sequences of interval ``intv`` (all
+    ``n_seq`` by default), drawn as the reference draws them (database.py:62-70).
+    The reference fills an interval [lo, hi) from rows 0 .. hi - lo - 1 of its
+    seeded draw table, whatever lo is, so an interval database with lo > 0
+    repeats the fields of the first hi - lo sequences; this function returns
+    the same rows."""
     rng = np.random.default_rng(seed)
     rnd = rng.random(size=(n_seq, 2))
     lo, hi = (0, n_seq) if intv is None else intv
@@ -33,7 +37,7 @@ def std_prob_4_fields(n_seq, h_ext_a=(0, 360), h_ext_n=(0, 50), seed=0, intv=Non
     f = np.zeros((n_seq, 3))
     f[:, 0] = d * np.cos(theta)
     f[:, 1] = d * np.sin(theta)
-    return f[lo:hi]
+    return f[: hi - lo]
 
 
 def sequence_layout(M, res):

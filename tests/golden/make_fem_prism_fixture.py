@@ -3,14 +3,16 @@ validation data for the rotated prism (COMSOL line graphs of |B| = mu0|H|):
 documentation/examples_FEM_validation/Validation_prism/Validation_prism_normH_{x,y,z}.txt
 of the MagTense project.  Every 8th point along each line is kept.
 
-Usage: python tests/golden/make_fem_prism_fixture.py [MagTense root]
+Usage: python tests/golden/make_fem_prism_fixture.py <MagTense source root>
 """
 import sys
 from pathlib import Path
 
 import numpy as np
 
-root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+if len(sys.argv) != 2:
+    sys.exit(__doc__)
+root = Path(sys.argv[1])
 src = root / "documentation" / "examples_FEM_validation" / "Validation_prism"
 out = {}
 for c in "xyz":

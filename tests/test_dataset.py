@@ -5,18 +5,34 @@ at [t, a, ix, iy], and the database round-trips through its file."""
 import numpy as np
 
 
+def reference_field_loop(n_seq, seed, intv=None, h_ext_a=(0, 360), h_ext_n=(0, 50)):
+    """database.py:58-70 restated: the interval's sequence i takes row i of the
+    seeded table, for i in range(intv[1] - intv[0])."""
+    if intv is None:
+        intv = [0, n_seq]
+    n_intv = intv[1] - intv[0]
+    rng = np.random.default_rng(seed)
+    rnd_mat = rng.random(size=(n_seq, 2))
+    out = np.zeros((n_intv, 3))
+    for i in range(n_intv):
+        d = (h_ext_n[1] - h_ext_n[0]) * rnd_mat[i, 0] + h_ext_n[0]
+        theta = np.deg2rad((h_ext_a[1] - h_ext_a[0]) * rnd_mat[i, 1] + h_ext_a[0])
+        out[i, :2] = d * np.array([np.cos(theta), np.sin(theta)])
+    return out
+
+
 def test_fields_are_the_reference_draws():
     from magtense_b200.dataset import std_prob_4_fields
     n_seq, seed = 7, 3
-    rng = np.random.default_rng(seed)
-    rnd = rng.random(size=(n_seq, 2))
-    want = np.zeros((n_seq, 3))
-    for i in range(n_seq):
-        d = (50 - 0) * rnd[i, 0] + 0
-        theta = np.deg2rad((360 - 0) * rnd[i, 1] + 0)
-        want[i, :2] = d * np.array([np.cos(theta), np.sin(theta)])
-    np.testing.assert_array_equal(std_prob_4_fields(n_seq, seed=seed), want)
-    np.testing.assert_array_equal(std_prob_4_fields(n_seq, seed=seed, intv=(2, 5)), want[2:5])
+    np.testing.assert_array_equal(std_prob_4_fields(n_seq, seed=seed), reference_field_loop(n_seq, seed))
+    np.testing.assert_array_equal(std_prob_4_fields(n_seq, seed=seed, intv=(0, 4)),
+                                  reference_field_loop(n_seq, seed, (0, 4)))
+    # an interval that starts past 0 reuses the table's first rows, as the reference does
+    got = std_prob_4_fields(n_seq, seed=seed, intv=(2, 5))
+    np.testing.assert_array_equal(got, reference_field_loop(n_seq, seed, (2, 5)))
+    np.testing.assert_array_equal(got, std_prob_4_fields(n_seq, seed=seed)[:3])
+    np.testing.assert_array_equal(std_prob_4_fields(9, seed=5, h_ext_a=(10, 20), h_ext_n=(5, 6), intv=(4, 9)),
+                                  reference_field_loop(9, 5, (4, 9), (10, 20), (5, 6)))
 
 
 def test_sequence_layout():
