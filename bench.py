@@ -76,8 +76,13 @@ def parse():
                     help="film-batch: instances of the same workload run through the plain FP32 path for the ratio")
     ap.add_argument("--window", type=float, default=None, help="simulated ns per instance per step")
     ap.add_argument("--cpu-window", type=float, default=0.3, help="simulated ns of the bounded CPU sample")
+    ap.add_argument("--ref-window", type=float, default=0.05,
+                    help="film workloads: simulated ns per instance per step of the reference arm (and CPU baseline)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3, help="end-to-end repetitions (median reported)")
+    ap.add_argument("--no-fp64", action="store_true", help="film-batch: skip the FP64 error statement")
+    ap.add_argument("--no-large", action="store_true", help="film-batch: skip the large-plain sub-record")
     ap.add_argument("--shards", type=int, default=1,
                     help="large-plain: row shards of the one instance (over the ranks when --gpus > 1)")
     ap.add_argument("--res", type=int, nargs=3, default=None,
@@ -157,46 +162,162 @@ def dist_setup():
 
 
 # --------------------------------------------------------------------------------------------
-def cpu_reference_sample(window_ns, workload="film"):
-    """Oracle (CPU restatement, OpenMP over all host cores) on a bounded window of one instance."""
+# The reference arm and the CPU baseline: the oracle (the CPU restatement of the reference's
+# FP32-demag path) on the host cores.  The film workload runs as the reference runs it: one
+# problem per process, each process single-threaded (LandauLifshitzEquationSolver.f90:927 sets
+# one OpenMP thread), the instances side by side on all host cores.
+def film_config(B_total, window, nt):
+    """The film-batch workload, identical in both arms' JSON lines."""
+    return {"workload": f"film-batch: {B_total} instances of the 80x20x1 std-problem-4 film (n=1600), each "
+                        f"{window} ns at alpha_G=0.02 from the s-state (seeded start relaxed 0.2 ns in zero field "
+                        "at alpha_G=1), in-plane field seeded per instance (seed 1000: angle U[0,360) deg, "
+                        "magnitude U[0,50] mT), per-instance RKSUITE 'M' (tol 1e-6), output every 1 ps",
+            "instances": B_total, "window_ns": window, "outputs": nt, "field_seed": 1000,
+            "parallelism": "instances split over ranks (device arm) or host processes (reference arm); no "
+                           "data-path exchange",
+            "l2": "device arm: flushed (256 MB write) before every timed step"}
+
+
+_REF = {}
+
+
+def _ref_init(res, L, m_s, fields, window_ns, barrier):
+    """Worker set-up (spawned process): one OpenMP thread, one oracle problem per instance."""
+    os.environ["OMP_NUM_THREADS"] = "1"
+    sys.path.insert(0, str(ROOT))
     from oracle import oracle as O
-    res, L = (FILM_RES, FILM_L) if workload.startswith("film") else (LARGE_RES, LARGE_L)
-    n = int(np.prod(res))
-    h = instance_fields(0, 1)[0]
+    K32, _ = O.assemble(list(res), list(L), fp32=True)
     win = window_ns * 1e-9
-    hext = np.array([[0.0, *h], [win, *h]])
-    P = O.Problem(res, L, mode=0, gamma=GAMMA, alpha=GAMMA * 0.02, hext=hext)
-    m0 = start_state(n)
-    nt = max(2, int(round(window_ns / 1e-3)) + 1)
-    t0 = time.perf_counter()
-    _, _, _, st = P.solve(np.linspace(0, win, nt), m0, tol=1e-6)
-    dt = time.perf_counter() - t0
-    return {"value": window_ns / dt, "unit": "simulated ns/s", "cores": O.threads(), "kind": "port",
-            "sample": f"{window_ns} ns of one {res[0]}x{res[1]}x{res[2]} instance ({st['f_evals']} RHS evals, "
-                      f"{dt:.1f} s, FP32-demag restatement of the reference on the host cores)"}
+    _REF.update(O=O, res=res, L=L, m_s=m_s, fields=fields, window_ns=window_ns, K32=K32, probs={},
+                barrier=barrier, t=np.linspace(0, win, max(2, int(round(window_ns / 1e-3)) + 1)))
+
+
+def _ref_run(k):
+    """Integrate instance k of the sample over the window from the s-state; returns (start,
+    end) wall-clock times and the RHS evaluations.  Every task waits at a barrier of all the
+    pool's processes first, so each process holds exactly one task and all start together."""
+    R = _REF
+    if k not in R["probs"]:
+        h = R["fields"][k]
+        win = R["window_ns"] * 1e-9
+        R["probs"][k] = R["O"].Problem(R["res"], R["L"], mode=0, gamma=GAMMA, alpha=GAMMA * 0.02,
+                                       hext=np.array([[0.0, *h], [win, *h]]), K32=R["K32"])
+    R["barrier"].wait()
+    t0 = time.time()
+    _, _, _, st = R["probs"][k].solve(R["t"], R["m_s"], tol=1e-6)
+    return t0, time.time(), int(st["f_evals"])
+
+
+class RefPool:
+    """The film workload's instance sample on the host cores through the oracle."""
+
+    def __init__(self, B_total, window_ns, procs=None):
+        import multiprocessing as mp
+        from oracle import oracle as O
+        self.procs = procs or os.cpu_count() or 1
+        n = int(np.prod(FILM_RES))
+        # the s-state by the same recipe as the device arm, on the oracle (all host threads)
+        relax = 0.2e-9
+        P = O.Problem(FILM_RES, FILM_L, mode=0, gamma=GAMMA, alpha=GAMMA * 1.0,
+                      hext=np.array([[0, 0, 0, 0], [relax, 0, 0, 0.0]]))
+        _, yr, _, _ = P.solve(np.linspace(0, relax, 3), start_state(n), tol=1e-6)
+        m_s = yr[-1].copy()
+        del P
+        allf = instance_fields(1000, B_total)
+        self.pick = [int(k * B_total // self.procs) for k in range(self.procs)]
+        self.window_ns = window_ns
+        ctx = mp.get_context("spawn")
+        barrier = ctx.Barrier(self.procs)
+        self.pool = ctx.Pool(self.procs, initializer=_ref_init,
+                             initargs=(FILM_RES, FILM_L, m_s, {k: allf[k] for k in self.pick}, window_ns, barrier))
+
+    def step(self):
+        """One step: every process integrates its instance; the step's time runs from the
+        common start to the last process's end (set-up and process start-up excluded)."""
+        out = self.pool.map(_ref_run, self.pick, chunksize=1)
+        wall = max(b for _, b, _ in out) - min(a for a, _, _ in out)
+        return wall, sum(e for _, _, e in out)
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+    def describe(self, wall, evals):
+        return (f"{len(self.pick)} instances of the set (indices {self.pick[0]}, {self.pick[1] if len(self.pick) > 1 else ''}"
+                f"...), each integrated over the first {self.window_ns} ns of its window from the s-state by its own "
+                f"single-threaded process ({evals} RHS evals, {wall:.1f} s wall); the early part of the window "
+                "needs fewer evaluations per ns than the whole window, so this rate is an upper bound for the CPU")
+
+
+def cpu_film_sample(B_total, window_ns):
+    """cpu_baseline of the film workloads: one bounded step of the reference arm."""
+    rp = RefPool(B_total, window_ns)
+    try:
+        wall, evals = rp.step()
+    finally:
+        rp.close()
+    return {"value": len(rp.pick) * window_ns / wall, "unit": "simulated ns/s", "cores": len(rp.pick),
+            "kind": "port", "sample": rp.describe(wall, evals)}
+
+
+def cpu_large_sample(evals_per_ns, rows=256, reps=3):
+    """cpu_baseline of large-plain: the 25.8 GB tensor does not fit a bounded CPU sample,
+    so the oracle's FP32 demag product (all host threads) is timed on a subset of receiver
+    rows and scaled to all n rows; one right-hand side costs that product, and the device
+    run's evaluations per simulated ns convert it to simulated ns/s."""
+    from oracle import oracle as O
+    res, L = LARGE_RES, LARGE_L
+    n = int(np.prod(res))
+    pick = np.sort(np.random.default_rng(3).choice(n, rows, replace=False))
+    K32, _ = O.assemble(list(res), list(L), rows=pick, fp32=True)
+    rng = np.random.default_rng(1)
+    m = rng.standard_normal((3, n))
+    m = (m / np.linalg.norm(m, axis=0)).reshape(-1)
+    best = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        O.demag_rows(K32, None, m, 8e5, mode=0)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    t_eval = best * n / rows
+    return {"value": 1.0 / (t_eval * evals_per_ns), "unit": "simulated ns/s", "cores": O.threads(), "kind": "port",
+            "sample": f"FP32 demag product of {rows} of the {n} receiver rows ({best * 1e3:.1f} ms, best of {reps}) "
+                      f"scaled to one right-hand side ({t_eval:.2f} s) and to the device run's {evals_per_ns:.0f} "
+                      "evaluations per simulated ns; tensor assembly excluded"}
 
 
 def run_reference(args):
     ws, rank, _ = dist_setup()
     if rank != 0:
         return
-    vals = []
-    for _ in range(args.warmup):
-        cpu_reference_sample(args.cpu_window / 10)
-    for _ in range(args.steps):
-        vals.append(cpu_reference_sample(args.cpu_window))
-    v = statistics.median([x["value"] for x in vals])
-    cb = dict(vals[0])
-    cb["value"] = v
+    B_total = ws * args.instances
+    window = 1.0 if args.window is None else args.window
+    nt = int(round(window / 1e-3)) + 1
+    rp = RefPool(B_total, args.ref_window)
+    try:
+        for _ in range(args.warmup):
+            rp.step()
+        walls, evals = [], 0
+        for _ in range(args.steps):
+            w, e = rp.step()
+            walls.append(w)
+            evals += e
+    finally:
+        rp.close()
+    ms = statistics.mean(walls) * 1e3
+    v = len(rp.pick) * args.ref_window / (ms / 1e3)
+    cb = {"value": v, "unit": "simulated ns/s", "cores": len(rp.pick), "kind": "port",
+          "sample": rp.describe(sum(walls), evals)}
     line = {"metric": "simulated ns/s", "value": v, "unit": "simulated ns/s", "impl": "reference",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.workload} (80x20x1 std-problem-4 film instances, seeded in-plane "
-                                   "fields, 1 ns each at alpha_G = 0.02, tol 1e-6)",
-                       "window_ns": args.cpu_window,
-                       "note": "CPU restatement of the reference (the Fortran reference cannot be built here: no "
-                               "Fortran compiler, no MKL); instances are independent, so the per-instance rate is "
-                               "the batch rate on one CPU"},
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": film_config(B_total, window, nt),
+            "sample_per_step": {"instances": rp.pick, "window_ns": args.ref_window, "processes": len(rp.pick),
+                                "threads_per_process": 1},
+            "note": "CPU restatement of the reference (oracle/, FP32 demag product as the reference; the Fortran "
+                    "reference cannot be built here: no Fortran compiler, no MKL); one single-threaded process "
+                    "per host core, each integrating its own instance, as the reference solves one problem per "
+                    "single-threaded call",
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "simulated ns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -263,8 +384,10 @@ def run_ours(args):
                 line["cpu_baseline"] = cpu_adjoint_sample(args.cpu_window)
             elif args.workload == "ragged":
                 line["cpu_baseline"] = cpu_ragged_sample(args.cpu_window)
+            elif args.workload == "large-plain":
+                line["cpu_baseline"] = cpu_large_sample(line["evals_per_ns"])
             else:
-                line["cpu_baseline"] = cpu_reference_sample(args.cpu_window, args.workload)
+                line["cpu_baseline"] = cpu_film_sample(ws * args.instances, args.ref_window)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -276,8 +399,79 @@ def max_over_ranks(torch, dist, vals):
     return mx(vals)
 
 
+def fp64_error(res, L, m_s, fields, window, t, runs):
+    """<m>(t) error of device runs against the FP64 oracle (FP64 tensor and FP64 product)
+    of the same instances: max over instances, components and the samples that both took
+    at the requested time (a flag-3 return every 5000 evaluations moves a sample to the
+    internal time, RKSuitef90.f90:1374-1387).  Test infrastructure: runs after timing."""
+    from oracle import oracle as O
+    n = int(np.prod(res))
+    win = window * 1e-9
+    _, K64 = O.assemble(list(res), list(L), fp32=False, fp64=True)
+    err = {name: 0.0 for name in runs}
+    matched = {name: 0 for name in runs}
+    evals = []
+    for k, h in enumerate(fields):
+        P = O.Problem(res, L, mode=1, gamma=GAMMA, alpha=GAMMA * 0.02, hext=np.array([[0.0, *h], [win, *h]]),
+                      K64=K64)
+        t_ref, y_ref, _, st = P.solve(t, m_s, tol=1e-6)
+        evals.append(int(st["f_evals"]))
+        m_ref = y_ref.reshape(len(t), 3, n).mean(axis=2)
+        for name, per in runs.items():
+            t_got, m_got = per[k]
+            same = t_got == t_ref
+            matched[name] += int(same.sum())
+            err[name] = max(err[name], float(np.abs(m_got[same] - m_ref[same]).max()))
+    return err, matched, evals
+
+
+def large_plain_record(torch, hbm, src, local, reps=3):
+    """The large single-instance configuration (64x64x8 cubes, n = 32768, 25.8 GB FP32
+    tensor streamed from HBM once per right-hand side): device time of the persistent
+    integrator over a short window, as tensor GB/s against the measured HBM copy peak."""
+    from magtense_b200 import Solver
+    res, L = LARGE_RES, LARGE_L
+    n = int(np.prod(res))
+    rng = np.random.default_rng(1)
+    axis = rng.standard_normal(3)
+    axis /= np.linalg.norm(axis)
+    m = rng.standard_normal((3, n))
+    m0 = torch.as_tensor((m / np.linalg.norm(m, axis=0)).reshape(-1), device="cuda")
+    h = np.array([10e-3 / MU0, 0.0, 0.0])
+    win = 0.002e-9
+    s = Solver(res, L, K0=5e3, u_ea=np.tile(axis, (n, 1)))
+    try:
+        s.assemble()
+        s.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.1, hext=np.array([[0.0, *h], [win, *h]]))
+        t = np.linspace(0, win, 3)
+        s.integrate(t, m0, tol=1e-6)   # warm-up
+        runs = []
+        with Clocks(local) as clk:
+            for _ in range(reps):
+                torch.cuda.synchronize()
+                _, y, _, st = s.integrate(t, m0, tol=1e-6)
+                torch.cuda.synchronize()
+                runs.append((st["f_evals"], st["kernel_ms"], st["launches"]))
+                del y
+        clocks = clk.summary()
+    finally:
+        s.close()
+    evals = sum(r[0] for r in runs)
+    kms = sum(r[1] for r in runs)
+    gbs = 24.0 * n * n * evals / (kms / 1e3) / 1e9
+    return {"workload": "large-plain: 64x64x8 cubes of 5 nm (n=32768, 25.77 GB FP32 tensor), K=5e3 J/m^3 along a "
+                        "seeded axis, 10 mT field, alpha_G=0.1, tol 1e-6, 0.002 ns windows",
+            "rhs_evals": evals, "kernel_ms": kms, "ms_per_eval": kms / evals,
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                         "traffic": TRAFFIC_PER_TENSOR_BYTE * 24.0 * n * n * evals / sum(r[2] for r in runs),
+                         "note": f"integrate_kernel: 24*n^2 tensor bytes per RHS evaluation x {evals} evaluations "
+                                 f"over {kms:.1f} ms of device time ({reps} runs); peak {src} HBM copy; traffic in "
+                                 "DRAM bytes per launch, scaled from the 32x32x4 ncu capture"},
+            "clocks": clocks}
+
+
 def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
-    from magtense_b200 import BatchSolver, Solver
+    from magtense_b200 import BatchSolver
     res, L = FILM_RES, FILM_L
     n = int(np.prod(res))
     B = args.instances
@@ -304,38 +498,41 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
         return st
 
     times, stats, clocks, flush = timed_steps(torch, step, args.steps, args.warmup, dist, local)
-    # end to end through the public API: host m0 in (pinned), host trajectories out
-    e2e_ms = None
-    if not args.no_e2e:
-        pin_in = torch.from_numpy(m0_host).pin_memory()
-        pin_out = torch.empty((B, nt, 3 * n), dtype=torch.float64).pin_memory()
-        e2e = []
-        for _ in range(max(1, args.steps)):
-            flush.fill_(1.0)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            dev_in = pin_in.to("cuda", non_blocking=True)
-            _, y, _, _ = bs.integrate(t, dev_in, tol=1e-6)
-            pin_out.copy_(y, non_blocking=True)
-            torch.cuda.synchronize()
-            e2e.append((time.perf_counter() - t0) * 1e3)
-            del y
-        e2e_ms = statistics.median(e2e)
     # the plain FP32 single-instance path on the same workload, for the ratio: seeded instances
     # of this rank's set, each integrated over the same window, one after another
     pick = sorted(int(k) for k in np.random.default_rng(7).choice(B, size=min(args.plain_sample, B), replace=False))
-    plain_s, plain_evals = 0.0, 0
+    plain_s, plain_evals, plain_m = 0.0, 0, []
     for k in pick:
         plain.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.02,
                            hext=np.array([[0.0, *fields[k]], [win, *fields[k]]]))
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        _, yp, _, pst = plain.integrate(t, m_s, tol=1e-6)
+        tp, yp, _, pst = plain.integrate(t, m_s, tol=1e-6)
         torch.cuda.synchronize()
         plain_s += time.perf_counter() - t0
         plain_evals += pst["f_evals"]
+        plain_m.append((tp, yp.view(nt, 3, n).mean(dim=2).cpu().numpy()))
         del yp
     plain_rate = len(pick) * window / plain_s
+    # end to end through the public API: host m0 in (pinned), host trajectories out
+    e2e_ms, batch_m = None, None
+    if not args.no_e2e:
+        pin_in = torch.from_numpy(m0_host).pin_memory()
+        pin_out = torch.empty((B, nt, 3 * n), dtype=torch.float64).pin_memory()
+        e2e = []
+        for _ in range(max(1, min(args.steps, args.e2e_steps))):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            dev_in = pin_in.to("cuda", non_blocking=True)
+            t_b, y, _, _ = bs.integrate(t, dev_in, tol=1e-6)
+            pin_out.copy_(y, non_blocking=True)
+            torch.cuda.synchronize()
+            e2e.append((time.perf_counter() - t0) * 1e3)
+            del y
+        e2e_ms = statistics.median(e2e)
+        batch_m = [(t_b[k], pin_out[k].view(nt, 3, n).mean(dim=2).numpy()) for k in pick]
+        del pin_out
     step_ms = sum(times) / len(times)   # the K timed steps as one bracket, L2 flushes excluded
     step_ms, e2e_red = max_over_ranks(torch, dist, [step_ms, e2e_ms or 0.0])
     if rank != 0:
@@ -352,12 +549,8 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
         "metric": "simulated ns/s", "value": value, "unit": "simulated ns/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
-        "config": {"workload": f"film-batch: {B} instances/rank of the 80x20x1 std-problem-4 film (n=1600), "
-                               f"{window} ns each at alpha_G=0.02, seeded in-plane fields, per-instance RKSUITE 'M' "
-                               f"(tol 1e-6, output every 1 ps), {args.precision} tcgen05 demag GEMM",
-                   "instances_per_rank": B, "window_ns": window, "outputs": nt,
-                   "parallelism": f"instances sharded over {ws} rank(s)",
-                   "l2": "flushed (256 MB write) before every timed step"},
+        "config": film_config(ws * B, window, nt),
+        "precision": f"{args.precision} tcgen05 demag GEMM inside one persistent kernel",
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
                      "frac": achieved / peak_tf, "traffic": None,
                      "note": f"batch_kernel (the whole persistent integrator, GEMM and RKSUITE coroutines): 18*n^2 "
@@ -380,6 +573,17 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
     if e2e_ms is not None:
         line["e2e"] = {"value": sim_ns / (e2e_red / 1e3), "unit": "simulated ns/s",
                        "h2d_bytes_per_step": B * 3 * n * 8, "d2h_bytes_per_step": B * nt * 3 * n * 8}
+    if not args.no_fp64 and batch_m is not None:
+        err, matched, ev = fp64_error(res, L, m_s.cpu().numpy(), [fields[k] for k in pick], window, t,
+                                      {args.precision: batch_m, "plain_fp32": plain_m})
+        line["m_err_vs_fp64"] = {
+            "max_abs_mean_m": err, "samples_compared": matched, "instances": pick, "fp64_rhs_evals": ev,
+            "bound": 1e-4, "within_bound": all(v <= 1e-4 for v in err.values()),
+            "note": f"max over the {len(pick)} instances, 3 components and all {nt} output samples taken at the "
+                    "requested time of |<m>_device - <m>_FP64|, <m> the mean over cells; FP64 = the oracle with "
+                    "the FP64 tensor and FP64 demag product, same s-state, field and tolerances, run after timing"}
+    if not args.no_large:
+        line["large_plain"] = large_plain_record(torch, hbm, src, local)
     return line
 
 
@@ -729,6 +933,7 @@ def bench_plain(torch, args, ws, rank, local, dist, hbm, src):
                 "d2h_bytes_per_step": nt * 3 * n * 8},
         "gpu_launches": int(launches),
         "rhs_evals_per_s": evals / (sum(times) / 1e3) * ws,
+        "evals_per_ns": evals / (len(stats) * window),
         "step_ms_each": [round(x, 3) for x in times],
         "kernel_ms_each": [round(sum(x["kernel_ms"] for x in st), 3) for st in stats],
         "clocks": clocks,

@@ -231,6 +231,11 @@ int mt_batch_set_material(mt_batch* b, double A0, const double* Ms, const double
  * solver 1 (explicit) uses row 0 of each instance's table */
 int mt_batch_set_dynamics(mt_batch* b, int solver, double gamma, const double* alpha0, const double* hext,
                           int nt_hext, int renormalize);
+/* damping table alpha_tab[nt_alpha][2] (rows {t, alpha}) shared by the instances whose
+ * alpha0 is 0: alpha() of LandauLifshitzEquationSolver.f90:281-294 (interp1 of the table,
+ * 0 outside it), as mt_set_dynamics's alpha_tab; may come before or after
+ * mt_batch_set_dynamics */
+int mt_batch_set_alpha_table(mt_batch* b, const double* alpha_tab, int nt_alpha);
 int mt_batch_assemble_demag(mt_batch* b, void* stream);
 /* m0_dev: B*3n FP64; y_out_dev: B*nt*3n FP64 or NULL; t_out, flags: B*nt host;
  * stats: B entries (kernel_ms/launches of the whole batch in stats[0]). */

@@ -1052,6 +1052,11 @@ struct mt_batch {
     double* alpha0 = nullptr;
     int nt_hext = 0;
     bool have_dynamics = false;
+    // the damping table shared by the instances whose alpha0 is 0 (alpha(), :281-294), and the
+    // shared dynamics last set, so that either call may come first
+    std::vector<double> alpha_tab;
+    int solver = 2, renorm = 0;
+    double gamma = 0.0;
 };
 
 namespace {
@@ -1155,6 +1160,17 @@ int mt_batch_set_material(mt_batch* bt, double A0, const double* Ms, const doubl
     return mt_set_material(bt->h, A0, Ms, K0, u_ea);
 }
 
+// The shared part of the batch's dynamics lives in the inner handle: solver, gamma, the
+// renormalisation switch and the damping table; per-instance fields and alpha0 are the
+// batch's own.  Its field table is unused.
+static int batch_shared_dynamics(mt_batch* bt)
+{
+    double dummy_tab[8] = {0, 0, 0, 0, 1, 0, 0, 0};
+    const bool tab = !bt->alpha_tab.empty();
+    return mt_set_dynamics(bt->h, bt->solver, bt->gamma, 1.0, tab ? bt->alpha_tab.data() : dummy_tab,
+                           tab ? (int)(bt->alpha_tab.size() / 2) : 1, dummy_tab, 2, 0, bt->renorm);
+}
+
 int mt_batch_set_dynamics(mt_batch* bt, int solver, double gamma, const double* alpha0, const double* hext, int nt_hext,
                           int renormalize)
 {
@@ -1171,12 +1187,18 @@ int mt_batch_set_dynamics(mt_batch* bt, int solver, double gamma, const double* 
     CUDA_TRY(cudaMemcpy(bt->hext, he.data(), sizeof(double) * he.size(), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(bt->alpha0, al.data(), sizeof(double) * al.size(), cudaMemcpyHostToDevice));
     bt->nt_hext = nt_hext;
-    // the shared part (solver, gamma) lives in the inner handle; its tables are unused
-    double dummy_tab[8] = {0, 0, 0, 0, 1, 0, 0, 0};
-    int rc = mt_set_dynamics(bt->h, solver, gamma, 1.0, dummy_tab, 1, dummy_tab, 2, 0, renormalize);
+    bt->solver = solver; bt->gamma = gamma; bt->renorm = renormalize ? 1 : 0;
+    int rc = batch_shared_dynamics(bt);
     if (rc) return rc;
     bt->have_dynamics = true;
     return MT_OK;
+}
+
+int mt_batch_set_alpha_table(mt_batch* bt, const double* alpha_tab, int nt_alpha)
+{
+    if (!bt || nt_alpha < 0 || (nt_alpha > 0 && !alpha_tab)) return fail(MT_ERR_ARG, "bad argument");
+    bt->alpha_tab.assign(alpha_tab, alpha_tab + 2 * (size_t)nt_alpha);
+    return bt->have_dynamics ? batch_shared_dynamics(bt) : MT_OK;
 }
 
 int mt_batch_assemble_demag(mt_batch* bt, void* stream)

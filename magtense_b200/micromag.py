@@ -239,32 +239,37 @@ class MicromagProblem:
         per call; its dataset workflow loops ``run_simulation`` over seeded fields
         (python/scripts/database.py:19-87).
 
-        h_ext: (B, nt_h_ext, 3) fields in A/m at the times linspace(0, t_end,
-            nt_h_ext), or (B, 3) constant fields (the explicit solver takes (B, 3):
-            one quasi-static field per instance).
+        h_ext, dynamic solver: (B, nt_h_ext, 3) fields in A/m at the times
+            linspace(0, t_end, nt_h_ext), or (B, 3) constant fields.
+        h_ext, explicit solver: (B, 3), one quasi-static field per instance, or
+            (B, K, 3), a branch of K fields per instance taken in turn, each from
+            the state the previous one ended in (sample nt - 1, as
+            LandauLifshitzEquationSolver.f90:165-186 chains its field rows), with
+            the t_conv / conv_tol early exit of every field's run.
         m0: None (this problem's m0 for every instance) or (B, n, 3).
         alpha: None (this problem's alpha) or a scalar or (B,) array, as ``alpha``
-            of the constructor.
+            of the constructor; instances whose alpha is 0 follow this problem's
+            alpha(t) table (``t_alpha``, ``alpha_fct``), as the reference's alpha().
         precision: "int8" (exact fixed-point product, the default), "fp32" (the
             reference's FP32 product), "bf16x3", "bf16x2" or "fp16s".
-        Returns (t_out (B, nt), M (B, nt, n, 1, 3) or None without the trajectory,
-        pts (n, 3)); per-instance statistics go to ``self.last_stats``."""
+        Returns (t_out (B, nt), M (B, nt, n, K, 3) or None without the trajectory,
+        pts (n, 3)), K = 1 except for an explicit branch; t_out is that of the last
+        field; per-instance statistics go to ``self.last_stats`` (a list per
+        field of a branch)."""
         from .solver import BatchSolver
         self._check_supported()
         if self.N_load > 2:
             raise NotImplementedError("run_batch assembles its tensor; loading one from disk is run_simulation only")
-        if alpha is None and self.alpha_mm == 0.0:
-            raise NotImplementedError("the batched path takes a constant alpha per instance, not an alpha(t) table")
         n = self.ntot
         h = np.asarray(h_ext, dtype=np.float64)
+        if h.ndim not in (2, 3) or h.shape[-1] != 3:
+            raise ValueError("h_ext must be (B, 3) or (B, K, 3)")
+        branch = self._solver == 1 and h.ndim == 3
         if h.ndim == 2:
             h = np.repeat(h[:, None, :], 2, axis=1)
-        if h.ndim != 3 or h.shape[2] != 3:
-            raise ValueError("h_ext must be (B, 3) or (B, nt_h_ext, 3)")
-        B, ntab = h.shape[0], h.shape[1]
-        tab = np.zeros((B, ntab, 4))
-        tab[:, :, 0] = np.linspace(0, t_end, ntab)[None, :]
-        tab[:, :, 1:] = h
+        B = h.shape[0]
+        # one table per run: the dynamic solver's time table, or one quasi-static row per field
+        rows = [h[:, k:k + 1, :] for k in range(h.shape[1])] if branch else [h]
         al = np.broadcast_to(np.asarray(self.alpha_mm if alpha is None else alpha, dtype=np.float64), (B,))
         if m0 is None:
             base = np.concatenate((self.m0[:, 0], self.m0[:, 1], self.m0[:, 2]))
@@ -273,16 +278,31 @@ class MicromagProblem:
             m0s = np.asarray(m0, dtype=np.float64).reshape(B, n, 3).transpose(0, 2, 1).reshape(B, 3 * n).copy()
         bs = BatchSolver(self.grid_n, self.grid_L, B, precision=precision, A0=self.A0, Ms=self.Ms, K0=self.K0,
                          u_ea=self.u_ea)
+        M = None if not keep_trajectory else np.zeros((B, nt, n, len(rows), 3))
+        stats = []
         try:
             bs.assemble()
-            bs.set_dynamics(hext=tab, alpha=al, solver=self._solver, gamma=self.gamma, renormalize=self.renormalize)
             t = np.linspace(0, t_end, nt)
-            t_out, y, _, st = bs.integrate(t, m0s, tol=self.tol, thres=self.thres, t_conv=self.t_conv,
-                                           conv_tol=float(self.conv_tol[0]), keep_trajectory=keep_trajectory)
-            M = None if y is None else y.view(B, nt, 3, n).permute(0, 1, 3, 2).cpu().numpy()[:, :, :, None, :]
+            m_cur = m0s
+            for k, hk in enumerate(rows):
+                ntab = hk.shape[1]
+                tab = np.zeros((B, ntab, 4))
+                tab[:, :, 0] = np.linspace(0, t_end, ntab)[None, :]
+                tab[:, :, 1:] = hk
+                bs.set_dynamics(hext=tab, alpha=al, solver=self._solver, gamma=self.gamma,
+                                renormalize=self.renormalize,
+                                alpha_tab=np.ascontiguousarray(self.alphat) if np.any(al == 0.0) else None)
+                t_out, y, _, st = bs.integrate(t, m_cur, tol=self.tol, thres=self.thres, t_conv=self.t_conv,
+                                               conv_tol=float(self.conv_tol[0]),
+                                               keep_trajectory=keep_trajectory or k + 1 < len(rows))
+                stats.append(st)
+                if y is not None:
+                    if M is not None:
+                        M[:, :, :, k, :] = y.view(B, nt, 3, n).permute(0, 1, 3, 2).cpu().numpy()
+                    m_cur = y[:, nt - 1].clone()
         finally:
             bs.close()
-        self.last_stats = st
+        self.last_stats = stats if branch else stats[0]
         return t_out, M, grid_points(self.grid_n, self.grid_L)
 
 

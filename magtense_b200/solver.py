@@ -347,11 +347,16 @@ class BatchSolver:
         with torch.cuda.device(self.device):
             check(_lib.lib().mt_batch_assemble_demag(self._h, _stream(stream)), "mt_batch_assemble_demag")
 
-    def set_dynamics(self, *, hext, alpha, solver=2, gamma=0.0, renormalize=False):
-        """hext: (B, nt_hext, 4) rows {t, Hx, Hy, Hz} per instance; alpha: scalar or (B,)."""
+    def set_dynamics(self, *, hext, alpha, solver=2, gamma=0.0, renormalize=False, alpha_tab=None):
+        """hext: (B, nt_hext, 4) rows {t, Hx, Hy, Hz} per instance; alpha: scalar or (B,);
+        alpha_tab: (nt_alpha, 2) rows {t, alpha}, the damping of the instances whose
+        alpha is 0 (interpolated in t, 0 outside the table), as the reference's alpha()."""
         he = _np_d(hext).reshape(self.B, -1, 4)
         al = _np_d(np.broadcast_to(np.asarray(alpha, dtype=np.float64), (self.B,)))
-        self._tables = (he, al)
+        at = np.zeros((0, 2)) if alpha_tab is None else _np_d(alpha_tab).reshape(-1, 2)
+        check(_lib.lib().mt_batch_set_alpha_table(self._h, at.ctypes.data_as(_lib.D), at.shape[0]),
+              "mt_batch_set_alpha_table")
+        self._tables = (he, al, at)
         check(_lib.lib().mt_batch_set_dynamics(self._h, int(solver), float(gamma), al.ctypes.data_as(_lib.D),
                                                he.ctypes.data_as(_lib.D), he.shape[1], int(bool(renormalize))),
               "mt_batch_set_dynamics")

@@ -46,6 +46,7 @@
 #include <string.h>
 #include <complex.h>
 #include <float.h>
+#include <omp.h>
 
 #define OR_PI 3.141592653589793
 /* mu0 = 4*pi*1e-7 evaluated left to right, TileTensorHelperFunctions.f90:5 */
@@ -278,6 +279,8 @@ typedef struct {
     double lap_coef[3];               /* 1/d^2 per axis as the reference forms it */
     const float* K32;                 /* [c][i][j], owned by caller */
     const double* K64;
+    float* KT32;                      /* [c][j][i]: the same tensors by source column, owned here */
+    double* KT64;
     int renorm;                       /* per-cell |m| renormalisation after accepted steps */
     float* ms;                        /* FP32 copy of m for the demag product */
     long nrhs;
@@ -328,9 +331,26 @@ or_problem* or_problem_create(int nx, int ny, int nz, double Lx, double Ly, doub
     return p;
 }
 
+/* Source-column copies of the tensors for the column sweep of the demag product. */
+static void *or_transpose(const void* src, int n, size_t es)
+{
+    if (!src) return NULL;
+    char* dst = (char*)malloc(es * 6 * (size_t)n * n);
+    const char* s = (const char*)src;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int c = 0; c < 6; ++c)
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i)
+                memcpy(dst + es * (((size_t)c * n + j) * n + i), s + es * (((size_t)c * n + i) * n + j), es);
+    return dst;
+}
+
 void or_problem_set_tensor(or_problem* p, const float* K32, const double* K64)
 {
     p->K32 = K32; p->K64 = K64;
+    free(p->KT32); free(p->KT64);
+    p->KT32 = (float*)or_transpose(K32, p->n, sizeof(float));
+    p->KT64 = (double*)or_transpose(K64, p->n, sizeof(double));
 }
 void or_problem_set_hext_ind(or_problem* p, int ind) { p->hext_ind = ind; }
 void or_problem_set_renorm(or_problem* p, int on) { p->renorm = on; }
@@ -341,9 +361,78 @@ void or_problem_destroy(or_problem* p)
 {
     if (!p) return;
     free(p->alpha_tab); free(p->hext); free(p->Jfact); free(p->Kfact); free(p->Mfact);
-    free(p->A6); free(p->ms); free(p->klimb); free(p->row_scale); free(p->mlimb); free(p);
+    free(p->A6); free(p->ms); free(p->klimb); free(p->row_scale); free(p->mlimb);
+    free(p->KT32); free(p->KT64); free(p);
 }
 int or_problem_range_err(const or_problem* p) { return p->range_err; }
+
+/* The demag product H_a(i) = Ms_i * sum_b sum_j (-m_b(j)) K_ab(i, j) as the reference
+ * BLAS SGEMV sweeps it (LandauLifshitzEquationSolver.f90:718-747): for every
+ * component a, y = 0, then for each block b = 1..3 and source j = 1..n in order,
+ * y(i) = y(i) + (-m_b(j)) * K_ab(i, j), each multiply and add rounded separately;
+ * finally Ms_i * y(i).  The sweep runs over source columns of the column-major
+ * copy, so it vectorises across the receivers i in [i0, i1) without changing any
+ * receiver's order of operations (blocks: x: xx xy xz; y: xy yy yz; z: xz yz zz). */
+static const int or_blk[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+
+__attribute__((target_clones("avx2", "default")))
+static void colsweep_f32(const float* KT, int n, const float* ms, const float* Mfact, int i0, int i1, double* Hm)
+{
+    float* y = (float*)malloc(sizeof(float) * (size_t)(i1 > i0 ? i1 - i0 : 1));
+    for (int a = 0; a < 3; ++a) {
+        for (int i = i0; i < i1; ++i) y[i - i0] = 0.0f;
+        for (int b = 0; b < 3; ++b) {
+            const float* K = KT + (size_t)or_blk[a][b] * n * n;
+            const float* xb = ms + (size_t)b * n;
+            for (int j = 0; j < n; ++j) {
+                const float tmp = -xb[j];
+                const float* col = K + (size_t)j * n + i0;
+                float* yy = y;
+                const int len = i1 - i0;
+#pragma omp simd
+                for (int i = 0; i < len; ++i) yy[i] = yy[i] + tmp * col[i];
+            }
+        }
+        for (int i = i0; i < i1; ++i) {
+            const float hm = y[i - i0] * Mfact[i];
+            Hm[(size_t)a * n + i] = (double)hm;
+        }
+    }
+    free(y);
+}
+
+__attribute__((target_clones("avx2", "default")))
+static void colsweep_f64(const double* KT, int n, const double* m, const float* Mfact, int i0, int i1, double* Hm)
+{
+    double* y = (double*)malloc(sizeof(double) * (size_t)(i1 > i0 ? i1 - i0 : 1));
+    for (int a = 0; a < 3; ++a) {
+        for (int i = i0; i < i1; ++i) y[i - i0] = 0.0;
+        for (int b = 0; b < 3; ++b) {
+            const double* K = KT + (size_t)or_blk[a][b] * n * n;
+            const double* xb = m + (size_t)b * n;
+            for (int j = 0; j < n; ++j) {
+                const double tmp = -xb[j];
+                const double* col = K + (size_t)j * n + i0;
+                double* yy = y;
+                const int len = i1 - i0;
+#pragma omp simd
+                for (int i = 0; i < len; ++i) yy[i] = yy[i] + tmp * col[i];
+            }
+        }
+        for (int i = i0; i < i1; ++i) Hm[(size_t)a * n + i] = y[i - i0] * (double)Mfact[i];
+    }
+    free(y);
+}
+
+/* this thread's receivers of an OpenMP team: contiguous blocks of 16 */
+static void or_thread_cells(int n, int* i0, int* i1)
+{
+    const int nth = omp_get_num_threads(), t = omp_get_thread_num();
+    const int blocks = (n + 15) / 16;
+    const int b0 = (int)((long long)blocks * t / nth), b1 = (int)((long long)blocks * (t + 1) / nth);
+    *i0 = b0 * 16 < n ? b0 * 16 : n;
+    *i1 = b1 * 16 < n ? b1 * 16 : n;
+}
 
 /* mode 2 tensor limbs from the FP32 tensor: row r = (a, i), column (b, j).
  * 2^e_r puts the row's largest |K| in [2^29, 2^30); Kq = rint(K 2^e_r) =
@@ -520,39 +609,18 @@ void or_fields(or_problem* p, double t, const double* m, double* Hj, double* Hh,
     } else if (p->mode == 0) {
         float* ms = p->ms;
         for (int i = 0; i < 3 * n; ++i) ms[i] = (float)m[i];
-        const float* K = p->K32;
-        /* blocks used per output component: x: xx xy xz ; y: xy yy yz ; z: xz yz zz */
-        static const int blk[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
-#pragma omp parallel for schedule(static)
-        for (int i = 0; i < n; ++i) {
-            for (int a = 0; a < 3; ++a) {
-                float acc = 0.0f;
-                for (int b = 0; b < 3; ++b) {
-                    const float* row = K + ((size_t)blk[a][b] * n + i) * (size_t)n;
-                    const float* xb = ms + (size_t)b * n;
-                    for (int j = 0; j < n; ++j) {
-                        float tmp = -xb[j];
-                        acc = acc + tmp * row[j];
-                    }
-                }
-                float hm = acc * p->Mfact[i];
-                Hm[(size_t)a * n + i] = (double)hm;
-            }
+#pragma omp parallel
+        {
+            int i0, i1;
+            or_thread_cells(n, &i0, &i1);
+            colsweep_f32(p->KT32, n, ms, p->Mfact, i0, i1, Hm);
         }
     } else {
-        const double* K = p->K64;
-        static const int blk[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
-#pragma omp parallel for schedule(static)
-        for (int i = 0; i < n; ++i) {
-            for (int a = 0; a < 3; ++a) {
-                double acc = 0.0;
-                for (int b = 0; b < 3; ++b) {
-                    const double* row = K + ((size_t)blk[a][b] * n + i) * (size_t)n;
-                    const double* xb = m + (size_t)b * n;
-                    for (int j = 0; j < n; ++j) acc = acc + (-xb[j]) * row[j];
-                }
-                Hm[(size_t)a * n + i] = acc * (double)p->Mfact[i];
-            }
+#pragma omp parallel
+        {
+            int i0, i1;
+            or_thread_cells(n, &i0, &i1);
+            colsweep_f64(p->KT64, n, m, p->Mfact, i0, i1, Hm);
         }
     }
 }
