@@ -173,9 +173,10 @@ int mt_integrate_shards_local(mt_handle* const* hs, int world, const double* t, 
                               double* t_out, double* y_out_dev, int* flags, mt_stats* stats, void* stream);
 
 /* Allocation-free dm/dt.  No counterpart in the reference: it exists for
- * callers that may not allocate device memory (for example code running while
- * a CUDA graph is captured, or a host framework that owns all device memory
- * through its own pool).  Same result as mt_rhs, but the FP32 copy of m that
+ * callers that may not allocate device memory (for example a host framework
+ * that owns all device memory through its own pool, or a host program whose
+ * device-memory budget is fixed once it has started).  Same result as mt_rhs,
+ * but the FP32 copy of m that
  * the demag product reads lives in a fixed array inside the library
  * (3 * MT_NOALLOC_MAX_CELLS floats, held on every GPU that loads the library
  * until the process exits) instead of memory allocated on first use; the call

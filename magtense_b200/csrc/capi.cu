@@ -1614,10 +1614,10 @@ int icl_MVMult_GetH_sparse(const float*, const float*, const float*, float*, flo
 // Allocation-free right-hand side
 // ---------------------------------------------------------------------------
 // mt_rhs keeps an FP32 copy of m for the demag product in memory it allocates
-// on first use.  Some callers may not allocate device memory at all: code that
-// runs while a CUDA graph is being captured, host frameworks that hand out all
-// device memory from their own pool, or control loops that must never touch
-// the allocator.  For them the same copy lives in this fixed array instead,
+// on first use.  Some callers may not allocate device memory at all: host
+// frameworks that hand out all device memory from their own pool, or host
+// programs and control loops whose device-memory budget is fixed once they have
+// started and must never touch the allocator again.  For them the same copy lives in this fixed array instead,
 // reserved once when the library loads and held by every GPU that loads it
 // until the process exits.  Its size fixes the largest grid this entry point
 // accepts.

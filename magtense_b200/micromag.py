@@ -19,6 +19,9 @@ Differences from the reference, all deliberate:
     field rows as the solver does (:165-186).
   * ``renormalize=True`` (keyword only, default False) rescales every cell's m
     to unit length after each accepted step.
+  * explicit mode: after a convergence exit (t_conv / conv_tol) the next field
+    starts from the sample the exit stored; the reference starts it from sample
+    nt, which that run did not write.
 """
 from __future__ import annotations
 
@@ -217,7 +220,7 @@ class MicromagProblem:
             t_out, y, flags, st = s.integrate(t, m_cur, tol=self.tol, thres=self.thres, t_conv=self.t_conv,
                                               conv_tol=float(self.conv_tol[0]))
             stats.append(st)
-            m_cur = y[nt - 1].clone()
+            m_cur = y[_chain_sample(st, nt)].clone()
             yh = y.view(nt, 3, n).permute(0, 2, 1).cpu().numpy()
             M[:, :, i, :] = yh
             if H is not None:   # StoreHeffComponents: fields at the requested times
@@ -299,11 +302,20 @@ class MicromagProblem:
                 if y is not None:
                     if M is not None:
                         M[:, :, :, k, :] = y.view(B, nt, 3, n).permute(0, 1, 3, 2).cpu().numpy()
-                    m_cur = y[:, nt - 1].clone()
+                    m_cur = torch.stack([y[b, _chain_sample(st[b], nt)] for b in range(B)])
         finally:
             bs.close()
         self.last_stats = stats if branch else stats[0]
         return t_out, M, grid_points(self.grid_n, self.grid_L)
+
+
+def _chain_sample(stats, nt):
+    """The sample the next field of an explicit chain starts from: the last one
+    (LandauLifshitzEquationSolver.f90:177 takes sample nt), or, after a
+    convergence exit, the sample the exit stored.  The reference reads sample nt
+    there too, which that run never wrote."""
+    k = int(stats.get("converged_at", -1))
+    return k if 0 <= k < nt else nt - 1
 
 
 def load_demag_tensor(filename: str, n: int):

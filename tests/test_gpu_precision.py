@@ -117,3 +117,54 @@ def test_precision_mean_m_trajectory_errors(torch_cuda, oracle):
           "median RHS evaluations:", evals)
     for prec in PRECS:
         assert errs[prec] <= M_BOUND[prec], (prec, errs[prec])
+
+
+def test_headline_geometry_mean_m_error_vs_fp64(torch_cuda, oracle):
+    """The error statement of the batching configuration on its own geometry: the
+    80x20x1 film from the s-state (seeded start relaxed 0.2 ns in zero field at
+    alpha_G = 1), 4 instances of the seed-1000 in-plane field set, 0.1 ns at
+    alpha_G = 0.02, tol 1e-6, output every 1 ps.  Both the int8 batched path and
+    the plain FP32 path stay within 1e-4 of the FP64 oracle in <m>(t) (about 1e-7
+    is measured over the full 1 ns)."""
+    from magtense_b200 import BatchSolver, Solver
+    res, L = [80, 20, 1], [500e-9, 125e-9, 3e-9]
+    n, B = 1600, 4
+    rng = np.random.default_rng(0)
+    m = np.ones((3, n)) / np.sqrt(3) + 0.01 * rng.standard_normal((3, n))
+    m = (m / np.linalg.norm(m, axis=0)).reshape(-1)
+    s = Solver(res, L)
+    s.assemble()
+    s.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 1.0, hext=np.array([[0, 0, 0, 0], [0.2e-9, 0, 0, 0.0]]))
+    _, yr, _, _ = s.integrate(np.linspace(0, 0.2e-9, 3), torch_cuda.as_tensor(m, device="cuda"), tol=1e-6)
+    m_s = yr[-1].cpu().numpy()
+    r2 = np.random.default_rng(1000)
+    ang = r2.uniform(0, 2 * np.pi, 256)
+    mag = r2.uniform(0, 50e-3, 256) / MU0
+    pick = [0, 85, 170, 255]
+    Hf = np.stack([mag * np.cos(ang), mag * np.sin(ang), np.zeros(256)], 1)[pick]
+    win = 0.1e-9
+    t = np.linspace(0, win, 101)
+    hext = np.zeros((B, 2, 4))
+    hext[:, 1, 0] = win
+    hext[:, :, 1:] = Hf[:, None, :]
+    bs = BatchSolver(res, L, B, precision="int8")
+    bs.assemble()
+    bs.set_dynamics(hext=hext, alpha=GAMMA * 0.02, gamma=GAMMA)
+    t_b, y_b, _, st_b = bs.integrate(t, np.tile(m_s, (B, 1)), tol=1e-6)
+    y_b = y_b.cpu().numpy().reshape(B, len(t), 3, n).mean(axis=3)
+    bs.close()
+    _, K64 = oracle.assemble(res, L, fp32=False, fp64=True)
+    worst = {"int8": 0.0, "fp32": 0.0}
+    for b in range(B):
+        s.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.02, hext=hext[b])
+        t_p, y_p, _, _ = s.integrate(t, torch_cuda.as_tensor(m_s, device="cuda"), tol=1e-6)
+        y_p = y_p.cpu().numpy().reshape(len(t), 3, n).mean(axis=2)
+        P = oracle.Problem(res, L, mode=1, gamma=GAMMA, alpha=GAMMA * 0.02, hext=hext[b], K64=K64)
+        t_r, y_r, _, _ = P.solve(t, m_s, tol=1e-6)
+        y_r = y_r.reshape(len(t), 3, n).mean(axis=2)
+        for name, tg, yg in (("int8", t_b[b], y_b[b]), ("fp32", t_p, y_p)):
+            same = tg == t_r
+            assert same.mean() > 0.95
+            worst[name] = max(worst[name], float(np.abs(yg[same] - y_r[same]).max()))
+    print(f"80x20x1, 4 instances, 0.1 ns: max |<m> - <m>_FP64| {worst}")
+    assert worst["int8"] <= 1e-4 and worst["fp32"] <= 1e-4, worst

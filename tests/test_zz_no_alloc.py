@@ -1,12 +1,14 @@
 """mt_rhs_noalloc: the allocation-free right-hand side, for callers that may not
-allocate device memory (code running during a CUDA graph capture, or a host
-framework that hands out all device memory from its own pool).  Its scratch is a
-fixed array inside the library, so the call itself allocates nothing.
+allocate device memory (a host framework that hands out all device memory from
+its own pool, or a host program whose device-memory budget is fixed once it has
+started).  Its scratch is a fixed array inside the library, so the call itself
+allocates nothing.
 
 Checked through the C ABI against mt_rhs on two calls in a row (the array keeps
-the previous call's contents, which must not leak into the next result), and
-the grid-size limit.  Collected last so that a stop at the first failure has
-already run every other test."""
+the previous call's contents, which must not leak into the next result), on a
+handle whose first right-hand side is the allocation-free one (device free
+memory unchanged across its calls), and the grid-size limit.  Collected last so
+that a stop at the first failure has already run every other test."""
 import ctypes
 
 import numpy as np
@@ -44,6 +46,48 @@ def test_noalloc_rhs_matches_rhs_twice():
                                       stream), "mt_rhs_noalloc")
         torch.cuda.synchronize()
         r, g = ref.cpu().numpy(), got.cpu().numpy()
+        assert np.all(np.isfinite(g))
+        np.testing.assert_allclose(g, r, rtol=1e-12, atol=1e-12 * np.abs(r).max())
+
+
+def test_noalloc_first_on_a_fresh_handle_allocates_nothing():
+    """The handle has never run mt_rhs (so it holds no FP32 copy of m of its own):
+    the first call sets up the array's address, later calls leave the device's free
+    memory as it was, and the result equals mt_rhs."""
+    import torch
+    from magtense_b200 import Solver, _lib
+    torch.cuda.set_device(0)
+    res, L = [20, 5, 1], [125e-9, 31.25e-9, 3e-9]
+    n = 100
+    s = Solver(res, L)
+    s.assemble()
+    s.set_dynamics(solver=2, gamma=2.211e5, alpha=2.211e5 * 0.02,
+                   hext=np.array([[0.0, -2e4, 3e3, 0.0], [1e-9, -2e4, 3e3, 0.0]]))
+    lib = _lib.lib()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rng = np.random.default_rng(5)
+    ms = []
+    for _ in range(3):
+        m = rng.standard_normal((3, n))
+        ms.append(torch.as_tensor((m / np.linalg.norm(m, axis=0)).reshape(-1), device="cuda"))
+    outs = [torch.full((3 * n,), float("nan"), dtype=torch.float64, device="cuda") for _ in range(3)]
+    refs = [torch.empty(3 * n, dtype=torch.float64, device="cuda") for _ in range(3)]
+    _lib.check(lib.mt_rhs_noalloc(s._h, 0.1e-9, ctypes.c_void_p(ms[0].data_ptr()),
+                                  ctypes.c_void_p(outs[0].data_ptr()), stream), "mt_rhs_noalloc")
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for k in (1, 2):
+        _lib.check(lib.mt_rhs_noalloc(s._h, 0.1e-9 * (k + 1), ctypes.c_void_p(ms[k].data_ptr()),
+                                      ctypes.c_void_p(outs[k].data_ptr()), stream), "mt_rhs_noalloc")
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    for k in range(3):
+        _lib.check(lib.mt_rhs(s._h, 0.1e-9 * (k + 1), ctypes.c_void_p(ms[k].data_ptr()),
+                              ctypes.c_void_p(refs[k].data_ptr()), stream), "mt_rhs")
+    torch.cuda.synchronize()
+    for k in range(3):
+        r, g = refs[k].cpu().numpy(), outs[k].cpu().numpy()
         assert np.all(np.isfinite(g))
         np.testing.assert_allclose(g, r, rtol=1e-12, atol=1e-12 * np.abs(r).max())
 
