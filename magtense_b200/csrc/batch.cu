@@ -7,17 +7,17 @@
 // :1185-1587, step_r1 :1726-1978, stiff_r1 :1981-2367, interpolate_r1
 // :2655-2997, range_integrate_r1 :942-1183; driver ODE_Solvers.f90:124-237).
 // The control flow is written once, synchronously, as a coroutine: it yields
-// when it needs a right-hand side f(t, y) or a norm over all its cells.  The
-// kernel advances all instances in lock-step "ticks":
+// when it needs a right-hand side f(t, y); norms over all its cells resolve in
+// place (post_reduce: the instance's cell-block CTAs meet on a per-instance
+// arrival counter).  The kernel advances all instances in lock-step "ticks":
 //
-//   P2  resolve pending reductions, advance each instance to its next yield
-//   B1  grid barrier (stage arguments of all cells visible)
-//   G   demag product of every (cell block x instance block) tile -> partial H
+//   B1  grid barrier (stage arguments and requests of all cells visible)
+//   G   demag product of the requesting instances -> partial H
 //   Bh  grid barrier (partial H visible)
 //   P1  for instances that asked for f: sum the partials, apply the LL
 //       epilogue (exchange, anisotropy, Zeeman at the instance's own t,
-//       cross products) on the owned cells, advance to the next yield
-//   B2  grid barrier (reduction partials visible)
+//       cross products) on the owned cells, advance to the next request,
+//       publish the requests of the next tick
 //
 // Tile (cb, ib, s): receiver cells [128 cb, 128 cb + 128) for all three field
 // components, instances [64 ib, 64 ib + 64), source range split s of S.  The
@@ -251,30 +251,82 @@ MT_DEV double warp_red(double v, bool is_max)
     return is_max ? warp_max(v) : warp_sum(v);
 }
 
-// post a reduction of K values (per-lane partials v[]) for instance b
+// Reductions of K values over all cells of instance b.  Every cell-block CTA of the
+// instance runs the same coroutine and reaches the same reduction: post_reduce
+// writes the warp's partials to the slots of its cell block, counts the CTA in the
+// instance's arrival counter and yields (req 2); resolve_reduce, run by the caller
+// before it resumes the coroutine, waits (bounded) until all CB cell blocks have
+// arrived and combines the CB partials in cell-block order, so every copy of the
+// coroutine gets the same bits.  Slots alternate between two halves by the
+// reduction's parity: a CTA can post reduction r + 1 only after all have arrived at
+// r, and reduction r + 2 (same half) only after all have read r.  On a timeout the
+// launch aborts and the coroutine is left with req 5.
+MT_DEV double* red_slot(const BCtx& X, const BInst& I, int b)
+{
+    return X.F.partials + (size_t)(I.red_seq & 1) * X.Q.Bp * kRedSlots * X.Q.CB + (size_t)b * kRedSlots * X.Q.CB;
+}
+
 MT_DEV void post_reduce(const BCtx& X, BInst& I, int b, const double* v, int K, bool is_max)
 {
+    double* slot = red_slot(X, I, b);
     for (int k = 0; k < K; ++k) {
         const double r = warp_red(v[k], is_max);
-        if (X.lane == 0) X.F.partials[((size_t)b * kRedSlots + k) * X.Q.CB + X.cb] = r;
+        if (X.lane == 0) slot[(size_t)k * X.Q.CB + X.cb] = r;
+    }
+    if (X.lane == 0) {
+        __threadfence();
+        atomicAdd(&X.F.redcnt[b], 1u);
     }
     I.req = 2;
     I.red_k = K;
     I.red_max = is_max ? 1 : 0;
 }
 
+__device__ __noinline__ int wait_arrivals(unsigned* cnt, unsigned target, GridSync* gs, int lane)
+{
+    int ok = 1;
+    if (lane == 0) {
+        long long it = 0;
+        const uint64_t t0 = globaltimer_ns();
+        while ((int)(ld_acquire_u32(cnt) - target) < 0) {
+            if (ld_volatile_i32(&gs->abort)) { ok = 0; break; }
+            if (++it > kSpinLimit || ((it & 1023) == 0 && globaltimer_ns() - t0 > kTimeoutNs)) {
+                if (atomicCAS(&gs->err, 0, KERR_BARRIER_TIMEOUT) == 0) gs->err_where = 400;
+                atomicExch(&gs->abort, 1);
+                ok = 0;
+                break;
+            }
+            __nanosleep(20);
+        }
+    }
+    __syncwarp();
+    return __shfl_sync(0xffffffffu, ok, 0);
+}
+
 MT_DEV void resolve_reduce(const BCtx& X, BInst& I, int b)
 {
+    const unsigned target = (unsigned)X.Q.CB * (unsigned)(I.red_seq + 1);
+    const double* slot = red_slot(X, I, b);
+    I.red_seq++;
+    if (!wait_arrivals(&X.F.redcnt[b], target, X.F.gs, X.lane)) { I.req = 5; return; }
     for (int k = 0; k < I.red_k; ++k) {
         double r = 0.0;
         for (int c = 0; c < X.Q.CB; ++c) {
-            const double x = ldcg(&X.F.partials[((size_t)b * kRedSlots + k) * X.Q.CB + c]);
+            const double x = ldcg(&slot[(size_t)k * X.Q.CB + c]);
             r = (c == 0) ? x : (I.red_max ? fmax(r, x) : r + x);
         }
         I.red[k] = r;
     }
     I.req = 0;
 }
+
+// advance instance b to its next right-hand-side request, resolving its reductions
+// on the way (returns with req 1, 3 done, 4 parked or 5 aborting)
+#define ADVANCE_TO_REQUEST(X, I, b)                             \
+    do {                                                        \
+        advance(X, I, b);                                       \
+        if ((I).req == 2) resolve_reduce(X, I, b);              \
+    } while ((I).req == 0)
 
 // time-dependent scalars of instance b
 MT_DEV TimeScalars inst_scalars(const BCtx& X, int b, double t)
@@ -1142,6 +1194,37 @@ MT_DEV void gemm_tile_simt(const BCtx& X)
 
 constexpr int kMaxInstPerWarp = 8;
 
+// Publish the state of the warp's coroutines for tick tk: active instances and
+// right-hand-side requests (per 64-instance tile, and as request bits for the int8
+// packing), counted once per instance by its cell block 0.  Slot tk % 3 was cleared
+// by CTA 0 after the first barrier of tick tk - 1 (or by the host before the
+// launch), and is read after the first barrier of tick tk.
+MT_DEV void publish_requests(const BInst* L, int mine, const BCtx& X, int W, bool i8, long long tk)
+{
+    const BatchParams& Q = X.Q;
+    const BatchBufs& F = X.F;
+    int my_active = 0, my_rhs = 0;
+    int rhs_tile[2] = {0, 0};   // requests per 64-instance tile, tiles jb0 and jb0 + 1
+    for (int k = 0; k < mine; ++k) {
+        const int req = L[k].req;
+        const int b = X.i0 + X.warp + k * X.nwarps;
+        if (b >= Q.B) continue;
+        if (req != 3 && req != 4) my_active++;
+        if (req == 1) {
+            my_rhs++;
+            rhs_tile[(b / kI8N - X.i0 / kI8N) & 1]++;
+            if (i8 && X.cb == 0 && X.lane == 0) atomicOr(&F.reqbits[(tk % 3) * W + (b >> 5)], 1u << (b & 31));
+        }
+    }
+    if (X.lane == 0 && X.cb == 0 && (my_active | my_rhs)) {
+        unsigned* c = F.counters + 2 * (tk % 3);
+        atomicAdd(&c[0], (unsigned)my_active);
+        atomicAdd(&c[1], (unsigned)my_rhs);
+        for (int h = 0; h < 2; ++h)
+            if (rhs_tile[h]) atomicAdd(&F.ibreq[(tk % 3) * 2 * Q.IB + X.i0 / kI8N + h], (unsigned)rhs_tile[h]);
+    }
+}
+
 
 __global__ void __launch_bounds__(kBatchThreads, 1)
 batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMaps maps)
@@ -1193,6 +1276,7 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
         long long* dst = reinterpret_cast<long long*>(&L[mine]);
         for (int w = 0; w < (int)(sizeof(BInst) / 8); ++w) dst[w] = __ldcg(src + w);
         if (L[mine].req == 4) L[mine].req = 0;                 // parked by the previous launch
+        L[mine].red_seq = 0;                                   // the arrival counters start at zero
         L[mine].budget_mark = L[mine].s.full_f_count + L[mine].s.f_count + Q.evals_budget;
     }
     bool ok = true;
@@ -1249,39 +1333,28 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
     } while (0)
     long long ticks_run = 0;
     unsigned long long hist_ns[5] = {0, 0, 0, 0, 0}, hist_n[5] = {0, 0, 0, 0, 0};   // ticks by active tiles
-    for (long long tick = 0; tick < Q.ticks_per_launch && ok; ++tick) {
-        unsigned* ctr = F.counters + 2 * (tick % 3);
-        ticks_run++;
+    // Each tick: A advance every coroutine whose request was served (and, in the first
+    // tick of a launch, those starting or resumed after a budget stop) to its next
+    // request, resolving reductions on the way, and publish the requests; B1; the
+    // demag product of the requesting instances; Bh; the LL epilogue of those
+    // instances.  Requests still pending when a launch ends are served by the next.
+    for (long long tick = 0; ok; ++tick) {
         const uint64_t t_tick = prof ? globaltimer_ns() : 0;
-        // P2: resolve reductions, advance
-        int my_active = 0, my_rhs = 0;
-        int rhs_tile[2] = {0, 0};   // requests per 64-instance tile, tiles jb0 and jb0 + 1
         for (int k = 0; k < mine; ++k) {
             BInst& I = L[k];
             const int b = X.i0 + X.warp + k * X.nwarps;
-            if (b >= Q.B) continue;
-            if (I.req == 2) resolve_reduce(X, I, b);
-            if (I.req == 0) {
-                const uint64_t ta = (F.prof && t == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0;
-                advance(X, I, b);
-                if (ta) { atomicAdd(&F.prof[27], globaltimer_ns() - ta); atomicAdd(&F.prof[28], 1ull); }
-            }
-            if (I.req != 3 && I.req != 4) my_active++;
-            if (I.req == 1) {
-                my_rhs++;
-                rhs_tile[(b / kI8N - X.i0 / kI8N) & 1]++;
-                if (i8 && X.cb == 0 && X.lane == 0) atomicOr(&F.reqbits[(tick % 3) * W + (b >> 5)], 1u << (b & 31));
-            }
+            if (b >= Q.B || I.req != 0) continue;
+            const uint64_t ta = (F.prof && t == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0;
+            ADVANCE_TO_REQUEST(X, I, b);
+            if (ta) { atomicAdd(&F.prof[27], globaltimer_ns() - ta); atomicAdd(&F.prof[28], 1ull); }
         }
+        if (tick >= Q.ticks_per_launch) break;
+        publish_requests(L, mine, X, W, i8, tick);
         asm volatile("fence.proxy.async.global;" ::: "memory");   // operand stores -> TMA reads
-        if (X.lane == 0 && X.cb == 0 && (my_active | my_rhs)) {
-            atomicAdd(&ctr[0], (unsigned)my_active);
-            atomicAdd(&ctr[1], (unsigned)my_rhs);
-            for (int h = 0; h < 2; ++h)
-                if (rhs_tile[h]) atomicAdd(&F.ibreq[(tick % 3) * 2 * Q.IB + X.i0 / kI8N + h], (unsigned)rhs_tile[h]);
-        }
         __syncthreads();
-        PROF_MARK(0);
+        PROF_MARK(4);
+        unsigned* ctr = F.counters + 2 * (tick % 3);
+        ticks_run++;
         if (!grid_sync(F.gs, 1)) { ok = false; break; }
         PROF_MARK(1);
         const unsigned active = __ldcg(&ctr[0]);
@@ -1320,7 +1393,7 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
                 }
                 X.jb0 = first < (1 << 30) ? first / kI8N : 0;
             }
-            i8_fill_cover(X, s_cov);   // read in P1, after the barriers that follow the GEMM
+            i8_fill_cover(X, s_cov);   // read in the epilogue, after the barrier that follows the GEMM
             i8_pack(X, nr, s_bits, s_pre, W);
             asm volatile("fence.proxy.async.global;" ::: "memory");   // packed rows -> TMA reads
             __syncthreads();
@@ -1341,8 +1414,7 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
         if (!grid_sync(F.gs, 2)) { ok = false; break; }
         PROF_MARK(3);
         if (!ok) break;
-        // P1: LL epilogue of every requesting instance on the owned cells, spread
-        // over all threads, then each warp advances its instances
+        // LL epilogue of every requesting instance on the owned cells, spread over all threads
         for (int k = 0; k < mine; ++k) {
             const BInst& I = L[k];
             if (X.lane == 0) {
@@ -1362,20 +1434,9 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
             epilogue_cell(X, X.i0 + li, s_req[li].ts, s_req[li].arg, s_req[li].dst, X.c0 + cell);
         }
         __syncthreads();
+        for (int k = 0; k < mine; ++k)   // served: the next tick resumes these coroutines
+            if (L[k].req == 1 && X.i0 + X.warp + k * X.nwarps < Q.B) L[k].req = 0;
         PROF_MARK(6);
-        for (int k = 0; k < mine; ++k) {
-            BInst& I = L[k];
-            const int b = X.i0 + X.warp + k * X.nwarps;
-            if (b >= Q.B || I.req != 1) continue;
-            I.req = 0;
-            const uint64_t ta = (F.prof && t == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0;
-            advance(X, I, b);
-            if (ta) { atomicAdd(&F.prof[27], globaltimer_ns() - ta); atomicAdd(&F.prof[28], 1ull); }
-        }
-        __syncthreads();
-        PROF_MARK(4);
-        if (!grid_sync(F.gs, 3)) { ok = false; break; }
-        PROF_MARK(5);
         if (prof && i8) {
             const int k = X.nact < 4 ? X.nact : 4;
             hist_ns[k] += globaltimer_ns() - t_tick;

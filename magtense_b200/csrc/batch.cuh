@@ -24,6 +24,7 @@ struct BInst {
     int rhs_dst;       // destination vector id (see batch.cu)
     double t_rhs;
     int red_k, red_max;
+    int red_seq, red_pad;   // reductions completed in this launch (arrival-counter target)
     double red[kRedSlots];
     // locals of the synchronous formulation
     int i_stage, failed, phase3, ier, ntry, maybe, lots, sure, dst_slot, cf, flag, argi;
@@ -56,7 +57,8 @@ struct BatchBufs {
     unsigned* reqbits; // [3][Bp / 32] instances that request a right-hand side (int8 backend)
     float* hpart;      // [S][Bp][3][np] partial demag sums
     long long* part;   // [G][maxseg][64][128] exact int64 segment sums (int8 backend)
-    double* partials;  // [Bp][kRedSlots][CB] reduction partials
+    double* partials;  // [2][Bp][kRedSlots][CB] reduction partials (two halves by reduction parity)
+    unsigned* redcnt;  // [Bp] arrivals of the instance's cell-block CTAs at its reductions (zero per launch)
     BInst* inst;       // [CB][Bp] private coroutine copies
     GridSync* gs;
     unsigned* counters;  // [3][2]: active instances, right-hand-side requests

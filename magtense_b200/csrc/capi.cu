@@ -1039,6 +1039,9 @@ int mt_integrate_shards_local(mt_handle* const* hs, int world, const double* t, 
 // ---------------------------------------------------------------------------
 }  // extern "C"
 
+namespace { struct BatchRun; }
+static void batch_ws_free(mt_batch* bt);
+
 struct mt_batch {
     mt_handle* h = nullptr;
     int B = 0, prec = 0;
@@ -1057,6 +1060,10 @@ struct mt_batch {
     std::vector<double> alpha_tab;
     int solver = 2, renorm = 0;
     double gamma = 0.0;
+    // device workspace of the integrator (state vectors, operands, partial sums), kept
+    // between calls while the output count nt is unchanged
+    BatchRun* ws = nullptr;
+    int ws_nt = -1;
 };
 
 namespace {
@@ -1147,6 +1154,7 @@ int mt_batch_create(const mt_grid* g, int B, int precision, mt_batch** out)
 int mt_batch_destroy(mt_batch* bt)
 {
     if (!bt) return MT_OK;
+    batch_ws_free(bt);
     free_ptr(bt->khi); free_ptr(bt->row_inv); free_ptr(bt->hext); free_ptr(bt->alpha0);
     free_ptr(bt->klimb); free_ptr(bt->row_scale);
     mt_destroy(bt->h);
@@ -1236,64 +1244,97 @@ struct BatchRun {
     BatchBufs F;
     BatchParams Q;
     TcMaps maps;
+    double* comb = nullptr;   // merged output and convergence times, capacity comb_cap
+    int* cflags = nullptr;
+    size_t comb_cap = 0;
 };
 
-int batch_alloc(mt_batch* bt, BatchRun& R, int nt, cudaStream_t s)
+}  // namespace
+
+static void batch_ws_free(mt_batch* bt)
+{
+    delete bt->ws;   // frees the device buffers (cudaFree synchronises with the device)
+    bt->ws = nullptr;
+    bt->ws_nt = -1;
+}
+
+namespace {
+
+// The workspace of one integration (or demag) call: allocated on the first call and
+// kept in the handle while nt is unchanged; every call re-initialises it.
+int batch_alloc(mt_batch* bt, BatchRun*& Rp, int nt, cudaStream_t s)
 {
     mt_handle* h = bt->h;
     const int n = h->n;
     const int Bp = bt->IB * kInstBlock;
     const size_t n3 = 3 * (size_t)n;
+    const int RB0 = bt->Kd / 128, nks0 = bt->Kd / kI8KB;
+    const int maxseg0 = bt->prec == MT_PREC_INT8 ? batch_i8_maxseg(RB0, nks0, Bp / kI8N, bt->grid) : 0;
+    if (!bt->ws || bt->ws_nt != nt) {
+        batch_ws_free(bt);
+        std::unique_ptr<BatchRun> W(new BatchRun());
+        BatchRun& R = *W;
+        BatchBufs& F = R.F;
+        memset(&F, 0, sizeof(F));
+        CUDA_TRY(R.A.get(&F.pool, 4 * (size_t)Bp * n3));
+        CUDA_TRY(R.A.get(&F.deriv, 3 * (size_t)Bp * n3));
+        CUDA_TRY(R.A.get(&F.stg, 12 * (size_t)Bp * n3));
+        CUDA_TRY(R.A.get(&F.p, 6 * (size_t)Bp * n3));
+        CUDA_TRY(R.A.get(&F.errest, (size_t)Bp * n3));
+        CUDA_TRY(R.A.get(&F.weights, (size_t)Bp * n3));
+        CUDA_TRY(R.A.get(&F.ylast, (size_t)Bp * n3));
+        CUDA_TRY(R.A.get(&F.ystep, (size_t)Bp * n3));
+        if (nt > 0) {
+            CUDA_TRY(R.A.get(&F.t_out, (size_t)Bp * nt));
+            CUDA_TRY(R.A.get(&F.flags_out, (size_t)Bp * nt));
+        }
+        if (bt->prec == MT_PREC_FP32) {
+            CUDA_TRY(R.A.get(&F.m32, (size_t)Bp * 3 * h->ldk));
+        } else if (bt->prec == MT_PREC_INT8) {
+            CUDA_TRY(R.A.get(&F.mlimb, 4 * (size_t)Bp * bt->Kd));
+            CUDA_TRY(R.A.get(&F.mcomp, 4 * (size_t)Bp * bt->Kd));
+            CUDA_TRY(R.A.get(&F.reqbits, 3 * (size_t)(Bp / 32)));
+        } else {
+            CUDA_TRY(R.A.get(&F.mhi, (size_t)Bp * bt->Kd));
+            CUDA_TRY(R.A.get(&F.mlo, (size_t)Bp * bt->Kd));
+        }
+        if (bt->prec == MT_PREC_INT8)
+            CUDA_TRY(R.A.get(&F.part, (size_t)bt->grid * maxseg0 * kI8SlotElems));
+        else
+            CUDA_TRY(R.A.get(&F.hpart, (size_t)bt->S * Bp * 3 * bt->np));
+        CUDA_TRY(R.A.get(&F.partials, 2 * (size_t)Bp * kRedSlots * bt->CB));
+        CUDA_TRY(R.A.get(&F.redcnt, (size_t)Bp));
+        CUDA_TRY(R.A.get(&F.inst, (size_t)bt->CB * Bp));
+        CUDA_TRY(R.A.get(&F.gs, 1));
+        CUDA_TRY(R.A.get(&F.counters, 6));
+        CUDA_TRY(R.A.get(&F.ibreq, 6 * (size_t)bt->IB));
+        if (getenv("MT_BATCH_PROFILE")) CUDA_TRY(R.A.get(&F.prof, 48));
+        bt->ws = W.release();
+        bt->ws_nt = nt;
+    }
+    Rp = bt->ws;
+    BatchRun& R = *Rp;
     BatchBufs& F = R.F;
-    memset(&F, 0, sizeof(F));
-    CUDA_TRY(R.A.get(&F.pool, 4 * (size_t)Bp * n3));
-    CUDA_TRY(R.A.get(&F.deriv, 3 * (size_t)Bp * n3));
-    CUDA_TRY(R.A.get(&F.stg, 12 * (size_t)Bp * n3));
-    CUDA_TRY(R.A.get(&F.p, 6 * (size_t)Bp * n3));
-    CUDA_TRY(R.A.get(&F.errest, (size_t)Bp * n3));
-    CUDA_TRY(R.A.get(&F.weights, (size_t)Bp * n3));
-    CUDA_TRY(R.A.get(&F.ylast, (size_t)Bp * n3));
-    CUDA_TRY(R.A.get(&F.ystep, (size_t)Bp * n3));
+    F.y_out = nullptr;
     CUDA_TRY(cudaMemsetAsync(F.pool, 0, sizeof(double) * 4 * (size_t)Bp * n3, s));
     if (nt > 0) {
-        CUDA_TRY(R.A.get(&F.t_out, (size_t)Bp * nt));
-        CUDA_TRY(R.A.get(&F.flags_out, (size_t)Bp * nt));
         CUDA_TRY(cudaMemsetAsync(F.t_out, 0, sizeof(double) * Bp * nt, s));
         CUDA_TRY(cudaMemsetAsync(F.flags_out, 0, sizeof(int) * Bp * nt, s));
     }
-    if (bt->prec == MT_PREC_FP32) {
-        CUDA_TRY(R.A.get(&F.m32, (size_t)Bp * 3 * h->ldk));
-        CUDA_TRY(cudaMemsetAsync(F.m32, 0, sizeof(float) * Bp * 3 * (size_t)h->ldk, s));
-    } else if (bt->prec == MT_PREC_INT8) {
-        CUDA_TRY(R.A.get(&F.mlimb, 4 * (size_t)Bp * bt->Kd));
+    if (F.m32) CUDA_TRY(cudaMemsetAsync(F.m32, 0, sizeof(float) * Bp * 3 * (size_t)h->ldk, s));
+    if (F.mlimb) {
         CUDA_TRY(cudaMemsetAsync(F.mlimb, 0, 4 * (size_t)Bp * bt->Kd, s));
-        CUDA_TRY(R.A.get(&F.mcomp, 4 * (size_t)Bp * bt->Kd));
         CUDA_TRY(cudaMemsetAsync(F.mcomp, 0, 4 * (size_t)Bp * bt->Kd, s));
-        CUDA_TRY(R.A.get(&F.reqbits, 3 * (size_t)(Bp / 32)));
         CUDA_TRY(cudaMemsetAsync(F.reqbits, 0, sizeof(unsigned) * 3 * (Bp / 32), s));
-    } else {
-        CUDA_TRY(R.A.get(&F.mhi, (size_t)Bp * bt->Kd));
-        CUDA_TRY(R.A.get(&F.mlo, (size_t)Bp * bt->Kd));
+    }
+    if (F.mhi) {
         CUDA_TRY(cudaMemsetAsync(F.mhi, 0, 2 * (size_t)Bp * bt->Kd, s));
         CUDA_TRY(cudaMemsetAsync(F.mlo, 0, 2 * (size_t)Bp * bt->Kd, s));
     }
-    const int RB = bt->Kd / 128, nks = bt->Kd / kI8KB;
-    const int maxseg = bt->prec == MT_PREC_INT8 ? batch_i8_maxseg(RB, nks, Bp / kI8N, bt->grid) : 0;
-    if (bt->prec == MT_PREC_INT8)
-        CUDA_TRY(R.A.get(&F.part, (size_t)bt->grid * maxseg * kI8SlotElems));
-    else
-        CUDA_TRY(R.A.get(&F.hpart, (size_t)bt->S * Bp * 3 * bt->np));
-    CUDA_TRY(R.A.get(&F.partials, (size_t)Bp * kRedSlots * bt->CB));
-    CUDA_TRY(R.A.get(&F.inst, (size_t)bt->CB * Bp));
-    CUDA_TRY(R.A.get(&F.gs, 1));
-    CUDA_TRY(R.A.get(&F.counters, 6));
     CUDA_TRY(cudaMemsetAsync(F.counters, 0, sizeof(unsigned) * 6, s));
-    CUDA_TRY(R.A.get(&F.ibreq, 6 * (size_t)bt->IB));
     CUDA_TRY(cudaMemsetAsync(F.ibreq, 0, sizeof(unsigned) * 6 * bt->IB, s));
-    if (getenv("MT_BATCH_PROFILE")) {
-        CUDA_TRY(R.A.get(&F.prof, 48));
-        CUDA_TRY(cudaMemsetAsync(F.prof, 0, sizeof(unsigned long long) * 48, s));
-    }
+    if (F.prof) CUDA_TRY(cudaMemsetAsync(F.prof, 0, sizeof(unsigned long long) * 48, s));
+    const int RB = RB0, nks = nks0, maxseg = maxseg0;
     F.hext = bt->hext;
     F.alpha0 = bt->alpha0;
     BatchParams& Q = R.Q;
@@ -1330,8 +1371,9 @@ int mt_batch_demag_field(mt_batch* bt, const double* m_dev, double* H_dev, void*
     if (rc) return rc;
     if (bt->prec != MT_PREC_FP32 && !bt->khi && !bt->klimb) return fail(MT_ERR_STATE, "call mt_batch_assemble_demag first");
     cudaStream_t s = (cudaStream_t)stream;
-    BatchRun R;
-    if ((rc = batch_alloc(bt, R, 0, s))) return rc;
+    BatchRun* Rp = nullptr;
+    if ((rc = batch_alloc(bt, Rp, 0, s))) return rc;
+    BatchRun& R = *Rp;
     R.Q.demag_only = 1;
     R.Q.out_h = H_dev;
     CUDA_TRY(cudaMemsetAsync(R.F.gs, 0, sizeof(GridSync), s));
@@ -1386,24 +1428,28 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
         for (int q = 0; q < nt; ++q) if (t[q] == comb[k]) { cflags[k] |= 1; break; }
         for (int q = 0; q < nt_conv; ++q) if (t_conv[q] == comb[k]) { cflags[k] |= 2; break; }
     }
-    BatchRun R;
-    if ((rc = batch_alloc(bt, R, nt, s))) return rc;
+    BatchRun* Rp = nullptr;
+    if ((rc = batch_alloc(bt, Rp, nt, s))) return rc;
+    BatchRun& R = *Rp;
     BatchBufs& F = R.F;
     BatchParams& Q = R.Q;
     const int Bp = Q.Bp;
-    double* d_comb = nullptr; int* d_cflags = nullptr;
-    CUDA_TRY(R.A.get(&d_comb, comb.size()));
-    CUDA_TRY(R.A.get(&d_cflags, comb.size()));
+    if (comb.size() > R.comb_cap) {
+        CUDA_TRY(R.A.get(&R.comb, comb.size()));
+        CUDA_TRY(R.A.get(&R.cflags, comb.size()));
+        R.comb_cap = comb.size();
+    }
+    double* d_comb = R.comb;
+    int* d_cflags = R.cflags;
     CUDA_TRY(cudaMemcpyAsync(d_comb, comb.data(), sizeof(double) * comb.size(), cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaMemcpyAsync(d_cflags, cflags.data(), sizeof(int) * comb.size(), cudaMemcpyHostToDevice, s));
     F.y_out = y_out_dev;
     // y <- m0 (pool slot 0 of every instance), first sample, convergence reference
     CUDA_TRY(cudaMemcpyAsync(F.pool, m0_dev, sizeof(double) * (size_t)B * n3, cudaMemcpyDeviceToDevice, s));
     CUDA_TRY(cudaMemcpyAsync(F.ylast, m0_dev, sizeof(double) * (size_t)B * n3, cudaMemcpyDeviceToDevice, s));
-    if (y_out_dev)
-        for (int b = 0; b < B; ++b)
-            CUDA_TRY(cudaMemcpyAsync(y_out_dev + (size_t)b * nt * n3, m0_dev + (size_t)b * n3, sizeof(double) * n3,
-                                     cudaMemcpyDeviceToDevice, s));
+    if (y_out_dev)   // first sample of every instance: rows nt * 3n apart
+        CUDA_TRY(cudaMemcpy2DAsync(y_out_dev, sizeof(double) * nt * n3, m0_dev, sizeof(double) * n3,
+                                   sizeof(double) * n3, B, cudaMemcpyDeviceToDevice, s));
     std::vector<BInst> init((size_t)bt->CB * Bp);
     for (int cb = 0; cb < bt->CB; ++cb)
         for (int b = 0; b < Bp; ++b) {
@@ -1443,7 +1489,10 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
     float l2_hit = 0.f;
     size_t prev_limit = 0;
     bool limit_set = false;
-    if (bt->prec != MT_PREC_FP32 && !getenv("MT_NO_L2_PERSIST")) {
+    // Opt-in L2 residency of the split tensor (MT_L2_PERSIST=1).  Off by default: for the
+    // int8 tensor the per-instance FP64 state gains more from L2 than the tensor does
+    // (measured 57.9 against 55.6 simulated ns/s on the 256-instance film batch).
+    if (bt->prec != MT_PREC_FP32 && getenv("MT_L2_PERSIST")) {
         int max_persist = 0, max_win = 0;
         cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, h->device);
         cudaDeviceGetAttribute(&max_win, cudaDevAttrMaxAccessPolicyWindowSize, h->device);
@@ -1467,6 +1516,7 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
         CUDA_TRY(cudaMemsetAsync(F.gs, 0, sizeof(GridSync), s));
         CUDA_TRY(cudaMemsetAsync(F.counters, 0, sizeof(unsigned) * 6, s));
         CUDA_TRY(cudaMemsetAsync(F.ibreq, 0, sizeof(unsigned) * 6 * bt->IB, s));
+        CUDA_TRY(cudaMemsetAsync(F.redcnt, 0, sizeof(unsigned) * Q.Bp, s));
         if (F.reqbits) CUDA_TRY(cudaMemsetAsync(F.reqbits, 0, sizeof(unsigned) * 3 * (Q.Bp / 32), s));
         CUDA_TRY(cudaEventRecord(ev0, s));
         CUDA_TRY(launch_batch(P, F, Q, bt->grid, bt->prec != MT_PREC_FP32 ? &R.maps : nullptr, s,
@@ -1530,12 +1580,10 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
             fprintf(stderr, "\n");
         }
         const double tk = pr[7] ? (double)pr[7] : 1.0;
-        fprintf(stderr, "[batch profile] ticks %llu  per tick (us) at CTA 0: P2 %.2f B1 %.2f GEMM %.2f Bh %.2f "
-                "P1 epilogue %.2f advance %.2f B2 %.2f  busiest CTA: P2 %.2f (cta %llu) GEMM %.2f (cta %llu) "
-                "P1 advance %.2f (cta %llu)\n",
+        fprintf(stderr, "[batch profile] ticks %llu  per tick (us) at CTA 0: start %.2f B1 %.2f GEMM %.2f Bh %.2f "
+                "P1 epilogue %.2f advance+publish %.2f  busiest CTA: GEMM %.2f (cta %llu) P1 advance %.2f (cta %llu)\n",
                 pr[7], pr[0] / tk / 1e3, pr[1] / tk / 1e3, pr[2] / tk / 1e3, pr[3] / tk / 1e3, pr[6] / tk / 1e3,
-                pr[4] / tk / 1e3, pr[5] / tk / 1e3, pr[8] / tk / 1e3, pr[12], pr[9] / tk / 1e3, pr[13],
-                pr[10] / tk / 1e3, pr[14]);
+                pr[4] / tk / 1e3, pr[9] / tk / 1e3, pr[13], pr[10] / tk / 1e3, pr[14]);
         if (bt->prec == MT_PREC_INT8)
             fprintf(stderr, "[batch profile] int8 GEMM at CTA 0 per tick (us): roles done %.2f, total %.2f; MMA waits "
                     "full %.2f tfree %.2f; epilogue waits %.2f drains %.2f; producer waits %.2f; units %.1f segments %.2f\n",

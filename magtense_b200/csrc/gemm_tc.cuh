@@ -336,8 +336,9 @@ MT_DEV uint64_t sdesc_sw128(uint32_t saddr)
     return d;
 }
 constexpr int kI8SlotElems = 2 * kI8N * 128;                 // int64 per segment slot (hi and lo parts)
-// D S32 (2 at bit 4), A and B signed 8-bit (1 at bits 7 and 10), N = 64, M = 128
-constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | (((uint32_t)kI8N >> 3) << 17) | ((128u >> 4) << 24);
+// D S32 (2 at bit 4), A and B signed 8-bit (1 at bits 7 and 10), M = 128, N at bits 17-22 (N / 8)
+constexpr uint32_t idesc_i8(uint32_t n) { return (2u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24); }
+constexpr uint32_t kIdescI8 = idesc_i8(kI8N);
 
 static inline size_t tc_i8_smem_bytes() { return 1024 + (size_t)kI8Stages * kI8StageBytes + 256; }
 
@@ -400,11 +401,11 @@ MT_DEV void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int 
         : "memory");
 }
 
-MT_DEV void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate)
+MT_DEV void umma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate, uint32_t idesc = kIdescI8)
 {
     asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
                  " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
-                 "l"(adesc), "l"(bdesc), "r"(kIdescI8), "r"(accumulate)
+                 "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
                  : "memory");
 }
 
@@ -520,20 +521,24 @@ MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int
                 wait_full += globaltimer_ns() - tw;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t base = smem_u32(L.stages + (size_t)stg * kI8StageBytes);
+                // The four m-limb tiles of a stage lie back to back as one K-major operand of
+                // 4 x 64 rows (8-row groups 1024 bytes apart), and accumulator D_s sits at
+                // columns 64 s, so one MMA of K limb a against m limbs b0..b1 (N = 64 (b1 - b0 + 1))
+                // adds K_a m_b into D_{a+b} for every b at once.  Five MMAs per 32-wide k step
+                // cover the sixteen limb pairs: (0, 0..3) and (3, 1..3) open D0..D3 and D4..D6
+                // at the first k step of a segment, then (1, 0..3), (2, 0..3) and (3, 0).
+                const uint32_t bbase = base + kI8KLimbs * kI8ATile;
 #pragma unroll
                 for (int kk = 0; kk < kI8KB / 32; ++kk) {
-#pragma unroll
-                    for (int a = 0; a < kI8KLimbs; ++a) {
-                        const uint64_t ad = sdesc_sw128(base + a * kI8ATile + kk * 32);
-#pragma unroll
-                        for (int b = 0; b < kI8MLimbs; ++b) {
-                            const uint64_t bd = sdesc_sw128(base + kI8KLimbs * kI8ATile + b * kI8BTile + kk * 32);
-                            // the first product into each accumulator of the segment overwrites it:
-                            // (0,b) opens s = 0..3, (1,3), (2,3), (3,3) open s = 4, 5, 6
-                            const bool first = ks == ks0 && kk == 0 && (a == 0 || b == kI8MLimbs - 1);
-                            umma_i8(st.tmem + (uint32_t)((a + b) * kI8N), ad, bd, first ? 0u : 1u);
-                        }
-                    }
+                    const uint32_t open = (ks == ks0 && kk == 0) ? 0u : 1u;
+                    const uint64_t b0 = sdesc_sw128(bbase + kk * 32);
+                    const uint64_t b1 = sdesc_sw128(bbase + kI8BTile + kk * 32);
+                    umma_i8(st.tmem, sdesc_sw128(base + kk * 32), b0, open, idesc_i8(4 * kI8N));
+                    umma_i8(st.tmem + 4u * kI8N, sdesc_sw128(base + 3 * kI8ATile + kk * 32), b1, open,
+                            idesc_i8(3 * kI8N));
+                    umma_i8(st.tmem + 1u * kI8N, sdesc_sw128(base + 1 * kI8ATile + kk * 32), b0, 1u, idesc_i8(4 * kI8N));
+                    umma_i8(st.tmem + 2u * kI8N, sdesc_sw128(base + 2 * kI8ATile + kk * 32), b0, 1u, idesc_i8(4 * kI8N));
+                    umma_i8(st.tmem + 3u * kI8N, sdesc_sw128(base + 3 * kI8ATile + kk * 32), b0, 1u, idesc_i8(kI8N));
                 }
                 umma_commit(smem_u32(&L.empty[stg]));
             }
