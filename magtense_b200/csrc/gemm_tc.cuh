@@ -393,6 +393,23 @@ MT_DEV void tc_i8_init(unsigned char* smem, TcState& st)
     st.tiles = 0;
 }
 
+// the same with an L2 cache policy (createpolicy): the tensor limbs stream through L2
+// with evict_first, so they do not push the instances' state out of L2
+MT_DEV uint64_t l2_evict_first_policy()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+MT_DEV void tma_load_3d_hint(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar, uint64_t policy)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, {%2, %3, %4}], [%5], %6;" ::"r"(dst),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(bar), "l"(policy)
+        : "memory");
+}
+
 MT_DEV void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar)
 {
     asm volatile(
@@ -473,6 +490,7 @@ MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int
     if (warp == 4 && lane == 0) {
         long long g = st.kb_done;
         unsigned long long wait_empty = 0;
+        const uint64_t kpol = l2_evict_first_policy();
         for (long long u = u0; u < u1 && ok;) {
             const int t = (int)(u / nks), ks0 = (int)(u - (long long)t * nks);
             const long long ue = min(u1, (long long)(t + 1) * nks);
@@ -488,7 +506,7 @@ MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int
                 mbar_expect_tx(fb, (uint32_t)kI8StageBytes);
                 const int x = ks * kI8KB;
                 for (int a = 0; a < kI8KLimbs; ++a)
-                    tma_load_3d(smem_u32(base + a * kI8ATile), &maps.ahi, x, rb * 128, a, fb);
+                    tma_load_3d_hint(smem_u32(base + a * kI8ATile), &maps.ahi, x, rb * 128, a, fb, kpol);
                 for (int b = 0; b < kI8MLimbs; ++b)
                     tma_load_3d(smem_u32(base + kI8KLimbs * kI8ATile + b * kI8BTile), bmap, x, jb * kI8N, b, fb);
             }
