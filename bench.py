@@ -83,6 +83,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3, help="end-to-end repetitions (median reported)")
     ap.add_argument("--no-fp64", action="store_true", help="film-batch: skip the FP64 error statement")
     ap.add_argument("--no-large", action="store_true", help="film-batch: skip the large-plain sub-record")
+    ap.add_argument("--no-tune", action="store_true", help="film-batch: keep the default GEMM schedule")
     ap.add_argument("--shards", type=int, default=1,
                     help="large-plain: row shards of the one instance (over the ranks when --gpus > 1)")
     ap.add_argument("--res", type=int, nargs=3, default=None,
@@ -489,6 +490,9 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
     hext[:, :, 1:] = fields[:, None, :]
     bs = BatchSolver(res, L, B, precision=args.precision)
     bs.assemble()
+    t0 = time.perf_counter()
+    sched = bs.tune() if not args.no_tune else bs.schedule()
+    tune_s = time.perf_counter() - t0
     bs.set_dynamics(hext=hext, alpha=GAMMA * 0.02, gamma=GAMMA)
     m0 = m_s.unsqueeze(0).expand(B, -1).contiguous()
     m0_host = m0.cpu().numpy()
@@ -566,6 +570,10 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
                                      "note": f"single-instance FP32 path (the reference's arithmetic) on {len(pick)} "
                                              f"seeded instances of the same set, {window} ns each, one after another"},
         "batched_over_plain": value / ws / plain_rate,
+        "gemm_schedule": {"tuned": not args.no_tune, "tuning_s": round(tune_s, 3),
+                          "per_active_tiles": [{"tiles": k, "streamk_ctas": g, "order": o} for k, g, o in sched],
+                          "note": "autotuned Stream-K schedule of the int8 product (mt_batch_tune), set up before "
+                                  "timing"} if args.precision == "int8" else None,
         "gpu_launches": int(launches),
         "rhs_evals_per_s": evals / (sum(times) / 1e3) * ws,
         "clocks": clocks,

@@ -238,6 +238,20 @@ int mt_batch_set_dynamics(mt_batch* b, int solver, double gamma, const double* a
  * mt_batch_set_dynamics */
 int mt_batch_set_alpha_table(mt_batch* b, const double* alpha_tab, int nt_alpha);
 int mt_batch_assemble_demag(mt_batch* b, void* stream);
+/* Autotuner of the int8 product's GEMM schedule (no counterpart in the reference,
+ * whose product is an MKL/cuBLAS SGEMV, LandauLifshitzEquationSolver.f90:718-747):
+ * for every count of active 64-instance tiles, times the candidate schedules on the
+ * device (Stream-K CTA count, tile-major or row-major unit order) and keeps the
+ * fastest for the integrations of this handle; cached per device and geometry for
+ * the process.  Every schedule gives the same bits.  A no-op for the other
+ * precisions.  Needs the assembled tensor. */
+int mt_batch_tune(mt_batch* b, void* stream);
+/* the schedule in use: per active tile count k = 1..n_tiles, ctas[k-1] and order[k-1]
+ * (0 tile-major, 1 row-major); fills at most max_tiles entries */
+int mt_batch_get_schedule(mt_batch* b, int* ctas, int* order, int max_tiles, int* n_tiles);
+/* set the schedule by hand (n_tiles entries; CTA counts from two thirds of the SMs up
+ * to all of them, order 0 or 1), for example to replay a tuned one */
+int mt_batch_set_schedule(mt_batch* b, const int* ctas, const int* order, int n_tiles);
 /* m0_dev: B*3n FP64; y_out_dev: B*nt*3n FP64 or NULL; t_out, flags: B*nt host;
  * stats: B entries (kernel_ms/launches of the whole batch in stats[0]). */
 int mt_batch_integrate(mt_batch* b, const double* t, int nt, const double* m0_dev, double tol, double thres,

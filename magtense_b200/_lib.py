@@ -84,6 +84,9 @@ SIGNATURES = {
     "mt_batch_set_material": [VP, C.c_double, D, D, D],
     "mt_batch_set_dynamics": [VP, C.c_int, C.c_double, D, D, C.c_int, C.c_int],
     "mt_batch_set_alpha_table": [VP, D, C.c_int],
+    "mt_batch_tune": [VP, VP],
+    "mt_batch_get_schedule": [VP, I, I, C.c_int, I],
+    "mt_batch_set_schedule": [VP, I, I, C.c_int],
     "mt_batch_assemble_demag": [VP, VP],
     "mt_batch_integrate": [VP, D, C.c_int, VP, C.c_double, C.c_double, D, C.c_int, C.c_double, D, VP, I,
                            C.POINTER(Stats), VP],

@@ -59,6 +59,7 @@ struct BCtx {
     bool packed;            // instances sit at their compact positions (integration) or at b (demag only)
     const unsigned* bits;   // [Bp / 32] request bits of this tick (packed)
     const int* pre;         // [Bp / 32] requests before each word (packed)
+    int sched;              // Stream-K schedule word of this tick's GEMM
 };
 
 // compact position of requesting instance b: requests with a smaller index
@@ -101,8 +102,8 @@ MT_DEV void split_store(float f, int prec, uint16_t* hi_out, uint16_t* lo_out)
 // own elements of one instance, lane-strided: component a, cell i, index q = a*n + i
 #define FOR_OWN_W(X, q)                                                                       \
     for (int _e = (X).lane; _e < 3 * (X).nc; _e += 32)                                        \
-        if ([[maybe_unused]] const int _a = _e / (X).nc, _i = (X).c0 + (_e - _a * (X).nc),   \
-                      q = _a * (X).P.n + _i; true)
+        if ([[maybe_unused]] const int _a = (_e >= (X).nc) + (_e >= 2 * (X).nc),              \
+                      _i = (X).c0 + (_e - _a * (X).nc), q = _a * (X).P.n + _i; true)
 
 // int8 limbs of one source value: mq = rint(v 2^30) = m0 2^24 + m1 2^16 + m2 2^8 + m3
 // (signed digits, m3 lowest).  |v| must stay below 1.96 so that m0 fits; a value
@@ -117,7 +118,9 @@ MT_DEV void i8_store_m(double v, int8_t* dst, size_t limb_stride, GridSync* gs)
         atomicExch(&gs->abort, 1);
         v = 0.0;
     }
-    long long x = __double2ll_rn(v * kI8MScale);
+    // |v| <= 1.96, so rint(v 2^30) fits in 32 bits; x - dl is a multiple of 256 and the
+    // arithmetic shift divides it exactly
+    int x = __double2int_rn(v * kI8MScale);
     int8_t d[4];
 #pragma unroll
     for (int l = 3; l >= 1; --l) {
@@ -135,7 +138,7 @@ MT_DEV void put_arg(const BCtx& X, int argi, int b, int q, double v)
 {
     VPOOL(X, argi, b)[q] = v;
     const int n = X.P.n;
-    const int a = q / n, i = q - a * n;
+    const int a = (q >= n) + (q >= 2 * n), i = q - a * n;   // q < 3n
     const float f = (float)v;
     if (X.Q.prec == kPrecI8) {
         i8_store_m(v, X.F.mlimb + (size_t)b * X.Q.Kd + (size_t)a * X.Q.np + i, (size_t)X.Q.Bp * X.Q.Kd, X.F.gs);
@@ -177,7 +180,7 @@ MT_DEV ArgDst arg_dst(const BCtx& X, int argi, int b)
 MT_DEV void put_arg_d(const ArgDst& d, int q, double v)
 {
     d.pool[q] = v;
-    const int a = q / d.n, i = q - a * d.n;
+    const int a = (q >= d.n) + (q >= 2 * d.n), i = q - a * d.n;   // q < 3n
     if (d.prec == kPrecI8) {
         i8_store_m(v, d.mlimb + (size_t)a * d.np + i, d.limb_stride, d.gs);
     } else if (d.prec == kPrecFP32) {
@@ -210,7 +213,7 @@ __device__ __noinline__ double stage_args(int i, const double* __restrict__ y, c
             const int e = e0 + 32 * u;
             on[u] = e < tot;
             const int ee = on[u] ? e : e0;
-            const int a = ee / nc;
+            const int a = (ee >= nc) + (ee >= 2 * nc);   // ee < 3 nc
             q[u] = a * n + c0 + (ee - a * nc);
 #pragma unroll
             for (int j = 2; j <= 7; ++j) kv[u][j] = (j <= i - 1) ? ldcg(&st.s[j][q[u]]) : 0.0;
@@ -1049,8 +1052,8 @@ MT_DEV void i8_fill_cover(BCtx& X, SkCover* cov)
         SkCover cv = {0, -1, 0};
         const int pos = X.packed ? (jb < X.nact ? jb : -1) : (jb < 2 * X.Q.IB ? X.act_pos[jb] : -1);
         if (pos >= 0) {
-            const long long t = (long long)pos * X.Q.RB + (a * X.Q.np + X.c0) / 128;
-            cv = sk_cover(t, X.Q.nks, X.U);
+            const long long t = sk_tile(sk_sched_order(X.sched), pos, (a * X.Q.np + X.c0) / 128, X.nact, X.Q.RB);
+            cv = sk_cover(t, X.Q.nks, X.U, sk_sched_ctas(X.sched));
         }
         cov[k] = cv;
     }
@@ -1252,6 +1255,7 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
     X.jb0 = X.i0 / kI8N;
     X.cov = s_cov;
     X.packed = false;
+    X.sched = 0;
     X.bits = s_bits;
     X.pre = s_pre;
     const int W = Q.Bp / 32;
@@ -1286,10 +1290,15 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
             const int JB = Q.Bp / kI8N;
             for (int k = threadIdx.x; k < JB; k += blockDim.x) { s_act[k] = k; s_actpos[k] = k; }
             __syncthreads();
-            X.nact = JB;
-            X.U = (long long)JB * Q.RB * Q.nks;
-            i8_fill_cover(X, s_cov);
-            ok = tc_i8_streamk(X.smem, F, F.part, Q.maxseg, maps, &maps.bhi, X.nact, s_act, Q.RB, Q.nks, tcs);
+            X.nact = Q.tune_nact > 0 ? Q.tune_nact : JB;
+            X.U = (long long)X.nact * Q.RB * Q.nks;
+            X.sched = Q.tune_sched ? Q.tune_sched : Q.sk_sched[X.nact];
+            if (Q.tune_nact == 0) i8_fill_cover(X, s_cov);
+            ok = tc_i8_streamk(X.smem, F, F.part, Q.maxseg, maps, &maps.bhi, X.nact, s_act, Q.RB, Q.nks, X.sched, tcs);
+            if (Q.tune_nact > 0) {   // schedule timing: the product only
+                tc_finish_impl(X.smem, tcs);
+                return;
+            }
         } else if (!tc) {
             gemm_tile_simt(X);
         } else {
@@ -1384,6 +1393,7 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
             X.packed = true;
             X.nact = (nr + kI8N - 1) / kI8N;
             X.U = (long long)X.nact * Q.RB * Q.nks;
+            X.sched = Q.sk_sched[X.nact];
             // first compact position among this CTA's requesting instances
             {
                 int first = 1 << 30;
@@ -1401,7 +1411,7 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
             for (int k = threadIdx.x; k < X.nact; k += blockDim.x) s_act[k] = k;
             __syncthreads();
             if (X.nact > 0 && !tc_i8_streamk(X.smem, F, F.part, Q.maxseg, maps, &maps.blo, X.nact, s_act, Q.RB, Q.nks,
-                                             tcs))
+                                             X.sched, tcs))
                 ok = false;
         } else if (nreq > 0) {
             if (!tc) gemm_tile_simt(X);

@@ -87,6 +87,11 @@ struct BatchParams {
     // int8 backend: Stream-K geometry and the per-row scale 2^(-30 - e_r)
     int RB, nks, maxseg;
     const double* row_scale;  // [3np]
+    // Stream-K schedule word (CTA count, unit order) per active tile count 0..2 kMaxIB,
+    // picked by the autotuner (mt_batch_tune) or the default (all CTAs, tile-major)
+    int sk_sched[2 * kMaxIB + 1];
+    int tune_nact;            // > 0: demag_only times the product over this many tiles with tune_sched
+    int tune_sched;
 };
 
 cudaError_t batch_upload_tables();

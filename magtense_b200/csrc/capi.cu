@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 #include <memory>
+#include <map>
 
 #include "../../include/magtense_b200.h"
 #include "common.cuh"
@@ -1064,6 +1065,9 @@ struct mt_batch {
     // between calls while the output count nt is unchanged
     BatchRun* ws = nullptr;
     int ws_nt = -1;
+    // int8 GEMM schedule word per active tile count (autotuned by mt_batch_tune)
+    std::vector<int> sched;
+    bool tuned = false;
 };
 
 namespace {
@@ -1142,6 +1146,7 @@ int mt_batch_create(const mt_grid* g, int B, int precision, mt_batch** out)
     bt->grid = batch_grid(h->n, B, h->num_sms, precision, &bt->CB, &bt->IB, &bt->S);
     bt->np = bt->CB * kCellBlock;
     bt->Kd = 3 * bt->np;
+    bt->sched.assign(2 * kMaxIB + 1, bt->grid);   // all CTAs, tile-major
     if (precision == MT_PREC_INT8 && bt->Kd > 32000) {
         // D_s sums up to four limb products of magnitude <= 2^14 over the k range in int32
         mt_batch_destroy(bt);
@@ -1260,6 +1265,9 @@ static void batch_ws_free(mt_batch* bt)
 
 namespace {
 
+// smallest Stream-K CTA count the autotuner tries (the slot storage is sized for it)
+int sk_min_ctas(int grid) { return std::max(1, (2 * grid) / 3); }
+
 // The workspace of one integration (or demag) call: allocated on the first call and
 // kept in the handle while nt is unchanged; every call re-initialises it.
 int batch_alloc(mt_batch* bt, BatchRun*& Rp, int nt, cudaStream_t s)
@@ -1269,7 +1277,7 @@ int batch_alloc(mt_batch* bt, BatchRun*& Rp, int nt, cudaStream_t s)
     const int Bp = bt->IB * kInstBlock;
     const size_t n3 = 3 * (size_t)n;
     const int RB0 = bt->Kd / 128, nks0 = bt->Kd / kI8KB;
-    const int maxseg0 = bt->prec == MT_PREC_INT8 ? batch_i8_maxseg(RB0, nks0, Bp / kI8N, bt->grid) : 0;
+    const int maxseg0 = bt->prec == MT_PREC_INT8 ? batch_i8_maxseg(RB0, nks0, Bp / kI8N, sk_min_ctas(bt->grid)) : 0;
     if (!bt->ws || bt->ws_nt != nt) {
         batch_ws_free(bt);
         std::unique_ptr<BatchRun> W(new BatchRun());
@@ -1343,6 +1351,7 @@ int batch_alloc(mt_batch* bt, BatchRun*& Rp, int nt, cudaStream_t s)
     Q.nt = nt; Q.nt_hext = bt->nt_hext; Q.prec = bt->prec;
     Q.khi = bt->khi; Q.klo = bt->klo; Q.row_inv = bt->row_inv;
     Q.RB = RB; Q.nks = nks; Q.maxseg = maxseg; Q.row_scale = bt->row_scale;
+    for (int k = 0; k <= 2 * kMaxIB; ++k) Q.sk_sched[k] = bt->sched[k];
     Q.renorm = h->renorm;
     memset(&R.maps, 0, sizeof(R.maps));
     if (bt->prec == MT_PREC_INT8) {
@@ -1363,6 +1372,109 @@ int batch_alloc(mt_batch* bt, BatchRun*& Rp, int nt, cudaStream_t s)
 }  // namespace
 
 extern "C" {
+
+// Autotuner of the int8 Stream-K GEMM.  For every count of active 64-instance tiles,
+// times the product alone (one launch of the batch kernel in schedule-timing mode,
+// CUDA events, best of three after a warm-up) for each candidate schedule: Stream-K CTA
+// counts from all SMs down to two thirds of them in steps of 8, in tile-major and
+// row-major unit order; keeps the fastest.  The exact product gives the same bits
+// under every schedule.  Results are kept per device, grid and batch size for the
+// life of the process.
+namespace {
+std::mutex g_tune_mu;
+std::map<std::string, std::vector<int>> g_tune_cache;
+}
+
+int mt_batch_tune(mt_batch* bt, void* stream)
+{
+    if (!bt) return fail(MT_ERR_ARG, "null handle");
+    if (bt->prec != MT_PREC_INT8) return MT_OK;   // the other precisions run fixed tiles
+    if (!bt->klimb) return fail(MT_ERR_STATE, "call mt_batch_assemble_demag first");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int JB = (bt->IB * kInstBlock) / kI8N;
+    char key[128];
+    snprintf(key, sizeof(key), "dev%d sms%d n%d Kd%d Bp%d grid%d", bt->h->device, bt->h->num_sms, bt->h->n, bt->Kd,
+             bt->IB * kInstBlock, bt->grid);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) { bt->sched = it->second; bt->tuned = true; return MT_OK; }
+    }
+    BatchRun* Rp = nullptr;
+    int rc = batch_alloc(bt, Rp, 0, s);
+    if (rc) return rc;
+    BatchRun& R = *Rp;
+    DevProb P = batch_prob(bt);
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    CUDA_TRY(cudaEventCreate(&ev0));
+    CUDA_TRY(cudaEventCreate(&ev1));
+    struct EvGuard { cudaEvent_t a, b; ~EvGuard() { cudaEventDestroy(a); cudaEventDestroy(b); } } evg{ev0, ev1};
+    std::vector<int> cands;
+    for (int G = bt->grid; G >= sk_min_ctas(bt->grid); G -= 8) cands.push_back(G);
+    std::vector<int> sched(2 * kMaxIB + 1, bt->grid);
+    R.Q.demag_only = 1;
+    for (int nact = 1; nact <= JB; ++nact) {
+        float best = 1e30f;
+        int best_w = bt->grid;
+        for (int order = 0; order < 2; ++order)
+            for (int G : cands) {
+                const int w = G | (order << 16);
+                R.Q.tune_nact = nact;
+                R.Q.tune_sched = w;
+                float t_min = 1e30f;
+                for (int rep = 0; rep < 4; ++rep) {
+                    CUDA_TRY(cudaMemsetAsync(R.F.gs, 0, sizeof(GridSync), s));
+                    CUDA_TRY(cudaEventRecord(ev0, s));
+                    CUDA_TRY(launch_batch(P, R.F, R.Q, bt->grid, &R.maps, s));
+                    CUDA_TRY(cudaEventRecord(ev1, s));
+                    CUDA_TRY(cudaEventSynchronize(ev1));
+                    float ms = 0.f;
+                    CUDA_TRY(cudaEventElapsedTime(&ms, ev0, ev1));
+                    if (rep > 0) t_min = std::min(t_min, ms);
+                }
+                GridSync gs_h;
+                CUDA_TRY(cudaMemcpy(&gs_h, R.F.gs, sizeof(gs_h), cudaMemcpyDeviceToHost));
+                if (gs_h.err || gs_h.abort)
+                    return fail(MT_ERR_TIMEOUT, "schedule timing: bounded wait gave up (at %d)", gs_h.err_where);
+                if (t_min < best) { best = t_min; best_w = w; }
+            }
+        sched[nact] = best_w;
+    }
+    bt->sched = sched;
+    bt->tuned = true;
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache[key] = sched;
+    return MT_OK;
+}
+
+int mt_batch_set_schedule(mt_batch* bt, const int* ctas, const int* order, int n_tiles)
+{
+    if (!bt || !ctas || !order) return fail(MT_ERR_ARG, "bad argument");
+    const int JB = (bt->IB * kInstBlock) / kI8N;
+    if (n_tiles != JB) return fail(MT_ERR_ARG, "need one entry per tile count (%d)", JB);
+    std::vector<int> sched(2 * kMaxIB + 1, bt->grid);
+    for (int k = 1; k <= JB; ++k) {
+        const int G = ctas[k - 1], o = order[k - 1];
+        if (G < sk_min_ctas(bt->grid) || G > bt->grid || (o != 0 && o != 1))
+            return fail(MT_ERR_ARG, "schedule %d: %d CTAs (allowed %d..%d), order %d", k, G, sk_min_ctas(bt->grid),
+                        bt->grid, o);
+        sched[k] = G | (o << 16);
+    }
+    bt->sched = sched;
+    return MT_OK;
+}
+
+int mt_batch_get_schedule(mt_batch* bt, int* ctas, int* order, int max_tiles, int* n_tiles)
+{
+    if (!bt || !n_tiles) return fail(MT_ERR_ARG, "bad argument");
+    const int JB = (bt->IB * kInstBlock) / kI8N;
+    *n_tiles = JB;
+    for (int k = 1; k <= JB && k <= max_tiles; ++k) {
+        if (ctas) ctas[k - 1] = bt->sched[k] & 0xffff;
+        if (order) order[k - 1] = (bt->sched[k] >> 16) & 1;
+    }
+    return MT_OK;
+}
 
 int mt_batch_demag_field(mt_batch* bt, const double* m_dev, double* H_dev, void* stream)
 {

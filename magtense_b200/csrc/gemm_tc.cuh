@@ -439,19 +439,40 @@ MT_DEV void mbar_arrive(uint32_t bar)
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-// Stream-K over U units on G = min(gridDim.x, U) CTAs (every range non-empty):
-// CTA c owns units [sk_start(c), sk_start(c + 1))
-MT_DEV long long sk_ctas(long long U) { return U < (long long)gridDim.x ? U : (long long)gridDim.x; }
+// Stream-K over U units on G = min(Gsel, U) CTAs (every range non-empty):
+// CTA c owns units [sk_start(c), sk_start(c + 1)).  Gsel (at most gridDim.x) and the
+// unit order come from the schedule the autotuner picked for the active tile count.
+MT_DEV long long sk_ctas(long long U, long long Gsel) { return U < Gsel ? U : Gsel; }
 MT_DEV long long sk_start(long long c, long long U, long long G) { return c * U / G; }
+
+// Schedule word: Stream-K CTA count in the low 16 bits, unit order in bit 16
+// (0: tile-major, the units of one 64-instance tile and row block after another;
+// 1: row-major, the active tiles of one row block after another, so a row block of
+// the tensor is read for all active tiles close together in time).
+constexpr int kSkOrderBit = 16;
+MT_DEV int sk_sched_ctas(int w) { return w & 0xffff; }
+MT_DEV int sk_sched_order(int w) { return (w >> kSkOrderBit) & 1; }
+
+// "tile" index tt of (active position pos, row block rb) in the unit order; unit u
+// belongs to tile tt = u / nks
+MT_DEV long long sk_tile(int order, int pos, int rb, int nact, int RB)
+{
+    return order ? (long long)rb * nact + pos : (long long)pos * RB + rb;
+}
+MT_DEV void sk_tile_coords(int order, long long tt, int nact, int RB, int* pos, int* rb)
+{
+    if (order) { *rb = (int)(tt / nact); *pos = (int)(tt - (long long)*rb * nact); }
+    else { *pos = (int)(tt / RB); *rb = (int)(tt - (long long)*pos * RB); }
+}
 
 // The CTAs whose ranges touch tile t (units [t nks, (t+1) nks)) are first..last;
 // the tile is the jf-th segment of CTA first and the first segment (slot 0) of
 // every later one, because their ranges start inside it.
 struct SkCover { int first, last, jf; };
 
-MT_DEV SkCover sk_cover(long long t, long long nks, long long U)
+MT_DEV SkCover sk_cover(long long t, long long nks, long long U, long long Gsel)
 {
-    const long long G = sk_ctas(U);
+    const long long G = sk_ctas(U, Gsel);
     const long long x0 = t * nks, x1 = (t + 1) * nks;
     long long f = ((x0 + 1) * G + U - 1) / U - 1;
     long long l = (x1 * G + U - 1) / U - 1;
@@ -476,12 +497,14 @@ MT_DEV void i8_prof_add(unsigned long long* prof, int slot, unsigned long long v
 // part: int64 slots [gridDim.x][maxseg][64][128].  Returns a CTA-uniform ok flag.
 template <typename FT>
 MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int maxseg, const TcMaps& maps,
-                          const CUtensorMap* bmap, int nact, const int* act_jb, int RB, int nks, TcState& st)
+                          const CUtensorMap* bmap, int nact, const int* act_jb, int RB, int nks, int sched,
+                          TcState& st)
 {
     I8Smem L = i8_layout(smem);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long U = (long long)nact * RB * nks;
-    const long long G = sk_ctas(U), c = blockIdx.x;
+    const int order = sk_sched_order(sched);
+    const long long G = sk_ctas(U, sk_sched_ctas(sched)), c = blockIdx.x;
     bool ok = true;
     if (c >= G) return __syncthreads_and(1) != 0;
     const long long u0 = sk_start(c, U, G), u1 = sk_start(c + 1, U, G);
@@ -494,7 +517,9 @@ MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int
         for (long long u = u0; u < u1 && ok;) {
             const int t = (int)(u / nks), ks0 = (int)(u - (long long)t * nks);
             const long long ue = min(u1, (long long)(t + 1) * nks);
-            const int rb = t % RB, jb = act_jb[t / RB];
+            int pos, rb;
+            sk_tile_coords(order, t, nact, RB, &pos, &rb);
+            const int jb = act_jb[pos];
             for (int ks = ks0; ks < ks0 + (int)(ue - u); ++ks, ++g) {
                 const int stg = (int)(g % kI8Stages);
                 const uint32_t ph = (uint32_t)((g / kI8Stages) & 1);

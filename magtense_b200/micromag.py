@@ -285,6 +285,7 @@ class MicromagProblem:
         stats = []
         try:
             bs.assemble()
+            bs.tune()
             t = np.linspace(0, t_end, nt)
             m_cur = m0s
             for k, hk in enumerate(rows):

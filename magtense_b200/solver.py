@@ -361,6 +361,30 @@ class BatchSolver:
                                                he.ctypes.data_as(_lib.D), he.shape[1], int(bool(renormalize))),
               "mt_batch_set_dynamics")
 
+    def tune(self, stream=None):
+        """Autotune the int8 GEMM schedule (Stream-K CTA count and unit order per count of
+        active 64-instance tiles) by timing the candidates on the device; the result is
+        kept for this handle and cached for the process.  A no-op for other precisions."""
+        with torch.cuda.device(self.device):
+            check(_lib.lib().mt_batch_tune(self._h, _stream(stream)), "mt_batch_tune")
+        return self.schedule()
+
+    def schedule(self):
+        """[(active tiles, Stream-K CTAs, "tile-major" | "row-major"), ...] in use."""
+        cap = 2 * 64
+        ctas = (C.c_int * cap)()
+        order = (C.c_int * cap)()
+        nt = C.c_int()
+        check(_lib.lib().mt_batch_get_schedule(self._h, ctas, order, cap, C.byref(nt)), "mt_batch_get_schedule")
+        return [(k + 1, int(ctas[k]), "row-major" if order[k] else "tile-major") for k in range(min(nt.value, cap))]
+
+    def set_schedule(self, entries):
+        """Set the schedule by hand: one (ctas, order 0|1) per active tile count 1..n_tiles."""
+        n = len(entries)
+        ctas = (C.c_int * n)(*[int(c) for c, _ in entries])
+        order = (C.c_int * n)(*[int(o) for _, o in entries])
+        check(_lib.lib().mt_batch_set_schedule(self._h, ctas, order, n), "mt_batch_set_schedule")
+
     def demag_field(self, m, stream=None):
         m = torch.as_tensor(m, dtype=torch.float64, device=self.device).reshape(self.B, 3 * self.n).contiguous()
         out = torch.empty_like(m)

@@ -190,3 +190,37 @@ def test_std_prob_4_dataset_sequences_match_oracle(torch_cuda, oracle, tmp_path)
         assert np.array_equal(seq[b], want), b
     out = D.write_database(tmp_path / "db", seq, fields, (0, 3))
     assert out.exists()
+
+
+def test_gemm_schedules_are_bit_exact_and_tuned(torch_cuda, oracle):
+    """The autotuner's candidate schedules of the int8 product (Stream-K CTA count from
+    all SMs down to two thirds of them, tile-major or row-major unit order) all give
+    the same bits, equal to oracle mode 2; the tuned schedule is one of them."""
+    from magtense_b200 import BatchSolver, MTError
+    res, L = [24, 8, 2], [120e-9, 40e-9, 10e-9]
+    n, B = 384, 192
+    m = unit_states(n, B, 17, tilt=1.0).reshape(B, -1)
+    bs = BatchSolver(res, L, B, precision="int8")
+    bs.assemble()
+    mt = torch_cuda.as_tensor(m, device="cuda")
+    H0 = bs.demag_field(mt).cpu().numpy().reshape(B, -1)
+    tiles = len(bs.schedule())
+    sms = torch_cuda.cuda.get_device_properties(0).multi_processor_count
+    lo = max(1, 2 * sms // 3)
+    for G, order in [(sms, 0), (sms, 1), (lo, 0), (lo, 1), (sms - 8, 1), (lo + 5, 0)]:
+        bs.set_schedule([(G, order)] * tiles)
+        H = bs.demag_field(mt).cpu().numpy().reshape(B, -1)
+        assert np.array_equal(H, H0), (G, order)
+    with pytest.raises(MTError):
+        bs.set_schedule([(lo - 1, 0)] * tiles)
+    sched = bs.tune()
+    assert len(sched) == tiles
+    for k, G, order in sched:
+        assert lo <= G <= sms and order in ("tile-major", "row-major")
+    H = bs.demag_field(mt).cpu().numpy().reshape(B, -1)
+    assert np.array_equal(H, H0)
+    P2 = oracle.Problem(res, L, mode=2, K32=device_tensor(res, L))
+    for b in (0, 77, 191):
+        Hm = P2.fields(0.0, m[b])[3].reshape(-1)
+        assert np.array_equal(H0[b], Hm), b
+    bs.close()
