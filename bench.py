@@ -59,6 +59,11 @@ FILM_L = (500e-9, 125e-9, 3e-9)
 # from an ncu capture of large-plain at 32x32x4 (43.906 GB read + 0.065 GB written
 # for 43.89 GB of tensor rows)
 TRAFFIC_PER_TENSOR_BYTE = (43.906 + 0.065) / 43.89
+# DRAM bytes (read + write) per lock-step tick of the batched integrator with all four
+# 64-instance tiles active, from an ncu capture of the first 200 ticks of the headline
+# workload (39.509 GB read + 12.506 GB written); ticks per full launch of the kernel
+BATCH_TRAFFIC_PER_TICK = (39.509e9 + 12.506e9) / 200
+BATCH_TICKS_PER_LAUNCH = 4000
 LARGE_RES = (64, 64, 8)
 LARGE_L = (320e-9, 320e-9, 40e-9)
 
@@ -556,7 +561,11 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
         "config": film_config(ws * B, window, nt),
         "precision": f"{args.precision} tcgen05 demag GEMM inside one persistent kernel",
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
-                     "frac": achieved / peak_tf, "traffic": None,
+                     "frac": achieved / peak_tf,
+                     "traffic": BATCH_TRAFFIC_PER_TICK * BATCH_TICKS_PER_LAUNCH if args.precision == "int8" else None,
+                     "traffic_note": "DRAM bytes per full 4000-tick launch, from the per-tick bytes of an ncu capture "
+                                     "of 200 ticks with all four instance tiles active (the heaviest ticks: an upper "
+                                     "bound for the tail)",
                      "note": f"batch_kernel (the whole persistent integrator, GEMM and RKSUITE coroutines): 18*n^2 "
                              f"useful flops per instance RHS evaluation x {evals} evaluations over {kms:.1f} ms of "
                              f"device time; peak = sustained cuBLAS bf16 ({src})"

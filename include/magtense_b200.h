@@ -96,6 +96,20 @@ int mt_load_demag_colmajor(mt_handle* h, const float* Kxx, const float* Kxy, con
 int mt_get_demag_colmajor(mt_handle* h, float* Kxx, float* Kxy, float* Kxz,
                           float* Kyy, float* Kyz, float* Kzz);
 
+/* Thresholded-sparse demag (dem_appr "threshold" = 2 / "threshold_fraction" = 4 of
+ * MagTenseMicroMagPyIO.f90; ApplyThresholdDense, DemagAuxFunctions.f90:20-122, and
+ * ConvertDenseToSparse_s, util_micromag.f90:81-138): keeps the entries of the
+ * assembled or loaded tensor with |K| > threshold and from then on computes every
+ * demag product (fields, right-hand side, integration) on those entries only.
+ * approx 2: value is the threshold; approx 4: value is the fraction of the positive
+ * entries to remove, turned into a threshold by the bisection of FindThresholdFraction
+ * (:353-428; a fraction >= 1 removes everything); approx 1 returns to the dense
+ * product.  Reports the kept entries (of the 9 block rows per cell; the symmetric
+ * blocks count twice) and the threshold used.  Assembling or loading a tensor
+ * again drops the sparse one.  Not for row shards or batches. */
+int mt_set_demag_threshold(mt_handle* h, int approx, double value, long long* nnz_out, float* threshold_out,
+                           void* stream);
+
 /* ---------------- fields and right-hand side ---------------- */
 
 /* Internal demag field Hm = Ms * (-K m) with m rounded to FP32 and an FP32
@@ -274,7 +288,9 @@ int icl_MVMult_GetH(const float* Mx, const float* My, const float* Mz, float* Hx
 /* replaces cu_destroy (MagTenseCudaBlas.cu:420-497) */
 int icl_destroy(void);
 /* replace cu_initDemagMatrices_sparse / cu_MVMult_GetH_sparse (MagTenseCudaBlas.cu:106-297):
- * thresholded-sparse demag is not on this path; they return MT_ERR_UNSUPPORTED. */
+ * called six times, once per block (mat_no 1..6 = xx xy xz yy yz zz), with 1-based CSR
+ * (rowInds of n + 1 entries, rowInds[n] = nnz + rowInds[0]); when all six are in, the
+ * product H = pref * K * M (FP32 host vectors) runs on the kept entries. */
 int icl_initDemagMatrices_sparse(int* n, int* nnz, int* mat_no, float* values, int* colInds,
                                  int* rowInds);
 int icl_MVMult_GetH_sparse(const float* Mx, const float* My, const float* Mz, float* Hx, float* Hy,

@@ -94,6 +94,7 @@ SIGNATURES = {
     "icl_initDemagMatrices": [F, F, F, F, F, F, I],
     "icl_MVMult_GetH": [F, F, F, F, F, F, I, F],
     "icl_destroy": [],
+    "mt_set_demag_threshold": [VP, C.c_int, C.c_double, C.POINTER(C.c_longlong), F, VP],
     "icl_initDemagMatrices_sparse": [I, I, I, F, I, I],
     "icl_MVMult_GetH_sparse": [F, F, F, F, F, F, I, F],
 }

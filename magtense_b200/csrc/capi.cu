@@ -6,6 +6,8 @@
 // every m / H / output device buffer.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <float.h>
+#include <stdint.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -26,6 +28,7 @@
 #include "llg.cuh"
 #include "batch.cuh"
 #include "gemm_tc.cuh"
+#include "sparse.cuh"
 #include <cudaTypedefs.h>
 
 namespace {
@@ -77,6 +80,9 @@ struct mt_handle {
     bool have_dynamics = false;
     // tensor
     float* K = nullptr; bool have_K = false;
+    // thresholded-sparse demag built from K (sparse.cu); nullptr: the dense product
+    int* sp_rowptr = nullptr; int* sp_col = nullptr; float* sp_val = nullptr;
+    long long sp_nnz = 0; float sp_thr = 0.f;
     // scratch
     float* m32 = nullptr;
     double* vjp_buf = nullptr;   // [lam (3n) | g_Ms (n)]
@@ -124,6 +130,7 @@ DevProb make_prob(const mt_handle* h)
     P.solver = h->solver; P.hext_row = h->hext_row; P.nt_hext = h->nt_hext; P.nt_alpha = h->nt_alpha;
     P.hext = h->hext; P.alpha_tab = h->alpha_tab;
     P.gamma = h->gamma; P.alpha0 = h->alpha0;
+    P.sp_rowptr = h->sp_rowptr; P.sp_col = h->sp_col; P.sp_val = h->sp_val;
     return P;
 }
 
@@ -222,6 +229,7 @@ int mt_destroy(mt_handle* h)
     free_ptr(h->Jfact); free_ptr(h->Kfact); free_ptr(h->Mfact); free_ptr(h->A6);
     free_ptr(h->hext); free_ptr(h->alpha_tab); free_ptr(h->K); free_ptr(h->m32);
     free_ptr(h->vjp_buf); free_ptr(h->vjp_z); free_ptr(h->vjp_v32);
+    free_ptr(h->sp_rowptr); free_ptr(h->sp_col); free_ptr(h->sp_val);
     for (int p = 0; p < kMaxShards; ++p)
         if (h->shard_ipc[p]) cudaIpcCloseMemHandle(h->shard_peer[p]);
     free_ptr(h->shard_region); free_ptr(h->shard_link);
@@ -286,9 +294,18 @@ int mt_set_dynamics(mt_handle* h, int solver, double gamma, double alpha0, const
     return MT_OK;
 }
 
+// a new dense tensor replaces the sparse one built from the old (call mt_set_demag_threshold again)
+static void drop_sparse(mt_handle* h)
+{
+    free_ptr(h->sp_rowptr); free_ptr(h->sp_col); free_ptr(h->sp_val);
+    h->sp_rowptr = nullptr; h->sp_col = nullptr; h->sp_val = nullptr;
+    h->sp_nnz = 0; h->sp_thr = 0.f;
+}
+
 int mt_assemble_demag(mt_handle* h, void* stream)
 {
     if (!h) return fail(MT_ERR_ARG, "null handle");
+    drop_sparse(h);
     int rc = ensure_tensor(h);
     if (rc) return rc;
     CUDA_TRY(launch_assemble(h->nx, h->ny, h->nz, h->L, h->d, h->n, h->ldk, h->shard_cell0, tensor_rows(h), h->K,
@@ -297,9 +314,91 @@ int mt_assemble_demag(mt_handle* h, void* stream)
     return MT_OK;
 }
 
+// FindThresholdFraction (DemagAuxFunctions.f90:353-428) on the positive entries of the
+// six blocks: bisection in single precision between the smallest and the largest
+// positive entry until the count of positive entries <= f_middle lies within +-0.01 of
+// frac times their number (the bounds in double, as the literal 0.01 is a default
+// real of the 8-byte-real build), at most 1000 steps; frac >= 1 removes everything.
+static int threshold_fraction(mt_handle* h, float frac, float* thr_out, cudaStream_t s)
+{
+    if (frac >= 1.0f) { *thr_out = FLT_MAX; return MT_OK; }
+    unsigned* mm = nullptr;
+    unsigned long long* cnt = nullptr;
+    CUDA_TRY(dalloc(&mm, 2));
+    struct FreeU { unsigned* p; ~FreeU() { cudaFree(p); } } fm{mm};
+    CUDA_TRY(dalloc(&cnt, 2));
+    struct FreeC { unsigned long long* p; ~FreeC() { cudaFree(p); } } fcn{cnt};
+    CUDA_TRY(sparse_positive_minmax(h->K, h->n, h->ldk, mm, s));
+    unsigned mmh[2];
+    CUDA_TRY(cudaMemcpyAsync(mmh, mm, sizeof(mmh), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (mmh[1] == 0u) { *thr_out = 0.f; return MT_OK; }   // no positive entry
+    float f_small, f_large;
+    memcpy(&f_small, &mmh[0], 4);
+    memcpy(&f_large, &mmh[1], 4);
+    unsigned long long ch[2] = {0, 0};
+    float f_middle = f_small;
+    for (int k_do = 1;; ++k_do) {
+        f_middle = (f_large - f_small) / 2.0f + f_small;
+        CUDA_TRY(sparse_count_positive(h->K, h->n, h->ldk, f_middle, cnt, s));
+        CUDA_TRY(cudaMemcpyAsync(ch, cnt, sizeof(ch), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        const unsigned long long n_pos = ch[0], count_middle = ch[1];
+        if ((float)count_middle > frac * (float)n_pos) f_large = f_middle;
+        else f_small = f_middle;
+        const double c = (double)count_middle, np = (double)n_pos;
+        if (c >= ((double)frac - 0.01) * np && c <= ((double)frac + 0.01) * np) break;
+        if (k_do > 1000) break;
+    }
+    *thr_out = f_middle;
+    return MT_OK;
+}
+
+int mt_set_demag_threshold(mt_handle* h, int approx, double value, long long* nnz_out, float* thr_out, void* stream)
+{
+    if (!h) return fail(MT_ERR_ARG, "null handle");
+    if (int rc = refuse_sharded(h, "mt_set_demag_threshold")) return rc;
+    if (!h->have_K) return fail(MT_ERR_STATE, "no demag tensor: assemble or load it first");
+    cudaStream_t s = (cudaStream_t)stream;
+    drop_sparse(h);
+    if (approx == 1) return MT_OK;   // the dense product
+    if (approx != 2 && approx != 4)
+        return fail(MT_ERR_UNSUPPORTED, "demag approximation %d: 1 (none), 2 (threshold), 4 (threshold fraction)", approx);
+    if (!(value >= 0.0)) return fail(MT_ERR_ARG, "threshold %g must be >= 0", value);
+    float thr = (float)value;
+    if (approx == 4) {
+        int rc = threshold_fraction(h, (float)value, &thr, s);
+        if (rc) return rc;
+    }
+    const int n = h->n, rows = 3 * n;
+    std::vector<int> counts(rows), rowptr(rows + 1);
+    int* d_counts = nullptr;
+    CUDA_TRY(dalloc(&d_counts, (size_t)rows));
+    struct Free { int* p; ~Free() { cudaFree(p); } } fc{d_counts};
+    CUDA_TRY(sparse_count_rows(h->K, n, h->ldk, thr, d_counts, s));
+    CUDA_TRY(cudaMemcpyAsync(counts.data(), d_counts, sizeof(int) * rows, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    long long nnz = 0;
+    for (int r = 0; r < rows; ++r) { rowptr[r] = (int)nnz; nnz += counts[r]; }
+    if (nnz > INT32_MAX) return fail(MT_ERR_UNSUPPORTED, "%lld kept entries exceed 32-bit CSR indices", nnz);
+    rowptr[rows] = (int)nnz;
+    CUDA_TRY(dalloc(&h->sp_rowptr, (size_t)rows + 1));
+    CUDA_TRY(dalloc(&h->sp_col, (size_t)std::max(nnz, 1LL)));
+    CUDA_TRY(dalloc(&h->sp_val, (size_t)std::max(nnz, 1LL)));
+    CUDA_TRY(cudaMemcpyAsync(h->sp_rowptr, rowptr.data(), sizeof(int) * (rows + 1), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(sparse_fill_rows(h->K, n, h->ldk, thr, h->sp_rowptr, h->sp_col, h->sp_val, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    h->sp_nnz = nnz;
+    h->sp_thr = thr;
+    if (nnz_out) *nnz_out = nnz;
+    if (thr_out) *thr_out = thr;
+    return MT_OK;
+}
+
 int mt_load_demag_colmajor(mt_handle* h, const float* Kxx, const float* Kxy, const float* Kxz, const float* Kyy,
                            const float* Kyz, const float* Kzz)
 {
+    if (h) drop_sparse(h);
     if (!h || !Kxx || !Kxy || !Kxz || !Kyy || !Kyz || !Kzz) return fail(MT_ERR_ARG, "null argument");
     if (int rc = refuse_sharded(h, "mt_load_demag_colmajor")) return rc;
     int rc = ensure_tensor(h);
@@ -1584,7 +1683,13 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
     Q.thres = thres; Q.round_off = round_off; Q.sqrrmc = sqrrmc; Q.cubrmc = cubrmc; Q.sqtiny = sqtiny;
     Q.toosml = toosml; Q.conv_tol = conv_tol;
     Q.comb_t = d_comb; Q.comb_flags = d_cflags; Q.ncomb = (int)comb.size();
+    // ticks per launch: 4000 (about a second at the 256-instance film); MT_BATCH_TICKS sets
+    // it, for example to profile one short launch
     Q.ticks_per_launch = 4000;
+    if (const char* e = getenv("MT_BATCH_TICKS")) {
+        const long long v = atoll(e);
+        if (v >= 1 && v <= 1000000) Q.ticks_per_launch = v;
+    }
     Q.evals_budget = 1LL << 60;
     DevProb P = batch_prob(bt);
     const size_t smem = batch_smem_bytes(n, h->ldk, bt->prec);
@@ -1758,14 +1863,77 @@ int icl_destroy(void)
     return MT_OK;
 }
 
-int icl_initDemagMatrices_sparse(int*, int*, int*, float*, int*, int*)
-{
-    return fail(MT_ERR_UNSUPPORTED, "thresholded-sparse demag is not on this path (dense tensor only)");
+// The six block matrices of the sparse shims (1-based CSR, rowInds[n] = nnz + rowInds[0]),
+// kept on the host until all six have arrived, then merged into the receiver-row CSR.
+namespace {
+struct IclSparse {
+    int n = 0;
+    bool have[6] = {false, false, false, false, false, false};
+    std::vector<int> rows[6], cols[6];
+    std::vector<float> vals[6];
+};
+IclSparse g_icl_sp;
 }
 
-int icl_MVMult_GetH_sparse(const float*, const float*, const float*, float*, float*, float*, const int*, const float*)
+int icl_initDemagMatrices_sparse(int* n, int* nnz, int* mat_no, float* values, int* colInds, int* rowInds)
 {
-    return fail(MT_ERR_UNSUPPORTED, "thresholded-sparse demag is not on this path (dense tensor only)");
+    if (!n || !nnz || !mat_no || *n < 1 || *nnz < 0 || *mat_no < 1 || *mat_no > 6 || !rowInds ||
+        (*nnz > 0 && (!values || !colInds)))
+        return fail(MT_ERR_ARG, "bad argument");
+    IclSparse& S = g_icl_sp;
+    if (S.n != *n) { S = IclSparse(); S.n = *n; }
+    const int k = *mat_no - 1, nn = *n, base = rowInds[0];
+    if (rowInds[nn] - base != *nnz) return fail(MT_ERR_ARG, "rowInds[n] - rowInds[0] must equal nnz");
+    S.rows[k].assign(rowInds, rowInds + nn + 1);
+    for (int& r : S.rows[k]) r -= base;
+    S.cols[k].resize(*nnz);
+    for (int e = 0; e < *nnz; ++e) {
+        S.cols[k][e] = colInds[e] - 1;
+        if (S.cols[k][e] < 0 || S.cols[k][e] >= nn) return fail(MT_ERR_ARG, "column index %d outside 1..n", colInds[e]);
+    }
+    S.vals[k].assign(values, values + *nnz);
+    S.have[k] = true;
+    for (int c = 0; c < 6; ++c) if (!S.have[c]) return MT_OK;
+    // all six blocks present: one problem with the merged receiver-row CSR
+    if (g_icl) { mt_destroy(g_icl); g_icl = nullptr; }
+    mt_grid g = {nn, 1, 1, 1.0, 1.0, 1.0};
+    int rc = mt_create(&g, &g_icl);
+    if (rc) return rc;
+    mt_handle* h = g_icl;
+    static const int blk[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    std::vector<int> rowptr(3 * (size_t)nn + 1), col;
+    std::vector<float> val;
+    for (int i = 0; i < nn; ++i)
+        for (int a = 0; a < 3; ++a) {
+            rowptr[3 * i + a] = (int)col.size();
+            for (int b = 0; b < 3; ++b) {
+                const int c = blk[a][b];
+                for (int e = S.rows[c][i]; e < S.rows[c][i + 1]; ++e) {
+                    col.push_back(b * h->ldk + S.cols[c][e]);
+                    val.push_back(S.vals[c][e]);
+                }
+            }
+        }
+    rowptr[3 * (size_t)nn] = (int)col.size();
+    const size_t nz = std::max<size_t>(col.size(), 1);
+    CUDA_TRY(dalloc(&h->sp_rowptr, rowptr.size()));
+    CUDA_TRY(dalloc(&h->sp_col, nz));
+    CUDA_TRY(dalloc(&h->sp_val, nz));
+    CUDA_TRY(cudaMemcpy(h->sp_rowptr, rowptr.data(), sizeof(int) * rowptr.size(), cudaMemcpyHostToDevice));
+    if (!col.empty()) {
+        CUDA_TRY(cudaMemcpy(h->sp_col, col.data(), sizeof(int) * col.size(), cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(h->sp_val, val.data(), sizeof(float) * val.size(), cudaMemcpyHostToDevice));
+    }
+    h->sp_nnz = (long long)col.size();
+    h->have_K = true;   // the product runs on the sparse rows; no dense tensor is kept
+    return MT_OK;
+}
+
+int icl_MVMult_GetH_sparse(const float* Mx, const float* My, const float* Mz, float* Hx, float* Hy, float* Hz,
+                           const int* n, const float* pref)
+{
+    if (!g_icl || !g_icl->sp_rowptr) return fail(MT_ERR_STATE, "icl_initDemagMatrices_sparse has not received all six blocks");
+    return icl_MVMult_GetH(Mx, My, Mz, Hx, Hy, Hz, const_cast<int*>(n), const_cast<float*>(pref));
 }
 
 }  // extern "C"

@@ -27,6 +27,11 @@ struct DevProb {
     const double* hext;      // [k*4 + {t,hx,hy,hz}]
     const double* alpha_tab; // [k*2 + {t,alpha}]
     double gamma, alpha0;
+    // thresholded-sparse demag (nullptr: the dense tensor): receiver row r = 3 i + a holds
+    // the kept entries K_ab(i, j) of blocks b = x, y, z in that order, column b*ldk + j
+    const int* sp_rowptr;    // [3n + 1]
+    const int* sp_col;
+    const float* sp_val;
 };
 
 // locate + interp1_MagTense (util.f90:39-85): 0 outside the table.
@@ -198,9 +203,43 @@ MT_DEV float4 ldg_stream(const float* p)
     return v;
 }
 
+// Sparse demag product for the receiver cells [c0, c0+nc): one warp per receiver row
+// (cell, component) sums its kept entries against m (staged in shared memory when
+// the whole [3][ldk] vector fits the chunk, read through L2 otherwise), lanes
+// strided over the row, then a fixed shuffle tree.
+MT_DEV void demag_cta_sparse(const DevProb& P, const float* __restrict__ m32, int c0, int nc, float* sm_m,
+                             float* S_out)
+{
+    const int ldk = P.ldk;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const bool staged = ldk <= kDemagJC;
+    __syncthreads();
+    if (staged) {
+        const int l4 = (3 * ldk) >> 2;
+        float4* d4 = reinterpret_cast<float4*>(sm_m);
+        const float4* s4 = reinterpret_cast<const float4*>(m32);
+        for (int e = threadIdx.x; e < l4; e += blockDim.x) d4[e] = __ldcg(s4 + e);
+    }
+    __syncthreads();
+    for (int r = warp; r < 3 * nc; r += nwarps) {
+        const int row = 3 * c0 + r;
+        const int e0 = __ldg(&P.sp_rowptr[row]), e1 = __ldg(&P.sp_rowptr[row + 1]);
+        float s = 0.f;
+        for (int e = e0 + lane; e < e1; e += 32) {
+            const int col = __ldg(&P.sp_col[e]);
+            const float mv = staged ? sm_m[col] : __ldcg(&m32[col]);
+            s = __fmaf_rn(__ldg(&P.sp_val[e]), mv, s);
+        }
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) S_out[r] = s;   // r = cell * 3 + a
+    }
+    __syncthreads();
+}
+
 MT_DEV void demag_cta(const DevProb& P, const float* __restrict__ m32, int c0, int nc, float* sm_m,
                       float* sm_part, float* S_out)
 {
+    if (P.sp_rowptr) { demag_cta_sparse(P, m32, c0, nc, sm_m, S_out); return; }
     const int ldk = P.ldk;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const int JC = ldk < kDemagJC ? ldk : kDemagJC;

@@ -9,9 +9,11 @@ sm_100a kernels of libmagtense_b200.so; there is no CPU path.
 
 Differences from the reference, all deliberate:
   * ``cuda`` is accepted and ignored (the device path is the only path).
-  * ``demag_approx`` other than None, ``cvode=True`` and non-uniform grids
-    raise NotImplementedError (thresholded/FFT demag and CVODE are not on
-    this path).
+  * ``demag_approx`` "threshold" / "threshold_fraction" with ``dem_thres``
+    run the thresholded-sparse demag of the reference; the FFT approximations,
+    ``cvode=True`` and non-uniform grids raise NotImplementedError (not on this
+    path).  After ``run_simulation`` the kept entries and the threshold used
+    are in ``demag_sparse``.
   * ``H_exc, H_ext, H_dem, H_ani`` are computed when ``ReturnHall=1``
     (StoreHeffComponents :306-349); otherwise they are zeros (the reference
     leaves the flag uninitialised on its Python path).
@@ -119,6 +121,7 @@ class MicromagProblem:
         self.renormalize = bool(renormalize)
         self.last_stats = None
         self._solver_obj = None
+        self.demag_sparse = None
 
     # --- properties with the reference's option maps ---------------------
     @property
@@ -177,8 +180,8 @@ class MicromagProblem:
     def _check_supported(self):
         if self._grid_type != 1:
             raise NotImplementedError("only grid_type='uniform' is on the B200 path")
-        if self._dem_appr != 1:
-            raise NotImplementedError("demag approximations (threshold/FFT) are not on the B200 path")
+        if self._dem_appr in (3, 5):
+            raise NotImplementedError("FFT demag approximations are not on the B200 path")
         if self.cvode:
             raise NotImplementedError("the CVODE integrator is not on the B200 path (RKSUITE 'M' only)")
         if self._solver not in (1, 2):
@@ -195,6 +198,9 @@ class MicromagProblem:
             s.load_tensor_colmajor(load_demag_tensor(self.N_file_in, self.ntot))
         else:
             s.assemble()
+        if self._dem_appr in (2, 4):   # ApplyThresholdDense (DemagAuxFunctions.f90:20-122)
+            self.demag_sparse = s.set_demag_threshold("threshold" if self._dem_appr == 2 else "threshold_fraction",
+                                                      self.dem_thres)
         return s
 
     def run_simulation(self, t_end, nt, fct_h_ext, nt_h_ext):
@@ -263,6 +269,8 @@ class MicromagProblem:
         self._check_supported()
         if self.N_load > 2:
             raise NotImplementedError("run_batch assembles its tensor; loading one from disk is run_simulation only")
+        if self._dem_appr != 1:
+            raise NotImplementedError("run_batch runs the dense demag product; thresholded demag is run_simulation only")
         n = self.ntot
         h = np.asarray(h_ext, dtype=np.float64)
         if h.ndim not in (2, 3) or h.shape[-1] != 3:

@@ -118,6 +118,18 @@ class Solver:
             check(_lib.lib().mt_load_demag_colmajor(self._h, *ptrs), "mt_load_demag_colmajor")
         self._have_tensor = True
 
+    def set_demag_threshold(self, approx, value, stream=None):
+        """Thresholded-sparse demag: approx "threshold" keeps |K| > value, "threshold_fraction"
+        removes the fraction value of the positive entries (the reference's bisection), None
+        returns to the dense product.  Returns (kept entries, threshold used)."""
+        code = {None: 1, "threshold": 2, "threshold_fraction": 4}[approx]
+        nnz = C.c_longlong(0)
+        thr = C.c_float(0.0)
+        with torch.cuda.device(self.device):
+            check(_lib.lib().mt_set_demag_threshold(self._h, code, float(value), C.byref(nnz), C.byref(thr),
+                                                    _stream(stream)), "mt_set_demag_threshold")
+        return nnz.value, thr.value
+
     def get_tensor_colmajor(self):
         """The six FP32 blocks as (n, n) arrays with K[i, j] = field at receiver i from source j."""
         out = [np.empty((self.n, self.n), dtype=np.float32, order="F") for _ in range(6)]

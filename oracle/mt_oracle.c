@@ -1399,3 +1399,63 @@ void or_demag_rows(const float* K32, const double* K64, int nrows, int n, const 
     }
     free(ms);
 }
+
+/* ------------------------------------------------------------------ */
+/* thresholded-sparse demag                                            */
+/* ------------------------------------------------------------------ */
+/* FindThresholdFraction (DemagAuxFunctions.f90:353-428) as ApplyThresholdDense
+ * (:20-122) calls it: on the positive entries of the six blocks (K32[c][i][j],
+ * masks K > 0 at :45-50), bisection in single precision between the smallest and
+ * the largest of them; a step counts the positive entries <= f_middle, moves the
+ * upper end when that count exceeds frac * (their number) and the lower end
+ * otherwise, and stops when the count lies within (frac -+ 0.01) * number, the
+ * literal 0.01 being a double in the 8-byte-real build; at most 1000 steps;
+ * frac >= 1 returns huge(). */
+float or_threshold_fraction(const float* K32, int n, float frac)
+{
+    if (frac >= 1.0f) return FLT_MAX;
+    const size_t tot = (size_t)6 * n * n;
+    long long n_pos = 0;
+    float f_small = FLT_MAX, f_large = 0.0f;
+    for (size_t e = 0; e < tot; ++e) {
+        const float v = K32[e];
+        if (v > 0.0f) {
+            n_pos++;
+            if (v < f_small) f_small = v;
+            if (v > f_large) f_large = v;
+        }
+    }
+    if (n_pos == 0) return 0.0f;
+    float f_middle = f_small;
+    for (int k_do = 1;; ++k_do) {
+        f_middle = (f_large - f_small) / 2.0f + f_small;
+        long long count_middle = 0;
+#pragma omp parallel for reduction(+ : count_middle) schedule(static)
+        for (long long e = 0; e < (long long)tot; ++e) {
+            const float v = K32[e];
+            if (v > 0.0f && v <= f_middle) count_middle++;
+        }
+        if ((float)count_middle > frac * (float)n_pos) f_large = f_middle;
+        else f_small = f_middle;
+        const double c = (double)count_middle, np = (double)n_pos;
+        if (c >= ((double)frac - 0.01) * np && c <= ((double)frac + 0.01) * np) break;
+        if (k_do > 1000) break;
+    }
+    return f_middle;
+}
+
+/* Keep only the entries with |K| > thr (ConvertDenseToSparse_s, util_micromag.f90:98)
+ * in the FP32 product of mode 0: the dropped entries are zeroed in the column copy,
+ * which leaves every remaining term and its order unchanged.  Returns the kept
+ * entries of the six blocks. */
+long long or_problem_set_threshold(or_problem* p, float thr)
+{
+    if (!p->KT32) return -1;
+    const size_t tot = (size_t)6 * p->n * p->n;
+    long long kept = 0;
+    for (size_t e = 0; e < tot; ++e) {
+        if (fabsf(p->KT32[e]) > thr) kept++;
+        else p->KT32[e] = 0.0f;
+    }
+    return kept;
+}

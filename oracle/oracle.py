@@ -78,6 +78,10 @@ def lib():
         L.or_solve_linear.argtypes = [C.c_int, D, D, C.c_int, D, C.c_double, C.c_double, D, D, I,
                                       C.POINTER(Stats)]
         L.or_demag_rows.argtypes = [F, D, C.c_int, C.c_int, D, D, C.c_int, D]
+        L.or_threshold_fraction.argtypes = [F, C.c_int, C.c_float]
+        L.or_threshold_fraction.restype = C.c_float
+        L.or_problem_set_threshold.argtypes = [C.c_void_p, C.c_float]
+        L.or_problem_set_threshold.restype = C.c_longlong
         L.or_stats_size.restype = C.c_int
         assert L.or_stats_size() == C.sizeof(Stats), "oracle stats layout mismatch"
     return _lib
@@ -138,6 +142,12 @@ def demag_rows(K32, K64, m, Ms_rows, mode=0):
     return out
 
 
+def threshold_fraction(K32, frac):
+    """FindThresholdFraction's threshold for the tensor K32[c][i][j] (FP32)."""
+    K32 = np.ascontiguousarray(K32, dtype=np.float32)
+    return float(lib().or_threshold_fraction(_f(K32), K32.shape[1], float(frac)))
+
+
 def interp1(table, col, x):
     table = np.ascontiguousarray(table, dtype=np.float64)
     return lib().or_interp1(_d(table), table.shape[1], col, table.shape[0], float(x))
@@ -186,6 +196,10 @@ class Problem:
 
     def set_hext_ind(self, i):
         lib().or_problem_set_hext_ind(self.h, int(i))
+
+    def set_threshold(self, thr):
+        """mode 0: keep only the tensor entries with |K| > thr (FP32); returns their count."""
+        return int(lib().or_problem_set_threshold(self.h, float(thr)))
 
     def set_renorm(self, on):
         lib().or_problem_set_renorm(self.h, int(bool(on)))

@@ -338,3 +338,61 @@ def test_std_problem_4_oracle_near_published_band(oracle):
     dist = sum(np.trapezoid(np.abs(mavg[:, j] - np.interp(tn, t_ns, mean[:, j])), tn) for j in range(3))
     assert dist <= 0.15, dist
     assert np.abs(mavg[:100] - mean[:100]).max() < 0.05
+
+
+# ---------------------------------------------------------------- thresholded-sparse demag
+def reference_threshold_fraction(K32, frac):
+    """FindThresholdFraction (DemagAuxFunctions.f90:353-428) restated with numpy
+    float32 scalars on the positive entries that ApplyThresholdDense packs (:45-99)."""
+    frac = np.float32(frac)
+    if frac >= 1:
+        return np.finfo(np.float32).max
+    pos = K32[K32 > 0].astype(np.float32)
+    n = pos.size
+    f_large, f_small = pos.max(), pos.min()
+    k_do = 1
+    while True:
+        f_middle = np.float32(np.float32(f_large - f_small) / np.float32(2)) + f_small
+        count_middle = int(np.count_nonzero(pos <= f_middle))
+        if np.float32(count_middle) > frac * np.float32(n):
+            f_large = f_middle
+        else:
+            f_small = f_middle
+        if (float(frac) - 0.01) * n <= count_middle <= (float(frac) + 0.01) * n:
+            return f_middle
+        if k_do > 1000:
+            return f_middle
+        k_do += 1
+
+
+@pytest.mark.parametrize("frac", [0.3, 0.75, 0.95, 1.0])
+def test_threshold_fraction_matches_reference_bisection(oracle, frac):
+    res, L = [12, 6, 2], [60e-9, 30e-9, 10e-9]
+    K32, _ = oracle.assemble(res, L, fp32=True)
+    got = np.float32(oracle.threshold_fraction(K32, frac))
+    want = reference_threshold_fraction(K32, frac)
+    assert got == want, (got, want)
+    if frac < 1:
+        pos = K32[K32 > 0]
+        assert abs(np.count_nonzero(pos <= got) / pos.size - frac) <= 0.01 + 1e-12
+
+
+def test_thresholded_demag_is_the_kept_entries_product(oracle):
+    """mode 0 with a threshold: the demag field of the tensor whose entries with
+    |K| <= threshold are dropped (ConvertDenseToSparse_s keeps |K| > threshold)."""
+    res, L = [10, 6, 2], [50e-9, 30e-9, 10e-9]
+    n = 120
+    K32, _ = oracle.assemble(res, L, fp32=True)
+    thr = np.float32(oracle.threshold_fraction(K32, 0.6))
+    P = oracle.Problem(res, L, mode=0, K32=K32)
+    kept = P.set_threshold(thr)
+    assert kept == int(np.count_nonzero(np.abs(K32) > thr))
+    rng = np.random.default_rng(4)
+    m = rng.standard_normal((3, n))
+    m /= np.linalg.norm(m, axis=0)
+    H = P.fields(0.0, m)[3]
+    Ks = np.where(np.abs(K32) > thr, K32, 0).astype(np.float64)
+    blk = [[0, 1, 2], [1, 3, 4], [2, 4, 5]]
+    m32 = m.astype(np.float32).astype(np.float64)
+    want = np.stack([-8e5 * sum(Ks[blk[a][b]] @ m32[b] for b in range(3)) for a in range(3)])
+    assert np.abs(H - want).max() <= 1e-5 * np.abs(want).max()
