@@ -60,6 +60,8 @@ struct BCtx {
     const unsigned* bits;   // [Bp / 32] request bits of this tick (packed)
     const int* pre;         // [Bp / 32] requests before each word (packed)
     int sched;              // Stream-K schedule word of this tick's GEMM
+    bool prev_valid;        // bits/pre hold the previous tick's requests (int8): the coroutines also
+                            // write their operand rows at those compact positions
 };
 
 // compact position of requesting instance b: requests with a smaller index
@@ -111,7 +113,7 @@ MT_DEV void split_store(float f, int prec, uint16_t* hi_out, uint16_t* lo_out)
 constexpr double kI8MScale = 1073741824.0;   // 2^30
 constexpr double kI8MMax = 1.96;
 
-MT_DEV void i8_store_m(double v, int8_t* dst, size_t limb_stride, GridSync* gs)
+MT_DEV void i8_store_m(double v, int8_t* dst, size_t limb_stride, GridSync* gs, int8_t* dst2 = nullptr)
 {
     if (!(fabs(v) <= kI8MMax)) {
         if (atomicCAS(&gs->err, 0, KERR_RANGE) == 0) gs->err_where = 300;
@@ -131,6 +133,10 @@ MT_DEV void i8_store_m(double v, int8_t* dst, size_t limb_stride, GridSync* gs)
     d[0] = (int8_t)x;
 #pragma unroll
     for (int l = 0; l < 4; ++l) dst[(size_t)l * limb_stride] = d[l];
+    if (dst2) {
+#pragma unroll
+        for (int l = 0; l < 4; ++l) dst2[(size_t)l * limb_stride] = d[l];
+    }
 }
 
 // write the stage argument (FP64) and the GEMM operand copy for one element
@@ -141,7 +147,10 @@ MT_DEV void put_arg(const BCtx& X, int argi, int b, int q, double v)
     const int a = (q >= n) + (q >= 2 * n), i = q - a * n;   // q < 3n
     const float f = (float)v;
     if (X.Q.prec == kPrecI8) {
-        i8_store_m(v, X.F.mlimb + (size_t)b * X.Q.Kd + (size_t)a * X.Q.np + i, (size_t)X.Q.Bp * X.Q.Kd, X.F.gs);
+        int8_t* comp = nullptr;
+        if (X.prev_valid && ((X.bits[b >> 5] >> (b & 31)) & 1u))
+            comp = X.F.mcomp + (size_t)compact_pos(X, b) * X.Q.Kd + (size_t)a * X.Q.np + i;
+        i8_store_m(v, X.F.mlimb + (size_t)b * X.Q.Kd + (size_t)a * X.Q.np + i, (size_t)X.Q.Bp * X.Q.Kd, X.F.gs, comp);
     } else if (X.Q.prec == kPrecFP32) {
         X.F.m32[((size_t)b * 3 + a) * X.P.ldk + i] = f;
     } else {
@@ -159,6 +168,7 @@ struct ArgDst {
     uint16_t* mhi;         // 16-bit splits: column b*Kd
     uint16_t* mlo;
     int8_t* mlimb;         // int8: column b*Kd of limb 0
+    int8_t* mcomp;         // int8: the instance's row at its previous compact position, or nullptr
     size_t limb_stride;
     GridSync* gs;
 };
@@ -172,6 +182,8 @@ MT_DEV ArgDst arg_dst(const BCtx& X, int argi, int b)
     d.mhi = X.F.mhi ? X.F.mhi + (size_t)b * X.Q.Kd : nullptr;
     d.mlo = X.F.mlo ? X.F.mlo + (size_t)b * X.Q.Kd : nullptr;
     d.mlimb = X.F.mlimb ? X.F.mlimb + (size_t)b * X.Q.Kd : nullptr;
+    d.mcomp = (X.F.mlimb && X.prev_valid && ((X.bits[b >> 5] >> (b & 31)) & 1u))
+                  ? X.F.mcomp + (size_t)compact_pos(X, b) * X.Q.Kd : nullptr;
     d.limb_stride = (size_t)X.Q.Bp * X.Q.Kd;
     d.gs = X.F.gs;
     return d;
@@ -182,7 +194,8 @@ MT_DEV void put_arg_d(const ArgDst& d, int q, double v)
     d.pool[q] = v;
     const int a = (q >= d.n) + (q >= 2 * d.n), i = q - a * d.n;   // q < 3n
     if (d.prec == kPrecI8) {
-        i8_store_m(v, d.mlimb + (size_t)a * d.np + i, d.limb_stride, d.gs);
+        i8_store_m(v, d.mlimb + (size_t)a * d.np + i, d.limb_stride, d.gs,
+                   d.mcomp ? d.mcomp + (size_t)a * d.np + i : nullptr);
     } else if (d.prec == kPrecFP32) {
         d.m32[(size_t)a * d.ldk + i] = (float)v;
     } else {
@@ -1256,6 +1269,7 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
     X.cov = s_cov;
     X.packed = false;
     X.sched = 0;
+    X.prev_valid = false;
     X.bits = s_bits;
     X.pre = s_pre;
     const int W = Q.Bp / 32;
@@ -1381,6 +1395,12 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
             // requesting instances, packed in index order: every CTA builds the same prefix table,
             // copies its share of their operand rows to the compact buffer, then the GEMM runs
             // over ceil(requests / 64) tiles of that buffer
+            // Every active instance requests a right-hand side in every tick (norms resolve
+            // in place), so the set of requests only shrinks within a launch: the same count
+            // as in the previous tick means the same set, and the coroutines have already
+            // written their rows at their compact positions (put_arg).  Otherwise pack.
+            const int nr_prev = X.prev_valid ? s_pre[W] : -1;
+            __syncthreads();
             for (int w = threadIdx.x; w < W; w += blockDim.x) s_bits[w] = __ldcg(&F.reqbits[(tick % 3) * W + w]);
             __syncthreads();
             if (threadIdx.x == 0) {
@@ -1390,6 +1410,7 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
             }
             __syncthreads();
             const int nr = s_pre[W];
+            const bool same = nr == nr_prev;
             X.packed = true;
             X.nact = (nr + kI8N - 1) / kI8N;
             X.U = (long long)X.nact * Q.RB * Q.nks;
@@ -1404,10 +1425,13 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
                 X.jb0 = first < (1 << 30) ? first / kI8N : 0;
             }
             i8_fill_cover(X, s_cov);   // read in the epilogue, after the barrier that follows the GEMM
-            i8_pack(X, nr, s_bits, s_pre, W);
-            asm volatile("fence.proxy.async.global;" ::: "memory");   // packed rows -> TMA reads
-            __syncthreads();
-            if (!grid_sync(F.gs, 6)) { ok = false; break; }
+            if (!same) {
+                i8_pack(X, nr, s_bits, s_pre, W);
+                asm volatile("fence.proxy.async.global;" ::: "memory");   // packed rows -> TMA reads
+                __syncthreads();
+                if (!grid_sync(F.gs, 6)) { ok = false; break; }
+            }
+            X.prev_valid = true;
             for (int k = threadIdx.x; k < X.nact; k += blockDim.x) s_act[k] = k;
             __syncthreads();
             if (X.nact > 0 && !tc_i8_streamk(X.smem, F, F.part, Q.maxseg, maps, &maps.blo, X.nact, s_act, Q.RB, Q.nks,
