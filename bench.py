@@ -506,9 +506,9 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
         _, y, _, st = bs.integrate(t, m0, tol=1e-6)
         return st
 
-    times, stats, clocks, flush = timed_steps(torch, step, args.steps, args.warmup, dist, local)
     # the plain FP32 single-instance path on the same workload, for the ratio: seeded instances
-    # of this rank's set, each integrated over the same window, one after another
+    # of this rank's set, each integrated over the same window, one after another (before the
+    # batched timing, on an idle device)
     pick = sorted(int(k) for k in np.random.default_rng(7).choice(B, size=min(args.plain_sample, B), replace=False))
     plain_s, plain_evals, plain_m = 0.0, 0, []
     for k in pick:
@@ -523,6 +523,7 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
         plain_m.append((tp, yp.view(nt, 3, n).mean(dim=2).cpu().numpy()))
         del yp
     plain_rate = len(pick) * window / plain_s
+    times, stats, clocks, flush = timed_steps(torch, step, args.steps, args.warmup, dist, local)
     # end to end through the public API: host m0 in (pinned), host trajectories out
     e2e_ms, batch_m = None, None
     if not args.no_e2e:

@@ -1286,17 +1286,27 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
     tcs.kb_done = 0; tcs.tiles = 0; tcs.tmem = 0;
     if (tc) tc_init_impl(X.smem, tcs);
     if (i8) tc_i8_init(X.smem, tcs);
-    // each lane keeps its own (identical) copy of the coroutines of its warp
-    BInst L[kMaxInstPerWarp];
+    // The coroutines of a warp: one copy per warp in shared memory when the CTA's copies
+    // fit next to the GEMM's buffers (every lane reads and writes the same, identical
+    // values), otherwise one copy per lane in local memory.
+    BInst L_loc[kMaxInstPerWarp];
+    BInst* L = Q.inst_smem_off ? reinterpret_cast<BInst*>(smem_raw + Q.inst_smem_off) + (size_t)X.warp * Q.inst_per_warp
+                               : L_loc;
     int mine = 0;
     for (int li = X.warp; li < X.ni && mine < kMaxInstPerWarp; li += X.nwarps, ++mine) {
         const long long* src = reinterpret_cast<const long long*>(&F.inst[(size_t)X.cb * Q.Bp + X.i0 + li]);
         long long* dst = reinterpret_cast<long long*>(&L[mine]);
-        for (int w = 0; w < (int)(sizeof(BInst) / 8); ++w) dst[w] = __ldcg(src + w);
+        if (Q.inst_smem_off) {
+            for (int w = X.lane; w < (int)(sizeof(BInst) / 8); w += 32) dst[w] = __ldcg(src + w);
+            __syncwarp();
+        } else {
+            for (int w = 0; w < (int)(sizeof(BInst) / 8); ++w) dst[w] = __ldcg(src + w);
+        }
         if (L[mine].req == 4) L[mine].req = 0;                 // parked by the previous launch
         L[mine].red_seq = 0;                                   // the arrival counters start at zero
         L[mine].budget_mark = L[mine].s.full_f_count + L[mine].s.f_count + Q.evals_budget;
     }
+    __syncwarp();
     bool ok = true;
     if (Q.demag_only) {
         // one product of the operands already in place, then H = -Ms * sum of partials
@@ -1689,10 +1699,24 @@ size_t batch_smem_bytes(int n, int ldk, int prec)
                              : tc_smem_bytes();
 }
 
+// where the coroutine copies go in dynamic shared memory (0: local memory) and how much
+// they add, for per_cta instances per CTA on kBatchThreads threads
+size_t batch_inst_smem(int n, int ldk, int prec, int per_cta, int* off, int* per_warp)
+{
+    const int nw = kBatchThreads / 32;
+    *per_warp = (per_cta + nw - 1) / nw;
+    const size_t base = (batch_smem_bytes(n, ldk, prec) + 127) & ~(size_t)127;
+    const size_t bytes = (size_t)nw * (*per_warp) * sizeof(BInst);
+    constexpr size_t kStaticBudget = 12 * 1024;   // the kernel's static shared memory, rounded up
+    if (*per_warp > kMaxInstPerWarp || base + bytes + kStaticBudget > 227 * 1024) { *off = 0; return 0; }
+    *off = (int)base;
+    return (base - batch_smem_bytes(n, ldk, prec)) + bytes;
+}
+
 cudaError_t launch_batch(const DevProb& P, const BatchBufs& Bf, const BatchParams& Q, int grid, const void* tmaps,
                          cudaStream_t s, const void* l2_base, size_t l2_bytes, float l2_hit)
 {
-    const size_t smem = batch_smem_bytes(P.n, P.ldk, Q.prec);
+    const size_t smem = batch_smem_bytes(P.n, P.ldk, Q.prec) + Q.inst_smem_bytes;
     cudaError_t e = cudaFuncSetAttribute(batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     TcMaps m;

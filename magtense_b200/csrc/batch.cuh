@@ -92,11 +92,15 @@ struct BatchParams {
     int sk_sched[2 * kMaxIB + 1];
     int tune_nact;            // > 0: demag_only times the product over this many tiles with tune_sched
     int tune_sched;
+    // coroutine copies in dynamic shared memory at this offset (0: local memory), per warp
+    int inst_smem_off, inst_per_warp;
+    size_t inst_smem_bytes;
 };
 
 cudaError_t batch_upload_tables();
 int batch_grid(int n, int B, int num_sms, int prec, int* CB, int* IB, int* S);
 size_t batch_smem_bytes(int n, int ldk, int prec);
+size_t batch_inst_smem(int n, int ldk, int prec, int per_cta, int* off, int* per_warp);
 cudaError_t launch_batch(const DevProb& P, const BatchBufs& Bf, const BatchParams& Q, int grid, const void* tmaps,
                          cudaStream_t s, const void* l2_base = nullptr, size_t l2_bytes = 0, float l2_hit = 0.f);
 cudaError_t launch_split_tensor(const float* K, int n, int ldk, int np, int prec, uint16_t* khi, uint16_t* klo,

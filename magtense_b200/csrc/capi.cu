@@ -1452,6 +1452,8 @@ int batch_alloc(mt_batch* bt, BatchRun*& Rp, int nt, cudaStream_t s)
     Q.RB = RB; Q.nks = nks; Q.maxseg = maxseg; Q.row_scale = bt->row_scale;
     for (int k = 0; k <= 2 * kMaxIB; ++k) Q.sk_sched[k] = bt->sched[k];
     Q.renorm = h->renorm;
+    if (!getenv("MT_BATCH_LOCAL_INST"))
+        Q.inst_smem_bytes = batch_inst_smem(n, h->ldk, bt->prec, kInstBlock / bt->S, &Q.inst_smem_off, &Q.inst_per_warp);
     memset(&R.maps, 0, sizeof(R.maps));
     if (bt->prec == MT_PREC_INT8) {
         int rc;
@@ -1692,7 +1694,7 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
     }
     Q.evals_budget = 1LL << 60;
     DevProb P = batch_prob(bt);
-    const size_t smem = batch_smem_bytes(n, h->ldk, bt->prec);
+    const size_t smem = batch_smem_bytes(n, h->ldk, bt->prec) + Q.inst_smem_bytes;
     if (smem > 227 * 1024) return fail(MT_ERR_UNSUPPORTED, "batch shared memory %zu exceeds 227 KB", smem);
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     CUDA_TRY(cudaEventCreate(&ev0));
