@@ -262,6 +262,185 @@ __device__ __noinline__ double stage_args(int i, const double* __restrict__ y, c
     return lm;
 }
 
+// The other per-element loops of a step, written like stage_args: non-inlined, plain
+// pointers, three elements per lane in flight, each element's arithmetic in the same
+// order as the synchronous formulation (and the oracle).
+constexpr int kInFlight = 3;
+
+MT_DEV int own_q(int e, int n, int c0, int nc)
+{
+    const int a = (e >= nc) + (e >= 2 * nc);   // e < 3 nc
+    return a * n + c0 + (e - a * nc);
+}
+
+// stage i = 9..11 of the interpolant: y_old + h_old (a_i1 k1 + sum_{j=2}^{i-1} a_ij k_j), k8 = y'
+struct IntPtrs { const double* k[11]; };
+
+__device__ __noinline__ void interp_stage_args(int i, const double* __restrict__ yold, const double* __restrict__ k1,
+                                               IntPtrs st, ArgDst d, double h_old, int lane, int c0, int nc)
+{
+    const int n = d.n, tot = 3 * nc;
+    for (int e0 = lane; e0 < tot; e0 += 32 * kInFlight) {
+        int q[kInFlight];
+        bool on[kInFlight];
+        double kv[kInFlight][11], k1q[kInFlight], yoq[kInFlight];
+#pragma unroll
+        for (int u = 0; u < kInFlight; ++u) {
+            const int e = e0 + 32 * u;
+            on[u] = e < tot;
+            q[u] = own_q(on[u] ? e : e0, n, c0, nc);
+#pragma unroll
+            for (int j = 2; j <= 10; ++j) kv[u][j] = (j <= i - 1) ? ldcg(&st.k[j][q[u]]) : 0.0;
+            k1q[u] = ldcg(&k1[q[u]]);
+            yoq[u] = ldcg(&yold[q[u]]);
+        }
+#pragma unroll
+        for (int u = 0; u < kInFlight; ++u) {
+            if (!on[u]) continue;
+            double e = xmul(cB.a[i][1], k1q[u]);
+#pragma unroll
+            for (int j = 2; j <= 10; ++j) {
+                if (j > i - 1) break;
+                e = xadd(e, xmul(cB.a[i][j], kv[u][j]));
+            }
+            put_arg_d(d, q[u], xadd(yoq[u], xmul(h_old, e)));
+        }
+    }
+    __syncwarp();
+}
+
+// the interpolant's coefficients p1..p5 (the vendored grouping of terms), times h_old
+struct PolyPtrs { const double* k[12]; double* p[6]; };
+
+__device__ __noinline__ void interp_coeffs(PolyPtrs pp, double ho, int lane, int n, int c0, int nc)
+{
+    const int tot = 3 * nc;
+    for (int e0 = lane; e0 < tot; e0 += 32 * kInFlight) {
+        int q[kInFlight];
+        bool on[kInFlight];
+        double K[kInFlight][12];
+#pragma unroll
+        for (int u = 0; u < kInFlight; ++u) {
+            const int e = e0 + 32 * u;
+            on[u] = e < tot;
+            q[u] = own_q(on[u] ? e : e0, n, c0, nc);
+            K[u][1] = ldcg(&pp.k[1][q[u]]);
+#pragma unroll
+            for (int j = 3; j <= 11; ++j) K[u][j] = ldcg(&pp.k[j][q[u]]);
+        }
+#pragma unroll
+        for (int u = 0; u < kInFlight; ++u) {
+            if (!on[u]) continue;
+            const double K1 = K[u][1], K3 = K[u][3], K4 = K[u][4], K5 = K[u][5], K6 = K[u][6], K7 = K[u][7];
+            const double K8 = K[u][8], K9 = K[u][9], K10 = K[u][10], K11 = K[u][11];
+#define R(i, j) cB.r[i][j]
+#define M(a, b2) xmul(a, b2)
+#define A(a, b2) xadd(a, b2)
+            const double p5 = A(A(M(R(5, 6), K5), A(A(M(R(10, 6), K10), M(R(8, 6), K8)), A(M(R(7, 6), K7), M(R(6, 6), K6)))),
+                                A(A(A(M(R(4, 6), K4), M(R(9, 6), K9)), A(M(R(3, 6), K3), M(R(11, 6), K11))), M(R(1, 6), K1)));
+            const double p4 = A(A(A(M(R(10, 5), K10), M(R(9, 5), K9)), A(A(M(R(7, 5), K7), M(R(6, 5), K6)), M(R(5, 5), K5))),
+                                A(A(A(M(R(4, 5), K4), M(R(8, 5), K8)), A(M(R(3, 5), K3), M(R(11, 5), K11))), M(R(1, 5), K1)));
+            const double p3 = A(A(A(A(M(R(4, 4), K4), M(R(8, 4), K8)), A(M(R(7, 4), K7), M(R(6, 4), K6))), M(R(5, 4), K5)),
+                                A(A(A(M(R(10, 4), K10), M(R(9, 4), K9)), A(M(R(3, 4), K3), M(R(11, 4), K11))), M(R(1, 4), K1)));
+            const double p2 = A(A(A(M(R(5, 3), K5), M(R(6, 3), K6)),
+                                  A(A(A(M(R(3, 3), K3), M(R(9, 3), K9)), A(M(R(10, 3), K10), M(R(8, 3), K8))), M(R(1, 3), K1))),
+                                A(A(M(R(4, 3), K4), M(R(11, 3), K11)), M(R(7, 3), K7)));
+            const double p1 = A(A(A(M(R(5, 2), K5), A(A(M(R(6, 2), K6), M(R(8, 2), K8)), M(R(1, 2), K1))),
+                                  A(A(M(R(3, 2), K3), M(R(9, 2), K9)), M(R(10, 2), K10))),
+                                A(A(M(R(4, 2), K4), M(R(11, 2), K11)), M(R(7, 2), K7)));
+#undef R
+#undef M
+#undef A
+            pp.p[5][q[u]] = xmul(ho, p5); pp.p[4][q[u]] = xmul(ho, p4); pp.p[3][q[u]] = xmul(ho, p3);
+            pp.p[2][q[u]] = xmul(ho, p2); pp.p[1][q[u]] = xmul(ho, p1);
+        }
+    }
+    __syncwarp();
+}
+
+// the interpolated solution at sigma: ((((p5 s + p4) s + p3) s + p2) s + p1) s + h y') s + y
+__device__ __noinline__ void interp_eval(PolyPtrs pp, const double* __restrict__ y, const double* __restrict__ yp,
+                                         double* __restrict__ dst, double sigma, double h_old, int lane, int n, int c0,
+                                         int nc)
+{
+    const int tot = 3 * nc;
+    for (int e0 = lane; e0 < tot; e0 += 32 * kInFlight) {
+        int q[kInFlight];
+        bool on[kInFlight];
+        double P[kInFlight][6], ypq[kInFlight], yq[kInFlight];
+#pragma unroll
+        for (int u = 0; u < kInFlight; ++u) {
+            const int e = e0 + 32 * u;
+            on[u] = e < tot;
+            q[u] = own_q(on[u] ? e : e0, n, c0, nc);
+#pragma unroll
+            for (int j = 1; j <= 5; ++j) P[u][j] = ldcg(&pp.p[j][q[u]]);
+            ypq[u] = ldcg(&yp[q[u]]);
+            yq[u] = ldcg(&y[q[u]]);
+        }
+#pragma unroll
+        for (int u = 0; u < kInFlight; ++u) {
+            if (!on[u]) continue;
+            double v = xmul(P[u][5], sigma);
+            v = xmul(xadd(v, P[u][4]), sigma);
+            v = xmul(xadd(v, P[u][3]), sigma);
+            v = xmul(xadd(v, P[u][2]), sigma);
+            v = xmul(xadd(v, P[u][1]), sigma);
+            dst[q[u]] = xadd(xmul(xadd(v, xmul(h_old, ypq[u])), sigma), yq[u]);
+        }
+    }
+    __syncwarp();
+}
+
+// the error estimate of a completed step and the new weights; returns the lane's max of |es| / w
+struct ErrPtrs { const double* k[8]; };
+
+__device__ __noinline__ double step_error(ErrPtrs st, const double* __restrict__ y, const double* __restrict__ yp,
+                                          const double* __restrict__ yn, const double* __restrict__ k8,
+                                          double* __restrict__ es, double* __restrict__ w, double htry, double thr,
+                                          int lane, int n, int c0, int nc)
+{
+    const int tot = 3 * nc;
+    double lm = 0.0;
+    for (int e0 = lane; e0 < tot; e0 += 32 * kInFlight) {
+        int q[kInFlight];
+        bool on[kInFlight];
+        double kv[kInFlight][8], esq[kInFlight], ypq[kInFlight], k8q[kInFlight], yq[kInFlight], ynq[kInFlight];
+#pragma unroll
+        for (int u = 0; u < kInFlight; ++u) {
+            const int e = e0 + 32 * u;
+            on[u] = e < tot;
+            q[u] = own_q(on[u] ? e : e0, n, c0, nc);
+#pragma unroll
+            for (int i = 2; i <= 7; ++i) kv[u][i] = ldcg(&st.k[i][q[u]]);
+            esq[u] = ldcg(&es[q[u]]);
+            ypq[u] = ldcg(&yp[q[u]]);
+            k8q[u] = ldcg(&k8[q[u]]);
+            yq[u] = ldcg(&y[q[u]]);
+            ynq[u] = ldcg(&yn[q[u]]);
+        }
+#pragma unroll
+        for (int u = 0; u < kInFlight; ++u) {
+            if (!on[u]) continue;
+            double v = esq[u];
+            v = xsub(v, xmul(cB.b[1], ypq[u]));
+#pragma unroll
+            for (int i = 2; i <= 7; ++i) {
+                if (cB.b[i] == 0.0) continue;
+                v = xsub(v, xmul(cB.b[i], kv[u][i]));
+            }
+            v = xsub(v, xmul(cB.b[8], k8q[u]));
+            v = xmul(htry, v);
+            es[q[u]] = v;
+            const double wq = fmax(xmul(0.5, xadd(fabs(yq[u]), fabs(ynq[u]))), thr);
+            w[q[u]] = wq;
+            lm = fmax(lm, fabs(v) / wq);
+        }
+    }
+    __syncwarp();
+    return lm;
+}
+
 MT_DEV double warp_red(double v, bool is_max)
 {
     return is_max ? warp_max(v) : warp_sum(v);
@@ -415,21 +594,9 @@ MT_DEV void advance(BCtx& X, BInst& I, int b)
                             const double* yold = VPOOL(X, s.iyold, b);
                             const double* k1 = VDER(X, s.dypold, b);
                             const double* k8 = VDER(X, s.dyp, b);
-                            FOR_OWN_W(X, q) {
-                                double kv[11];
-#pragma unroll
-                                for (int j = 2; j <= 10; ++j)
-                                    kv[j] = (j <= i - 1) ? ldcg(&((j == 8) ? k8 : VSTG(X, j, b))[q]) : 0.0;
-                                const double k1q = ldcg(&k1[q]), yoq = ldcg(&yold[q]);
-                                double e = xmul(cB.a[i][1], k1q);
-#pragma unroll
-                                for (int j = 2; j <= 10; ++j) {
-                                    if (j > i - 1) break;
-                                    e = xadd(e, xmul(cB.a[i][j], kv[j]));
-                                }
-                                put_arg(X, argi, b, q, xadd(yoq, xmul(s.h_old, e)));
-                            }
-                            __syncwarp();
+                            IntPtrs ip;
+                            for (int j = 0; j < 11; ++j) ip.k[j] = (j == 8) ? k8 : (j >= 2) ? VSTG(X, j, b) : nullptr;
+                            interp_stage_args(i, yold, k1, ip, arg_dst(X, argi, b), s.h_old, X.lane, X.c0, X.nc);
                             I.tstg = xadd(s.t_old, xmul(cB.c[i], s.h_old));
                             I.argi = argi;
                         }
@@ -440,33 +607,10 @@ MT_DEV void advance(BCtx& X, BInst& I, int b)
                         const double ho = s.h_old;
                         const double* k1 = VDER(X, s.dypold, b);
                         const double* k8 = VDER(X, s.dyp, b);
-                        FOR_OWN_W(X, q) {
-                            const double K1 = ldcg(&k1[q]), K3 = ldcg(&VSTG(X, 3, b)[q]), K4 = ldcg(&VSTG(X, 4, b)[q]);
-                            const double K5 = ldcg(&VSTG(X, 5, b)[q]), K6 = ldcg(&VSTG(X, 6, b)[q]);
-                            const double K7 = ldcg(&VSTG(X, 7, b)[q]), K8 = ldcg(&k8[q]), K9 = ldcg(&VSTG(X, 9, b)[q]);
-                            const double K10 = ldcg(&VSTG(X, 10, b)[q]), K11 = ldcg(&VSTG(X, 11, b)[q]);
-#define R(i, j) cB.r[i][j]
-#define M(a, b2) xmul(a, b2)
-#define A(a, b2) xadd(a, b2)
-                            const double p5 = A(A(M(R(5, 6), K5), A(A(M(R(10, 6), K10), M(R(8, 6), K8)), A(M(R(7, 6), K7), M(R(6, 6), K6)))),
-                                                A(A(A(M(R(4, 6), K4), M(R(9, 6), K9)), A(M(R(3, 6), K3), M(R(11, 6), K11))), M(R(1, 6), K1)));
-                            const double p4 = A(A(A(M(R(10, 5), K10), M(R(9, 5), K9)), A(A(M(R(7, 5), K7), M(R(6, 5), K6)), M(R(5, 5), K5))),
-                                                A(A(A(M(R(4, 5), K4), M(R(8, 5), K8)), A(M(R(3, 5), K3), M(R(11, 5), K11))), M(R(1, 5), K1)));
-                            const double p3 = A(A(A(A(M(R(4, 4), K4), M(R(8, 4), K8)), A(M(R(7, 4), K7), M(R(6, 4), K6))), M(R(5, 4), K5)),
-                                                A(A(A(M(R(10, 4), K10), M(R(9, 4), K9)), A(M(R(3, 4), K3), M(R(11, 4), K11))), M(R(1, 4), K1)));
-                            const double p2 = A(A(A(M(R(5, 3), K5), M(R(6, 3), K6)),
-                                                  A(A(A(M(R(3, 3), K3), M(R(9, 3), K9)), A(M(R(10, 3), K10), M(R(8, 3), K8))), M(R(1, 3), K1))),
-                                                A(A(M(R(4, 3), K4), M(R(11, 3), K11)), M(R(7, 3), K7)));
-                            const double p1 = A(A(A(M(R(5, 2), K5), A(A(M(R(6, 2), K6), M(R(8, 2), K8)), M(R(1, 2), K1))),
-                                                  A(A(M(R(3, 2), K3), M(R(9, 2), K9)), M(R(10, 2), K10))),
-                                                A(A(M(R(4, 2), K4), M(R(11, 2), K11)), M(R(7, 2), K7)));
-#undef R
-#undef M
-#undef A
-                            VP(X, 5, b)[q] = xmul(ho, p5); VP(X, 4, b)[q] = xmul(ho, p4); VP(X, 3, b)[q] = xmul(ho, p3);
-                            VP(X, 2, b)[q] = xmul(ho, p2); VP(X, 1, b)[q] = xmul(ho, p1);
-                        }
-                        __syncwarp();
+                        PolyPtrs pp;
+                        for (int j = 0; j < 12; ++j) pp.k[j] = (j == 1) ? k1 : (j == 8) ? k8 : (j >= 3) ? VSTG(X, j, b) : nullptr;
+                        for (int j = 0; j < 6; ++j) pp.p[j] = (j >= 1) ? VP(X, j, b) : nullptr;
+                        interp_coeffs(pp, ho, X.lane, X.P.n, X.c0, X.nc);
                         s.intrp_ready = 1;
                     }
                 }
@@ -476,15 +620,10 @@ MT_DEV void advance(BCtx& X, BInst& I, int b)
                     const double* yp = VDER(X, s.dyp, b);
                     double* dst = I.dst_slot ? X.F.y_out ? X.F.y_out + ((size_t)b * X.Q.nt + s.ko) * X.n3 : VONE(X, X.F.ystep, b)
                                              : VONE(X, X.F.ystep, b);
-                    FOR_OWN_W(X, q) {
-                        double v = xmul(ldcg(&VP(X, 5, b)[q]), sigma);
-                        v = xmul(xadd(v, ldcg(&VP(X, 4, b)[q])), sigma);
-                        v = xmul(xadd(v, ldcg(&VP(X, 3, b)[q])), sigma);
-                        v = xmul(xadd(v, ldcg(&VP(X, 2, b)[q])), sigma);
-                        v = xmul(xadd(v, ldcg(&VP(X, 1, b)[q])), sigma);
-                        dst[q] = xadd(xmul(xadd(v, xmul(s.h_old, ldcg(&yp[q]))), sigma), ldcg(&y[q]));
-                    }
-                    __syncwarp();
+                    PolyPtrs pp;
+                    for (int j = 0; j < 12; ++j) pp.k[j] = nullptr;
+                    for (int j = 0; j < 6; ++j) pp.p[j] = (j >= 1) ? VP(X, j, b) : nullptr;
+                    interp_eval(pp, y, yp, dst, sigma, s.h_old, X.lane, X.P.n, X.c0, X.nc);
                     I.t_got = I.t_want;
                 }
                 break;
@@ -884,26 +1023,9 @@ MT_DEV void advance(BCtx& X, BInst& I, int b)
                             const double* k8 = VDER(X, s.d8, b);
                             double* es = X.F.errest + (size_t)b * X.n3;
                             double* w = X.F.weights + (size_t)b * X.n3;
-                            double lm = 0.0;
-                            FOR_OWN_W(X, q) {
-                                double kv[8];
-#pragma unroll
-                                for (int i = 2; i <= 7; ++i) kv[i] = ldcg(&VSTG(X, i, b)[q]);
-                                const double esq = ldcg(&es[q]), ypq = ldcg(&yp[q]), k8q = ldcg(&k8[q]);
-                                double v = esq;
-                                v = xsub(v, xmul(cB.b[1], ypq));
-#pragma unroll
-                                for (int i = 2; i <= 7; ++i) {
-                                    if (cB.b[i] == 0.0) continue;
-                                    v = xsub(v, xmul(cB.b[i], kv[i]));
-                                }
-                                v = xsub(v, xmul(cB.b[8], k8q));
-                                v = xmul(I.htry, v);
-                                es[q] = v;
-                                const double wq = fmax(xmul(0.5, xadd(fabs(ldcg(&y[q])), fabs(ldcg(&yn[q])))), thr);
-                                w[q] = wq;
-                                lm = fmax(lm, fabs(v) / wq);
-                            }
+                            ErrPtrs ep;
+                            for (int j = 0; j < 8; ++j) ep.k[j] = (j >= 2) ? VSTG(X, j, b) : nullptr;
+                            double lm = step_error(ep, y, yp, yn, k8, es, w, I.htry, thr, X.lane, X.P.n, X.c0, X.nc);
                             post_reduce(X, I, b, &lm, 1, true);
                         }
                         CO_YIELD(I, L_FINAL);
