@@ -1240,6 +1240,67 @@ MT_DEV void epilogue_cell(const BCtx& X, int b, const TimeScalars& ts, int arg, 
     out[i] = o[0]; out[n + i] = o[1]; out[2 * n + i] = o[2];
 }
 
+// request of one instance in the LL epilogue: the field and damping at its time, the
+// argument and the destination
+struct ReqDesc { TimeScalars ts; int on, arg, dst, pad; };
+
+// LL epilogue of the int8 backend over the CTA's requesting instances.  Thread t keeps
+// cell t % 128 of the block, with the cell's constants loaded once, and takes every
+// fourth requesting instance; all loads of one (instance, cell) are in flight together.
+// The arithmetic is that of the per-cell form (cell_rhs_h with the exact demag field).
+MT_DEV void epilogue_i8(const BCtx& X, const ReqDesc* req, int* eli, int* s_nel)
+{
+    static_assert(kBatchThreads % kCellBlock == 0, "whole cell blocks of threads");
+    constexpr int kGroups = kBatchThreads / kCellBlock;
+    const int tid = threadIdx.x, cell = tid % kCellBlock, g = tid / kCellBlock;
+    const int n = X.P.n;
+    if (tid == 0) {
+        int k = 0;
+        for (int li = 0; li < X.ni; ++li)
+            if (req[li].on) eli[k++] = li;
+        *s_nel = k;
+    }
+    __syncthreads();
+    const int nel = *s_nel;
+    if (cell >= X.nc) return;
+    const int i = X.c0 + cell;
+    double rs[3], ac[7];
+    int lr[3];
+    const double ms = (double)__ldg(&X.P.Mfact[i]), jf = __ldg(&X.P.Jfact[i]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        rs[a] = __ldg(&X.Q.row_scale[a * X.Q.np + i]);
+        lr[a] = (a * X.Q.np + i) & 127;
+    }
+    aniso_load(X.P, i, ac);
+    for (int le = g; le < nel; le += kGroups) {
+        const int li = eli[le], b = X.i0 + li;
+        const int k = compact_pos(X, b), lj = k % kI8N, jl = k / kI8N - X.jb0;
+        const double* m = VPOOL(X, req[li].arg, b);
+        long long hv[3][6];
+        double o[3][7];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            i8_tile_load(X.F.part, X.Q.maxseg, X.cov[a * 3 + jl], lr[a], lj, hv[a]);
+            lap_load(X.P, m + (size_t)a * n, i, o[a]);
+        }
+        const TimeScalars& ts = req[li].ts;
+        double he[3], hk[3], out[3];
+        aniso_from(ac, o[0][3], o[1][3], o[2][3], hk);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const double h = i8_tile_finish(X.F.part, X.Q.maxseg, X.cov[a * 3 + jl], lr[a], lj, hv[a]);
+            const double hm = xmul(-ms, xmul(h, rs[a]));
+            const double hj = xmul(xmul(-2.0, lap_from(X.P, o[a], i)), jf);
+            const double hh = -(a == 0 ? ts.hx : a == 1 ? ts.hy : ts.hz);
+            he[a] = xadd(xadd(xadd(hh, hj), hm), hk[a]);
+        }
+        ll_from_heff(X.P, o[0][3], o[1][3], o[2][3], he, ts.alpha, out);
+        double* d = dst_ptr(X, req[li].dst, b);
+        d[i] = out[0]; d[n + i] = out[1]; d[2 * n + i] = out[2];
+    }
+}
+
 // ---------------------------------------------------------------------------
 // FP32 SIMT demag tile: H[s][inst][a][cell] for cells of block cb, instances of
 // block ib, sources of split s, from the cell-row FP32 tensor.
@@ -1402,8 +1463,8 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
     X.smem = smem_raw;
     const bool i8 = Q.prec == kPrecI8;
     const bool tc = Q.prec != kPrecFP32 && !i8;
-    struct ReqDesc { TimeScalars ts; int on, arg, dst, pad; };
     __shared__ ReqDesc s_req[kInstBlock];
+    __shared__ int s_eli[kInstBlock], s_nel;
     TcState tcs;
     tcs.kb_done = 0; tcs.tiles = 0; tcs.tmem = 0;
     if (tc) tc_init_impl(X.smem, tcs);
@@ -1594,10 +1655,14 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
             }
         }
         __syncthreads();
-        for (int e = threadIdx.x; e < X.ni * X.nc; e += blockDim.x) {
-            const int li = e / X.nc, cell = e - li * X.nc;
-            if (!s_req[li].on) continue;
-            epilogue_cell(X, X.i0 + li, s_req[li].ts, s_req[li].arg, s_req[li].dst, X.c0 + cell);
+        if (i8) {
+            epilogue_i8(X, s_req, s_eli, &s_nel);
+        } else {
+            for (int e = threadIdx.x; e < X.ni * X.nc; e += blockDim.x) {
+                const int li = e / X.nc, cell = e - li * X.nc;
+                if (!s_req[li].on) continue;
+                epilogue_cell(X, X.i0 + li, s_req[li].ts, s_req[li].arg, s_req[li].dst, X.c0 + cell);
+            }
         }
         __syncthreads();
         for (int k = 0; k < mine; ++k)   // served: the next tick resumes these coroutines

@@ -659,25 +659,40 @@ MT_DEV bool tc_i8_streamk(unsigned char* smem, const FT& F, long long* part, int
 
 // exact demag sum of row lr of a tile for instance lj, rounded once to double:
 // the hi and lo parts of the slots of the CTAs cv.first..cv.last that cover the
-// tile are summed exactly in int64 and combined as RN(2^24 hi + lo)
-MT_DEV double i8_tile_sum(const long long* part, int maxseg, const SkCover& cv, int lr, int lj)
+// tile are summed exactly in int64 and combined as RN(2^24 hi + lo).
+// i8_tile_load issues the loads of the first three covering slots (most tiles have
+// at most three; slots past the last cover are not loaded), i8_tile_finish adds the
+// rest and rounds.
+MT_DEV void i8_tile_load(const long long* part, int maxseg, const SkCover& cv, int lr, int lj, long long v[6])
 {
     const size_t off = (size_t)lj * 128 + (size_t)lr, lo = (size_t)kI8N * 128;
     const long long* p0 = part + ((size_t)cv.first * maxseg + (size_t)cv.jf) * kI8SlotElems + off;
-    // the first three covering slots are loaded together (most tiles have at most three)
-    const int c1 = cv.first + 1 <= cv.last ? cv.first + 1 : cv.first;
-    const int c2 = cv.first + 2 <= cv.last ? cv.first + 2 : cv.first;
-    const long long* p1 = (c1 != cv.first) ? part + (size_t)c1 * maxseg * kI8SlotElems + off : p0;
-    const long long* p2 = (c2 != cv.first) ? part + (size_t)c2 * maxseg * kI8SlotElems + off : p0;
-    const long long h0 = __ldcg(p0), l0 = __ldcg(p0 + lo), h1 = __ldcg(p1), l1 = __ldcg(p1 + lo);
-    const long long h2 = __ldcg(p2), l2 = __ldcg(p2 + lo);
-    long long hi_s = h0, lo_s = l0;
-    if (c1 != cv.first) { hi_s += h1; lo_s += l1; }
-    if (c2 != cv.first) { hi_s += h2; lo_s += l2; }
+    const bool has1 = cv.first + 1 <= cv.last, has2 = cv.first + 2 <= cv.last;
+    const long long* p1 = part + (size_t)(cv.first + 1) * maxseg * kI8SlotElems + off;
+    const long long* p2 = part + (size_t)(cv.first + 2) * maxseg * kI8SlotElems + off;
+    v[0] = __ldcg(p0);
+    v[1] = __ldcg(p0 + lo);
+    v[2] = has1 ? __ldcg(p1) : 0ll;
+    v[3] = has1 ? __ldcg(p1 + lo) : 0ll;
+    v[4] = has2 ? __ldcg(p2) : 0ll;
+    v[5] = has2 ? __ldcg(p2 + lo) : 0ll;
+}
+
+MT_DEV double i8_tile_finish(const long long* part, int maxseg, const SkCover& cv, int lr, int lj, const long long v[6])
+{
+    const size_t off = (size_t)lj * 128 + (size_t)lr, lo = (size_t)kI8N * 128;
+    long long hi_s = v[0] + v[2] + v[4], lo_s = v[1] + v[3] + v[5];
     for (int c = cv.first + 3; c <= cv.last; ++c) {
         const long long* pc = part + (size_t)c * maxseg * kI8SlotElems + off;
         hi_s += __ldcg(pc);
         lo_s += __ldcg(pc + lo);
     }
     return __dadd_rn(__dmul_rn((double)hi_s, 16777216.0), (double)lo_s);
+}
+
+MT_DEV double i8_tile_sum(const long long* part, int maxseg, const SkCover& cv, int lr, int lj)
+{
+    long long v[6];
+    i8_tile_load(part, maxseg, cv, lr, lj, v);
+    return i8_tile_finish(part, maxseg, cv, lr, lj, v);
 }

@@ -79,8 +79,23 @@ MT_DEV TimeScalars time_scalars(const DevProb& P, double t)
 // Neumann Laplacian of one component at cell i (ComputeExchangeTerm3D_Uniform,
 // LandauLifshitzEquationSolver.f90:1194-1522): merged diagonal plus the
 // neighbour terms in increasing column order.  v is read through L2 because
-// other CTAs wrote it during the same launch.
-MT_DEV double lap_cell_dev(const DevProb& P, const double* v, int i)
+// other CTAs wrote it during the same launch.  lap_load issues the loads (only
+// of neighbours that exist, all in flight together: o = z0 y0 x0 c x1 y1 z1),
+// lap_from sums them.
+MT_DEV void lap_load(const DevProb& P, const double* v, int i, double o[7])
+{
+    const int nx = P.nx, ny = P.ny, nz = P.nz;
+    const int ix = i % nx, iy = (i / nx) % ny, iz = i / (nx * ny);
+    o[0] = (nz > 1 && iz > 0) ? ldcg(&v[i - nx * ny]) : 0.0;
+    o[1] = (ny > 1 && iy > 0) ? ldcg(&v[i - nx]) : 0.0;
+    o[2] = (nx > 1 && ix > 0) ? ldcg(&v[i - 1]) : 0.0;
+    o[3] = ldcg(&v[i]);
+    o[4] = (nx > 1 && ix < nx - 1) ? ldcg(&v[i + 1]) : 0.0;
+    o[5] = (ny > 1 && iy < ny - 1) ? ldcg(&v[i + nx]) : 0.0;
+    o[6] = (nz > 1 && iz < nz - 1) ? ldcg(&v[i + nx * ny]) : 0.0;
+}
+
+MT_DEV double lap_from(const DevProb& P, const double o[7], int i)
 {
     const int nx = P.nx, ny = P.ny, nz = P.nz;
     const int ix = i % nx, iy = (i / nx) % ny, iz = i / (nx * ny);
@@ -89,14 +104,8 @@ MT_DEV double lap_cell_dev(const DevProb& P, const double* v, int i)
     double dgz = (nz > 1) ? ((iz == 0 || iz == nz - 1) ? P.diag_b[2] : P.diag_i[2]) : 0.0;
     double diag = xadd(dgx, dgy);
     if (nz > 1) diag = xadd(diag, dgz);
-    // which neighbours exist; every value is loaded up front (an absent neighbour
-    // loads the cell itself and is not used), so the loads are in flight together
     const bool hz0 = nz > 1 && iz > 0, hy0 = ny > 1 && iy > 0, hx0 = nx > 1 && ix > 0;
     const bool hx1 = nx > 1 && ix < nx - 1, hy1 = ny > 1 && iy < ny - 1, hz1 = nz > 1 && iz < nz - 1;
-    const double vz0 = ldcg(&v[hz0 ? i - nx * ny : i]), vy0 = ldcg(&v[hy0 ? i - nx : i]);
-    const double vx0 = ldcg(&v[hx0 ? i - 1 : i]), vc = ldcg(&v[i]);
-    const double vx1 = ldcg(&v[hx1 ? i + 1 : i]), vy1 = ldcg(&v[hy1 ? i + nx : i]);
-    const double vz1 = ldcg(&v[hz1 ? i + nx * ny : i]);
     double s = 0.0;
     bool first = true;
 #define MT_ACC(term)                              \
@@ -105,15 +114,64 @@ MT_DEV double lap_cell_dev(const DevProb& P, const double* v, int i)
         if (first) { s = _t; first = false; }     \
         else s = xadd(s, _t);                     \
     } while (0)
-    if (hz0) MT_ACC(xmul(P.lapc[2], vz0));
-    if (hy0) MT_ACC(xmul(P.lapc[1], vy0));
-    if (hx0) MT_ACC(xmul(P.lapc[0], vx0));
-    MT_ACC(xmul(diag, vc));
-    if (hx1) MT_ACC(xmul(P.lapc[0], vx1));
-    if (hy1) MT_ACC(xmul(P.lapc[1], vy1));
-    if (hz1) MT_ACC(xmul(P.lapc[2], vz1));
+    if (hz0) MT_ACC(xmul(P.lapc[2], o[0]));
+    if (hy0) MT_ACC(xmul(P.lapc[1], o[1]));
+    if (hx0) MT_ACC(xmul(P.lapc[0], o[2]));
+    MT_ACC(xmul(diag, o[3]));
+    if (hx1) MT_ACC(xmul(P.lapc[0], o[4]));
+    if (hy1) MT_ACC(xmul(P.lapc[1], o[5]));
+    if (hz1) MT_ACC(xmul(P.lapc[2], o[6]));
 #undef MT_ACC
     return s;
+}
+
+MT_DEV double lap_cell_dev(const DevProb& P, const double* v, int i)
+{
+    double o[7];
+    lap_load(P, v, i, o);
+    return lap_from(P, o, i);
+}
+
+// anisotropy field of one cell: -2 K0/(mu0 Ms) (u u^T) m.  aniso_load reads the cell's
+// constants (K0/(mu0 Ms), then u u^T as xx xy xz yy yz zz), aniso_from applies them.
+MT_DEV void aniso_load(const DevProb& P, int i, double c[7])
+{
+    const int n = P.n;
+    c[0] = __ldg(&P.Kfact[i]);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) c[1 + k] = __ldg(&P.A6[k * (size_t)n + i]);
+}
+
+MT_DEV void aniso_from(const double c[7], double mx, double my, double mz, double hk[3])
+{
+    const double k2 = xmul(-2.0, c[0]);
+    const double axx = c[1], axy = c[2], axz = c[3], ayy = c[4], ayz = c[5], azz = c[6];
+    hk[0] = xmul(k2, xadd(xadd(xmul(axx, mx), xmul(axy, my)), xmul(axz, mz)));
+    hk[1] = xmul(k2, xadd(xadd(xmul(axy, mx), xmul(ayy, my)), xmul(ayz, mz)));
+    hk[2] = xmul(k2, xadd(xadd(xmul(axz, mx), xmul(ayz, my)), xmul(azz, mz)));
+}
+
+MT_DEV void aniso_field(const DevProb& P, int i, double mx, double my, double mz, double hk[3])
+{
+    double c[7];
+    aniso_load(P, i, c);
+    aniso_from(c, mx, my, mz, hk);
+}
+
+// dm/dt from m and the effective field he (dmdt_fct :251-271)
+MT_DEV void ll_from_heff(const DevProb& P, double mx, double my, double mz, const double he[3], double alpha,
+                         double out[3])
+{
+    const double cx = xmul(-1.0, xsub(xmul(my, he[2]), xmul(mz, he[1])));
+    const double cy = xmul(-1.0, xsub(xmul(mz, he[0]), xmul(mx, he[2])));
+    const double cz = xmul(-1.0, xsub(xmul(mx, he[1]), xmul(my, he[0])));
+    const double h2x = xsub(xmul(my, cz), xmul(mz, cy));
+    const double h2y = xsub(xmul(mz, cx), xmul(mx, cz));
+    const double h2z = xsub(xmul(mx, cy), xmul(my, cx));
+    const double g = -P.gamma;
+    out[0] = xsub(xmul(g, cx), xmul(alpha, h2x));
+    out[1] = xsub(xmul(g, cy), xmul(alpha, h2y));
+    out[2] = xsub(xmul(g, cz), xmul(alpha, h2z));
 }
 
 // The four internal field terms of one cell (dmdt_fct :239-248).
@@ -128,13 +186,7 @@ MT_DEV CellFields cell_fields_local(const DevProb& P, const double* m, int i, co
     const double jf = __ldg(&P.Jfact[i]);
     for (int a = 0; a < 3; ++a) F.hj[a] = xmul(xmul(-2.0, lap_cell_dev(P, m + (size_t)a * n, i)), jf);
     F.hh[0] = -ts.hx; F.hh[1] = -ts.hy; F.hh[2] = -ts.hz;
-    const double k2 = xmul(-2.0, __ldg(&P.Kfact[i]));
-    const double axx = __ldg(&P.A6[0 * (size_t)n + i]), axy = __ldg(&P.A6[1 * (size_t)n + i]);
-    const double axz = __ldg(&P.A6[2 * (size_t)n + i]), ayy = __ldg(&P.A6[3 * (size_t)n + i]);
-    const double ayz = __ldg(&P.A6[4 * (size_t)n + i]), azz = __ldg(&P.A6[5 * (size_t)n + i]);
-    F.hk[0] = xmul(k2, xadd(xadd(xmul(axx, mx), xmul(axy, my)), xmul(axz, mz)));
-    F.hk[1] = xmul(k2, xadd(xadd(xmul(axy, mx), xmul(ayy, my)), xmul(ayz, mz)));
-    F.hk[2] = xmul(k2, xadd(xadd(xmul(axz, mx), xmul(ayz, my)), xmul(azz, mz)));
+    aniso_field(P, i, mx, my, mz, F.hk);
     return F;
 }
 
@@ -155,16 +207,7 @@ MT_DEV void cell_rhs_from(const DevProb& P, const double* m, int i, const CellFi
     const double mx = ldcg(&m[i]), my = ldcg(&m[n + i]), mz = ldcg(&m[2 * n + i]);
     double he[3];
     for (int a = 0; a < 3; ++a) he[a] = xadd(xadd(xadd(F.hh[a], F.hj[a]), F.hm[a]), F.hk[a]);
-    const double cx = xmul(-1.0, xsub(xmul(my, he[2]), xmul(mz, he[1])));
-    const double cy = xmul(-1.0, xsub(xmul(mz, he[0]), xmul(mx, he[2])));
-    const double cz = xmul(-1.0, xsub(xmul(mx, he[1]), xmul(my, he[0])));
-    const double h2x = xsub(xmul(my, cz), xmul(mz, cy));
-    const double h2y = xsub(xmul(mz, cx), xmul(mx, cz));
-    const double h2z = xsub(xmul(mx, cy), xmul(my, cx));
-    const double g = -P.gamma;
-    out[0] = xsub(xmul(g, cx), xmul(ts.alpha, h2x));
-    out[1] = xsub(xmul(g, cy), xmul(ts.alpha, h2y));
-    out[2] = xsub(xmul(g, cz), xmul(ts.alpha, h2z));
+    ll_from_heff(P, mx, my, mz, he, ts.alpha, out);
 }
 
 MT_DEV void cell_rhs(const DevProb& P, const double* m, int i, const float S[3], const TimeScalars& ts,
