@@ -31,8 +31,14 @@ regions ("scaling": "strong").
 
 Multi-GPU: one process per GPU (torchrun); instances are sharded across ranks
 with no data-path collective ("scaling": "weak"); the step time is the max over
-ranks.  --impl reference times the CPU restatement of the reference (oracle/,
-OpenMP on all host cores) on the same workload, rank 0 only.
+ranks.  --impl reference times the CPU restatement of the reference (oracle/)
+on the same workload, rank 0 only: the instances side by side on the host cores,
+one single-threaded process each, as the reference runs one problem per thread.
+
+Besides the headline, the default film-batch line carries the FP64 error of
+<m>(t) for a seeded sample of instances ("m_err_vs_fp64"), the large-plain HBM
+record ("large_plain") and the split 16-bit product next to int8 on a short
+window ("split16_short_window").
 """
 from __future__ import annotations
 
@@ -89,6 +95,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="film-batch: skip the FP64 error statement")
     ap.add_argument("--no-large", action="store_true", help="film-batch: skip the large-plain sub-record")
     ap.add_argument("--no-tune", action="store_true", help="film-batch: keep the default GEMM schedule")
+    ap.add_argument("--no-split16", action="store_true",
+                    help="film-batch: skip the short-window record of the split 16-bit product")
     ap.add_argument("--shards", type=int, default=1,
                     help="large-plain: row shards of the one instance (over the ranks when --gpus > 1)")
     ap.add_argument("--res", type=int, nargs=3, default=None,
@@ -476,6 +484,44 @@ def large_plain_record(torch, hbm, src, local, reps=3):
             "clocks": clocks}
 
 
+def split16_record(torch, res, L, m_s, fields, window_ns=0.02, precisions=("fp16s", "int8")):
+    """The split 16-bit form of the batched product next to int8 on the same instances
+    over a short window: simulated ns/s from device time, RHS evaluations per instance.
+    FP32-level rounding in the 16-bit sums sets the step size of the weakest-field
+    instances, so the lock-step batch runs at their pace."""
+    from magtense_b200 import BatchSolver
+    B = len(fields)
+    win = window_ns * 1e-9
+    t = np.linspace(0, win, int(round(window_ns / 1e-3)) + 1)
+    hext = np.zeros((B, 2, 4))
+    hext[:, 1, 0] = win
+    hext[:, :, 1:] = fields[:, None, :]
+    m0 = m_s.unsqueeze(0).expand(B, -1).contiguous()
+    out = {}
+    for prec in precisions:
+        bs = BatchSolver(res, L, B, precision=prec)
+        try:
+            bs.assemble()
+            bs.set_dynamics(hext=hext, alpha=GAMMA * 0.02, gamma=GAMMA)
+            bs.integrate(t, m0, tol=1e-6)   # warm-up
+            torch.cuda.synchronize()
+            _, y, _, st = bs.integrate(t, m0, tol=1e-6)
+            torch.cuda.synchronize()
+            del y
+        finally:
+            bs.close()
+        ev = [x["f_evals"] for x in st]
+        kms = st[0]["kernel_ms"]
+        out[prec] = {"value": B * window_ns / (kms / 1e3), "unit": "simulated ns/s", "kernel_ms": kms,
+                     "rhs_evals_per_instance": {"min": int(min(ev)), "median": float(np.median(ev)),
+                                                "max": int(max(ev))}}
+    out["window_ns"] = window_ns
+    out["note"] = (f"{B} instances of the headline set over {window_ns} ns from the same s-state, device time of "
+                   "one integration after a warm-up; the 16-bit split product accumulates in FP32, whose rounding "
+                   "noise sets the step size of the weakest-field instances")
+    return out
+
+
 def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
     from magtense_b200 import BatchSolver
     res, L = FILM_RES, FILM_L
@@ -602,6 +648,9 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
                     "the FP64 tensor and FP64 demag product, same s-state, field and tolerances, run after timing"}
     if not args.no_large:
         line["large_plain"] = large_plain_record(torch, hbm, src, local)
+    if not args.no_split16 and args.precision == "int8":
+        bs.close()
+        line["split16_short_window"] = split16_record(torch, res, L, m_s, fields)
     return line
 
 

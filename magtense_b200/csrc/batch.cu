@@ -214,7 +214,7 @@ __device__ __noinline__ double stage_args(int i, const double* __restrict__ y, c
                                           StgPtrs st, double* __restrict__ es, ArgDst d, double htry, double thr,
                                           int lane, int c0, int nc)
 {
-    constexpr int U = 3;   // elements per lane in flight
+    constexpr int U = 2;   // elements per lane in flight
     double lm = 0.0;
     const int n = d.n, tot = 3 * nc;
     for (int e0 = lane; e0 < tot; e0 += 32 * U) {
@@ -263,9 +263,11 @@ __device__ __noinline__ double stage_args(int i, const double* __restrict__ y, c
 }
 
 // The other per-element loops of a step, written like stage_args: non-inlined, plain
-// pointers, three elements per lane in flight, each element's arithmetic in the same
-// order as the synchronous formulation (and the oracle).
-constexpr int kInFlight = 3;
+// pointers, kInFlight elements per lane in flight, each element's arithmetic in the same
+// order as the synchronous formulation (and the oracle).  Two measured faster than one,
+// three or six (the stage-argument loop too): more loads in flight per lane slowed
+// every warp's loop down.
+constexpr int kInFlight = 2;
 
 MT_DEV int own_q(int e, int n, int c0, int nc)
 {
@@ -1443,7 +1445,7 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
     X.ni = owner ? per : 0;
     X.nact = 0;
     X.U = 0;
-    __shared__ int s_act[2 * kMaxIB], s_actpos[2 * kMaxIB], s_nact;
+    __shared__ int s_act[2 * kMaxIB], s_actpos[2 * kMaxIB];
     __shared__ SkCover s_cov[9];
     __shared__ unsigned s_bits[4 * kMaxIB];
     __shared__ int s_pre[4 * kMaxIB + 1];
@@ -1473,8 +1475,9 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
     // fit next to the GEMM's buffers (every lane reads and writes the same, identical
     // values), otherwise one copy per lane in local memory.
     BInst L_loc[kMaxInstPerWarp];
-    BInst* L = Q.inst_smem_off ? reinterpret_cast<BInst*>(smem_raw + Q.inst_smem_off) + (size_t)X.warp * Q.inst_per_warp
-                               : L_loc;
+    BInst* Lsm = Q.inst_smem_off ? reinterpret_cast<BInst*>(smem_raw + Q.inst_smem_off) : nullptr;
+    BInst* L = Lsm ? Lsm + (size_t)X.warp * Q.inst_per_warp : L_loc;
+    __shared__ int s_adv[kInstBlock], s_nadv;
     int mine = 0;
     for (int li = X.warp; li < X.ni && mine < kMaxInstPerWarp; li += X.nwarps, ++mine) {
         const long long* src = reinterpret_cast<const long long*>(&F.inst[(size_t)X.cb * Q.Bp + X.i0 + li]);
@@ -1556,13 +1559,42 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
     // instances.  Requests still pending when a launch ends are served by the next.
     for (long long tick = 0; ok; ++tick) {
         const uint64_t t_tick = prof ? globaltimer_ns() : 0;
-        for (int k = 0; k < mine; ++k) {
-            BInst& I = L[k];
-            const int b = X.i0 + X.warp + k * X.nwarps;
-            if (b >= Q.B || I.req != 0) continue;
-            const uint64_t ta = (F.prof && t == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0;
-            ADVANCE_TO_REQUEST(X, I, b);
-            if (ta) { atomicAdd(&F.prof[27], globaltimer_ns() - ta); atomicAdd(&F.prof[28], 1ull); }
+        if (Lsm) {
+            // Every coroutine of the CTA is in shared memory: the ones to advance are dealt to
+            // the warps in index order, so a thinned-out set still keeps every warp busy.  The
+            // order is the same in every cell-block copy of the instances (their states are
+            // identical), so the in-place reductions wait on copies that run in the same order.
+            __syncthreads();
+            if (X.warp == 0) {
+                int cnt = 0;
+                for (int c = 0; c < X.ni; c += 32) {
+                    const int li = c + X.lane;
+                    const bool need = li < X.ni && X.i0 + li < Q.B &&
+                                      Lsm[(li % X.nwarps) * Q.inst_per_warp + li / X.nwarps].req == 0;
+                    const unsigned bal = __ballot_sync(0xffffffffu, need);
+                    if (need) s_adv[cnt + __popc(bal & ((1u << X.lane) - 1u))] = li;
+                    cnt += __popc(bal);
+                }
+                if (X.lane == 0) s_nadv = cnt;
+            }
+            __syncthreads();
+            for (int j = X.warp; j < s_nadv; j += X.nwarps) {
+                const int li = s_adv[j];
+                BInst& I = Lsm[(li % X.nwarps) * Q.inst_per_warp + li / X.nwarps];
+                const uint64_t ta = (F.prof && t == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0;
+                ADVANCE_TO_REQUEST(X, I, X.i0 + li);
+                if (ta) { atomicAdd(&F.prof[27], globaltimer_ns() - ta); atomicAdd(&F.prof[28], 1ull); }
+            }
+            __syncthreads();
+        } else {
+            for (int k = 0; k < mine; ++k) {
+                BInst& I = L[k];
+                const int b = X.i0 + X.warp + k * X.nwarps;
+                if (b >= Q.B || I.req != 0) continue;
+                const uint64_t ta = (F.prof && t == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0;
+                ADVANCE_TO_REQUEST(X, I, b);
+                if (ta) { atomicAdd(&F.prof[27], globaltimer_ns() - ta); atomicAdd(&F.prof[28], 1ull); }
+            }
         }
         if (tick >= Q.ticks_per_launch) break;
         publish_requests(L, mine, X, W, i8, tick);
