@@ -1901,6 +1901,7 @@ int batch_grid(int n, int B, int num_sms, int prec, int* CB, int* IB, int* S)
     int s = num_sms / tiles;
     if (s > 4) s = 4;
     if (s < 1) s = 1;
+    if (s == 3) s = 2;   // every split owns kInstBlock / s instances: s divides 128
     // the source range of every split is a whole number of 32-wide k-blocks
     const int Kd = 3 * (*CB) * kCellBlock;
     while (s > 1 && (Kd % (32 * s)) != 0) --s;

@@ -224,3 +224,41 @@ def test_gemm_schedules_are_bit_exact_and_tuned(torch_cuda, oracle):
         Hm = P2.fields(0.0, m[b])[3].reshape(-1)
         assert np.array_equal(H0[b], Hm), b
     bs.close()
+
+
+def test_every_instance_owned_when_blocks_split_unevenly(torch_cuda):
+    """300 film instances (n = 1600): 13 x 3 tiles, so 148 SMs would allow three splits
+    of each 128-instance block; the splits must divide the block (two here), or the
+    last instances of every block have no coroutine owner.  Instances at the ends of
+    the blocks follow the same bits as the same instances integrated in a small batch
+    (the exact product makes every instance independent of the others)."""
+    from magtense_b200 import BatchSolver
+    res, L = [80, 20, 1], [500e-9, 125e-9, 3e-9]
+    n, B = 1600, 300
+    rng = np.random.default_rng(21)
+    ang = rng.uniform(0, 2 * np.pi, B)
+    mag = rng.uniform(5e-3, 50e-3, B) / MU0
+    Hf = np.stack([mag * np.cos(ang), mag * np.sin(ang), np.zeros(B)], 1)
+    window = 0.002e-9
+    hext = np.zeros((B, 2, 4))
+    hext[:, 1, 0] = window
+    hext[:, :, 1:] = Hf[:, None, :]
+    m0 = unit_states(n, B, 22)
+    t = np.linspace(0, window, 3)
+    bs = BatchSolver(res, L, B, precision="int8")
+    bs.assemble()
+    bs.set_dynamics(hext=hext, alpha=GAMMA * 0.02, gamma=GAMMA)
+    t_out, y, _, stats = bs.integrate(t, torch_cuda.as_tensor(m0.reshape(B, -1), device="cuda"), tol=1e-6)
+    y = y.cpu().numpy()
+    bs.close()
+    assert all(s["f_evals"] > 0 and s["status"] == 0 for s in stats)
+    pick = [0, 126, 127, 255, 299]
+    sb = BatchSolver(res, L, len(pick), precision="int8")
+    sb.assemble()
+    sb.set_dynamics(hext=hext[pick], alpha=GAMMA * 0.02, gamma=GAMMA)
+    t2, y2, _, st2 = sb.integrate(t, torch_cuda.as_tensor(m0[pick].reshape(len(pick), -1), device="cuda"), tol=1e-6)
+    y2 = y2.cpu().numpy()
+    sb.close()
+    for k, b in enumerate(pick):
+        assert stats[b]["f_evals"] == st2[k]["f_evals"], (b, stats[b], st2[k])
+        assert np.array_equal(t_out[b], t2[k]) and np.array_equal(y[b], y2[k]), b
