@@ -749,8 +749,19 @@ struct GroupBack { GridSync gs; RKS st; };
 // relaunched until every group has finished (replayed from a CUDA graph when
 // `graph`).  runs[k]->grid CTAs go to group k.  back receives each group's final
 // barrier and state.
+// Relaunch planning of a ragged batch: after a launch in which instances finished, their
+// CTAs go to the unfinished groups, one at a time to the group with the most demag work
+// (n^2) per CTA, up to cap CTAs each; a group never shrinks, so its shared-memory need
+// stays within the first plan's.  CTAs left over join a finished instance's group, which
+// returns at once.  An instance's trajectory does not depend on its group size.
+struct GroupPlan {
+    std::vector<int> cap;
+    std::vector<double> work;
+    double launch_s = 0.25;   // target device time of one launch per group
+};
+
 int run_groups(const std::vector<IntegRun*>& runs, bool graph, cudaStream_t cs, std::vector<GroupBack>& back_out,
-               long long& launches, double& kernel_ms)
+               long long& launches, double& kernel_ms, const GroupPlan* plan)
 {
     const int ninst = (int)runs.size();
     size_t smem = 0;
@@ -842,6 +853,47 @@ int run_groups(const std::vector<IntegRun*>& runs, bool graph, cudaStream_t cs, 
         }
         if (all) break;
         if (!progress) return fail(MT_ERR_SOLVER, "grouped integrator made no progress");
+        if (plan) {
+            // re-plan when an instance with CTAs of its own has finished
+            bool freed = false;
+            for (int k = 0; k < ninst; ++k)
+                if (back[k].st.finished && tab[k].ncta > 0 && runs[k]->grid > 0) freed = true;
+            if (freed) {
+                std::vector<int> nc(ninst, 0);
+                int given = 0;
+                for (int k = 0; k < ninst; ++k)
+                    if (!back[k].st.finished) { nc[k] = runs[k]->grid; given += nc[k]; }
+                for (; given < used; ++given) {
+                    int j = -1;
+                    double best = 0.0;
+                    for (int k = 0; k < ninst; ++k)
+                        if (!back[k].st.finished && nc[k] < plan->cap[k] && plan->work[k] / nc[k] > best) {
+                            best = plan->work[k] / nc[k];
+                            j = k;
+                        }
+                    if (j < 0) break;
+                    nc[j]++;
+                }
+                int idle_k = -1;
+                for (int k = 0; k < ninst && idle_k < 0; ++k)
+                    if (back[k].st.finished) idle_k = k;
+                nc[idle_k] += used - given;   // some instance has finished, so idle_k >= 0
+                for (int k = 0, c0 = 0; k < ninst; ++k) {
+                    tab[k].cta0 = c0;
+                    tab[k].ncta = nc[k];
+                    for (int j = 0; j < nc[k]; ++j) cta_inst[c0 + j] = k;
+                    c0 += nc[k];
+                    if (!back[k].st.finished && nc[k] != runs[k]->grid) {
+                        const double t_eval = plan->work[k] * 24.0 / (nc[k] * 30.0e9) + 15e-6;
+                        tab[k].Q.evals_per_launch =
+                            std::min(100000LL, std::max(plan->launch_s < 0.25 ? 1LL : 64LL, (long long)(plan->launch_s / t_eval)));
+                    }
+                    runs[k]->grid = back[k].st.finished ? 0 : nc[k];
+                }
+                CUDA_TRY(cudaMemcpyAsync(d_tab, tab.data(), sizeof(RaggedInst) * ninst, cudaMemcpyHostToDevice, s));
+                CUDA_TRY(cudaMemcpyAsync(d_cta, cta_inst.data(), sizeof(int) * used, cudaMemcpyHostToDevice, s));
+            }
+        }
     }
     CUDA_TRY(cudaEventRecord(evc, s));
     CUDA_TRY(cudaStreamWaitEvent(cs, evc, 0));
@@ -953,28 +1005,20 @@ int mt_integrate_ragged(mt_handle* const* hs, int ninst, const double* t, int nt
     }
     const int G = hs[0]->num_sms;
     if (ninst > G) return fail(MT_ERR_UNSUPPORTED, "%d instances exceed the %d SMs of one launch", ninst, G);
-    // CTA groups in proportion to the demag work n^2, at least one CTA, at most n/8
+    // CTA groups for the demag work n^2 per evaluation (at least one CTA, at most n/8): one
+    // CTA each, then every further CTA to the group with the most work per CTA, which
+    // minimises the slowest group's time per evaluation
     std::vector<double> w(ninst);
-    double wsum = 0.0;
-    for (int k = 0; k < ninst; ++k) { w[k] = (double)hs[k]->n * (double)hs[k]->n; wsum += w[k]; }
-    std::vector<int> ncta(ninst), cap(ninst);
-    int used = 0;
-    for (int k = 0; k < ninst; ++k) {
-        cap[k] = integrate_grid_size(hs[k]->n, G);
-        ncta[k] = std::min(cap[k], std::max(1, (int)((double)G * w[k] / wsum)));
-        used += ncta[k];
-    }
-    while (used > G) {   // the floor of one CTA each can overshoot: take from the largest group
-        int j = (int)(std::max_element(ncta.begin(), ncta.end()) - ncta.begin());
-        ncta[j]--; used--;
-    }
-    for (bool grew = true; grew && used < G;) {   // hand out the rest to the most loaded groups
-        grew = false;
+    for (int k = 0; k < ninst; ++k) w[k] = (double)hs[k]->n * (double)hs[k]->n;
+    std::vector<int> ncta(ninst, 1), cap(ninst);
+    for (int k = 0; k < ninst; ++k) cap[k] = integrate_grid_size(hs[k]->n, G);
+    for (int used = ninst; used < G; ++used) {
         int j = -1;
         double best = 0.0;
         for (int k = 0; k < ninst; ++k)
             if (ncta[k] < cap[k] && w[k] / ncta[k] > best) { best = w[k] / ncta[k]; j = k; }
-        if (j >= 0) { ncta[j]++; used++; grew = true; }
+        if (j < 0) break;
+        ncta[j]++;
     }
     cudaStream_t cs = (cudaStream_t)stream;
     std::vector<std::unique_ptr<IntegRun>> runs(ninst);
@@ -982,9 +1026,15 @@ int mt_integrate_ragged(mt_handle* const* hs, int ninst, const double* t, int nt
     for (int k = 0; k < ninst; ++k) {
         runs[k].reset(new IntegRun());
         rp[k] = runs[k].get();
-        if ((rc = integ_prepare(hs[k], t, nt, m0_dev[k], tol, thres, nullptr, 0, 0.0, y_out_dev[k], ncta[k], *runs[k],
+        // the reduction slots for the largest group the instance may get (cap CTAs); the group
+        // starts with ncta CTAs and the shared memory those need
+        if ((rc = integ_prepare(hs[k], t, nt, m0_dev[k], tol, thres, nullptr, 0, 0.0, y_out_dev[k], cap[k], *runs[k],
                                 &stats[k], cs)))
             return rc;
+        runs[k]->grid = ncta[k];
+        runs[k]->smem = integrate_smem_bytes(hs[k]->n, hs[k]->ldk, ncta[k]);
+        if (runs[k]->smem > 227 * 1024)
+            return fail(MT_ERR_UNSUPPORTED, "integrator shared memory %zu exceeds 227 KB", runs[k]->smem);
         // about 0.25 s per launch for this group: 24 n^2 bytes per evaluation over ncta SMs
         const double t_eval = 24.0 * (double)hs[k]->n * (double)hs[k]->ldk / (ncta[k] * 30.0e9) + 15e-6;
         runs[k]->Q.evals_per_launch = std::min(100000LL, std::max(64LL, (long long)(0.25 / t_eval)));
@@ -992,7 +1042,21 @@ int mt_integrate_ragged(mt_handle* const* hs, int ninst, const double* t, int nt
     std::vector<GroupBack> back;
     long long launches = 0;
     double kernel_ms = 0.0;
-    if ((rc = run_groups(rp, (options & MT_RAGGED_GRAPH) != 0, cs, back, launches, kernel_ms))) return rc;
+    GroupPlan plan;
+    plan.cap = cap;
+    if (const char* e = getenv("MT_RAGGED_LAUNCH_S")) {   // device time per launch (tests: many relaunches)
+        const double v = atof(e);
+        if (v > 0.0 && v <= 10.0) {
+            plan.launch_s = v;
+            for (int k = 0; k < ninst; ++k) {
+                const double t_eval = 24.0 * (double)hs[k]->n * (double)hs[k]->ldk / (ncta[k] * 30.0e9) + 15e-6;
+                runs[k]->Q.evals_per_launch = std::min(100000LL, std::max(1LL, (long long)(v / t_eval)));
+            }
+        }
+    }
+    plan.work.resize(ninst);
+    for (int k = 0; k < ninst; ++k) plan.work[k] = (double)hs[k]->n * (double)hs[k]->ldk;
+    if ((rc = run_groups(rp, (options & MT_RAGGED_GRAPH) != 0, cs, back, launches, kernel_ms, &plan))) return rc;
     int worst = MT_OK;
     for (int k = 0; k < ninst; ++k) {
         const int r = integ_finish(*runs[k], back[k].st, t, nt, t_out + (size_t)k * nt, flags ? flags + (size_t)k * nt : nullptr,
@@ -1112,7 +1176,7 @@ int mt_integrate_shards_local(mt_handle* const* hs, int world, const double* t, 
     std::vector<GroupBack> back;
     long long launches = 0;
     double kernel_ms = 0.0;
-    rc = run_groups(rp, false, cs, back, launches, kernel_ms);
+    rc = run_groups(rp, false, cs, back, launches, kernel_ms, nullptr);
     if (rc) {
         for (int r = 0; r < world; ++r) mark_broken(hs[r]);
         return rc;
