@@ -98,6 +98,10 @@ struct mt_handle {
     std::chrono::steady_clock::time_point shard_broken_at;   // when a run of this rank gave up
     ShardLink* shard_link = nullptr;                // device copy of the link
     long long shard_xseq = 0, shard_rseq = 0;       // barrier and reduction counts after the last run
+    // device buffers of an integration, kept between calls (one integration at a time)
+    unsigned char* integ_arena = nullptr;
+    size_t integ_arena_bytes = 0;
+    bool integ_arena_busy = false;
 };
 
 namespace {
@@ -233,6 +237,7 @@ int mt_destroy(mt_handle* h)
     for (int p = 0; p < kMaxShards; ++p)
         if (h->shard_ipc[p]) cudaIpcCloseMemHandle(h->shard_peer[p]);
     free_ptr(h->shard_region); free_ptr(h->shard_link);
+    free_ptr(h->integ_arena);
     delete h;
     return MT_OK;
 }
@@ -510,11 +515,31 @@ int mt_rhs_vjp(mt_handle* h, double t, const double* m_dev, const double* lam_de
 
 namespace {
 
+// Device buffers of one call.  Bound to a handle (bind), they come from the handle's
+// arena, kept between calls; what does not fit is allocated separately, and the arena is
+// grown to the whole amount when the call ends, so repeated calls allocate nothing.  A
+// handle lends its arena to one integration at a time.
 struct IntegAlloc {
     std::vector<void*> ptrs;
+    mt_handle* h = nullptr;
+    size_t used = 0, want = 0;
+    void bind(mt_handle* hh)
+    {
+        if (hh->integ_arena_busy) return;
+        hh->integ_arena_busy = true;
+        h = hh;
+    }
     template <typename T>
     cudaError_t get(T** p, size_t count)
     {
+        if (count == 0) count = 1;
+        const size_t bytes = (sizeof(T) * count + 255) & ~(size_t)255;
+        want += bytes;
+        if (h && used + bytes <= h->integ_arena_bytes) {
+            *p = reinterpret_cast<T*>(h->integ_arena + used);
+            used += bytes;
+            return cudaSuccess;
+        }
         cudaError_t e = dalloc(p, count);
         if (e == cudaSuccess) ptrs.push_back((void*)*p);
         return e;
@@ -522,6 +547,15 @@ struct IntegAlloc {
     ~IntegAlloc()
     {
         for (void* p : ptrs) cudaFree(p);
+        if (!h) return;
+        if (!ptrs.empty()) {   // grow the arena for the next call (the device is idle: cudaFree synchronised)
+            free_ptr(h->integ_arena);
+            h->integ_arena = nullptr;
+            h->integ_arena_bytes = 0;
+            if (cudaMalloc((void**)&h->integ_arena, want) == cudaSuccess) h->integ_arena_bytes = want;
+            else cudaGetLastError();
+        }
+        h->integ_arena_busy = false;
     }
 };
 
@@ -586,6 +620,7 @@ int integ_prepare(mt_handle* h, const double* t, int nt, const double* m0_dev, d
 
     // ---- buffers ----
     IntegAlloc& A = R.A;
+    A.bind(h);
     IntegBufs& B = R.B;
     memset(&B, 0, sizeof(B));
     if (sharded(h)) {   // stage arguments and partials in the exchange region, which peers write into
