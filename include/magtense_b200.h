@@ -271,6 +271,16 @@ int mt_batch_set_schedule(mt_batch* b, const int* ctas, const int* order, int n_
 int mt_batch_integrate(mt_batch* b, const double* t, int nt, const double* m0_dev, double tol, double thres,
                        const double* t_conv, int nt_conv, double conv_tol, double* t_out, double* y_out_dev,
                        int* flags, mt_stats* stats, void* stream);
+/* the same, with the trajectories also delivered to page-locked host memory y_out_host
+ * ([B][nt][3n] FP64), as the reference returns M(t) in host arrays
+ * (MagTenseMicroMagPyIO.f90:200-206, the intent(out) M of runMicroMagSimulation): after
+ * every relaunch of the persistent kernel the samples that all unfinished instances have
+ * passed are copied there on a stream of their own while the next launch runs.
+ * y_out_dev is still required as the device copy.  MT_ERR_ARG if y_out_host is not
+ * page-locked. */
+int mt_batch_integrate_host(mt_batch* b, const double* t, int nt, const double* m0_dev, double tol, double thres,
+                            const double* t_conv, int nt_conv, double conv_tol, double* t_out, double* y_out_dev,
+                            double* y_out_host, int* flags, mt_stats* stats, void* stream);
 /* demag field of all instances with the batch's precision: H_dev = -Ms K m, B*3n FP64 */
 int mt_batch_demag_field(mt_batch* b, const double* m_dev, double* H_dev, void* stream);
 

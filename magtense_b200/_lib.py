@@ -90,6 +90,8 @@ SIGNATURES = {
     "mt_batch_assemble_demag": [VP, VP],
     "mt_batch_integrate": [VP, D, C.c_int, VP, C.c_double, C.c_double, D, C.c_int, C.c_double, D, VP, I,
                            C.POINTER(Stats), VP],
+    "mt_batch_integrate_host": [VP, D, C.c_int, VP, C.c_double, C.c_double, D, C.c_int, C.c_double, D, VP, VP,
+                                I, C.POINTER(Stats), VP],
     "mt_batch_demag_field": [VP, VP, VP, VP],
     "icl_initDemagMatrices": [F, F, F, F, F, F, I],
     "icl_MVMult_GetH": [F, F, F, F, F, F, I, F],

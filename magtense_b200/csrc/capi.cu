@@ -1676,6 +1676,32 @@ int mt_batch_get_schedule(mt_batch* bt, int* ctas, int* order, int max_tiles, in
     return MT_OK;
 }
 
+static int batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_dev, double tol, double thres,
+                           const double* t_conv, int nt_conv, double conv_tol, double* t_out, double* y_out_dev,
+                           double* y_out_host, int* flags, mt_stats* stats, void* stream);
+
+int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_dev, double tol, double thres,
+                       const double* t_conv, int nt_conv, double conv_tol, double* t_out, double* y_out_dev,
+                       int* flags, mt_stats* stats, void* stream)
+{
+    return batch_integrate(bt, t, nt, m0_dev, tol, thres, t_conv, nt_conv, conv_tol, t_out, y_out_dev, nullptr, flags,
+                           stats, stream);
+}
+
+int mt_batch_integrate_host(mt_batch* bt, const double* t, int nt, const double* m0_dev, double tol, double thres,
+                            const double* t_conv, int nt_conv, double conv_tol, double* t_out, double* y_out_dev,
+                            double* y_out_host, int* flags, mt_stats* stats, void* stream)
+{
+    if (!y_out_dev || !y_out_host) return fail(MT_ERR_ARG, "y_out_dev and y_out_host are required");
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, y_out_host) != cudaSuccess || a.type != cudaMemoryTypeHost) {
+        cudaGetLastError();
+        return fail(MT_ERR_ARG, "y_out_host must be page-locked host memory (cudaHostAlloc / pinned)");
+    }
+    return batch_integrate(bt, t, nt, m0_dev, tol, thres, t_conv, nt_conv, conv_tol, t_out, y_out_dev, y_out_host,
+                           flags, stats, stream);
+}
+
 int mt_batch_demag_field(mt_batch* bt, const double* m_dev, double* H_dev, void* stream)
 {
     if (!bt || !m_dev || !H_dev) return fail(MT_ERR_ARG, "bad argument");
@@ -1701,9 +1727,12 @@ int mt_batch_demag_field(mt_batch* bt, const double* m_dev, double* H_dev, void*
     return MT_OK;
 }
 
-int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_dev, double tol, double thres,
-                       const double* t_conv, int nt_conv, double conv_tol, double* t_out, double* y_out_dev,
-                       int* flags, mt_stats* stats, void* stream)
+// y_out_host (page-locked, [B][nt][3n], or nullptr): the samples every instance has
+// finished are copied there after each launch, on a stream of their own, while the next
+// launch runs; the rest after the last launch.
+static int batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_dev, double tol, double thres,
+                           const double* t_conv, int nt_conv, double conv_tol, double* t_out, double* y_out_dev,
+                           double* y_out_host, int* flags, mt_stats* stats, void* stream)
 {
     if (!bt) return fail(MT_ERR_ARG, "null handle");
     int rc = check_ready(bt->h, true, false);
@@ -1830,6 +1859,22 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
         ~L2Guard() { if (on) { cudaCtxResetPersistingL2Cache(); cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, prev); } }
     } l2g{limit_set, prev_limit};
     long long last_sig = -1;
+    // streamed read-back of finished samples (y_out_host)
+    cudaStream_t cs2 = nullptr;
+    if (y_out_host) CUDA_TRY(cudaStreamCreateWithFlags(&cs2, cudaStreamNonBlocking));
+    struct CopyStream {
+        cudaStream_t s;
+        ~CopyStream() { if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); } }
+    } csg{cs2};
+    int k_sent = 0;   // samples 0 .. k_sent - 1 of every instance are on their way to the host
+    const size_t row = n3 * sizeof(double), pitch = (size_t)nt * row;
+    auto send = [&](int k_to) -> cudaError_t {
+        if (!y_out_host || k_to <= k_sent) return cudaSuccess;
+        cudaError_t e = cudaMemcpy2DAsync(y_out_host + (size_t)k_sent * n3, pitch, y_out_dev + (size_t)k_sent * n3, pitch,
+                                          (size_t)(k_to - k_sent) * row, (size_t)B, cudaMemcpyDeviceToHost, cs2);
+        if (e == cudaSuccess) k_sent = k_to;
+        return e;
+    };
     for (;;) {
         CUDA_TRY(cudaMemsetAsync(F.gs, 0, sizeof(GridSync), s));
         CUDA_TRY(cudaMemsetAsync(F.counters, 0, sizeof(unsigned) * 6, s));
@@ -1863,6 +1908,16 @@ int mt_batch_integrate(mt_batch* bt, const double* t, int nt, const double* m0_d
         if (all_done) break;
         if (sig == last_sig) return fail(MT_ERR_SOLVER, "batch integrator made no progress");
         last_sig = sig;
+        if (y_out_host) {   // samples below every unfinished instance's output index are final
+            int k_done = nt;
+            for (int b = 0; b < B; ++b)
+                if (hs[b].req != 3) k_done = std::min(k_done, hs[b].s.ko);
+            CUDA_TRY(send(k_done));
+        }
+    }
+    if (y_out_host) {
+        CUDA_TRY(send(nt));
+        CUDA_TRY(cudaStreamSynchronize(cs2));
     }
     std::vector<int> fl((size_t)Bp * nt);
     std::vector<double> to((size_t)Bp * nt);

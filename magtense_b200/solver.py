@@ -406,8 +406,12 @@ class BatchSolver:
         return out.view(self.B, 3, self.n)
 
     def integrate(self, t, m0, *, tol=1e-4, thres=1e-6, t_conv=None, conv_tol=1e-4, keep_trajectory=True,
-                  stream=None):
-        """Returns (t_out (B, nt), y_out (B, nt, 3n) cuda FP64 or None, flags (B, nt), stats list)."""
+                  host_out=None, stream=None):
+        """Returns (t_out (B, nt), y_out (B, nt, 3n) cuda FP64 or None, flags (B, nt), stats list).
+
+        host_out: a pinned CPU FP64 tensor (B, nt, 3n) that receives the trajectories as
+        the integration proceeds (finished samples after every relaunch, overlapped with
+        the next); it is then returned in place of the device trajectories."""
         t = _np_d(t).reshape(-1)
         nt = t.shape[0]
         m0 = torch.as_tensor(m0, dtype=torch.float64, device=self.device).reshape(self.B, 3 * self.n).contiguous()
@@ -417,6 +421,20 @@ class BatchSolver:
         t_out = np.zeros((self.B, nt))
         flags = np.zeros((self.B, nt), dtype=np.int32)
         st = (_lib.Stats * self.B)()
+        if host_out is not None:
+            if not (host_out.is_pinned() and host_out.dtype == torch.float64 and host_out.is_contiguous()
+                    and tuple(host_out.shape) == (self.B, nt, 3 * self.n)):
+                raise ValueError("host_out must be a contiguous pinned float64 tensor of shape (B, nt, 3n)")
+            if y_out is None:
+                y_out = torch.zeros((self.B, nt, 3 * self.n), dtype=torch.float64, device=self.device)
+            with torch.cuda.device(self.device):
+                rc = _lib.lib().mt_batch_integrate_host(
+                    self._h, t.ctypes.data_as(_lib.D), nt, _dptr(m0), float(tol), float(thres),
+                    tc.ctypes.data_as(_lib.D), tc.shape[0], float(conv_tol), t_out.ctypes.data_as(_lib.D),
+                    _dptr(y_out), C.c_void_p(host_out.data_ptr()), flags.ctypes.data_as(_lib.I), st,
+                    _stream(stream))
+            check(rc, "mt_batch_integrate_host")
+            return t_out, host_out, flags, [x.as_dict() for x in st]
         with torch.cuda.device(self.device):
             rc = _lib.lib().mt_batch_integrate(self._h, t.ctypes.data_as(_lib.D), nt, _dptr(m0), float(tol),
                                                float(thres), tc.ctypes.data_as(_lib.D), tc.shape[0], float(conv_tol),

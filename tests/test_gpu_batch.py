@@ -115,3 +115,51 @@ def test_batch_fp16s_trajectories(torch_cuda, oracle):
     worst, stats = run_batch_vs_oracle(torch_cuda, oracle, [20, 5, 1], [125e-9, 31.25e-9, 3e-9], B=6,
                                        precision="fp16s", window=0.1e-9, nt=21, atol=2e-5)
     print("fp16s worst |dm| vs oracle", worst)
+
+
+def test_host_streamed_trajectories_match_device(torch_cuda, monkeypatch):
+    """mt_batch_integrate_host: short launches (MT_BATCH_TICKS) make the host copies of
+    finished samples overlap later launches; the page-locked host trajectories equal the
+    device trajectories of the same integration bit for bit, and a pageable host buffer
+    is refused."""
+    import ctypes
+    from magtense_b200 import BatchSolver, _lib
+    torch = torch_cuda
+    monkeypatch.setenv("MT_BATCH_TICKS", "25")
+    res, L = [20, 5, 1], [125e-9, 31.25e-9, 3e-9]
+    n, B = 100, 6
+    rng = np.random.default_rng(31)
+    ang = rng.uniform(0, 2 * np.pi, B)
+    mag = rng.uniform(5e-3, 50e-3, B) / MU0
+    window = 0.05e-9
+    hext = np.zeros((B, 2, 4))
+    hext[:, 1, 0] = window
+    hext[:, :, 1] = (mag * np.cos(ang))[:, None]
+    hext[:, :, 2] = (mag * np.sin(ang))[:, None]
+    m = np.ones((B, 3, n)) / np.sqrt(3) + 0.05 * rng.standard_normal((B, 3, n))
+    m0 = torch.as_tensor((m / np.linalg.norm(m, axis=1, keepdims=True)).reshape(B, -1), device="cuda")
+    t = np.linspace(0, window, 26)
+    bs = BatchSolver(res, L, B, precision="int8")
+    bs.assemble()
+    bs.set_dynamics(hext=hext, alpha=GAMMA * 0.05, gamma=GAMMA)
+    t_dev, y_dev, f_dev, st_dev = bs.integrate(t, m0, tol=1e-6)
+    host = torch.empty((B, len(t), 3 * n), dtype=torch.float64).pin_memory()
+    t_h, y_h, f_h, st_h = bs.integrate(t, m0, tol=1e-6, host_out=host)
+    assert y_h is host and st_h[0]["launches"] > 3
+    assert np.array_equal(t_h, t_dev) and np.array_equal(f_h, f_dev)
+    assert torch.equal(host, y_dev.cpu())
+    with pytest.raises(ValueError):
+        bs.integrate(t, m0, tol=1e-6, host_out=torch.empty((B, len(t), 3 * n), dtype=torch.float64))
+    pageable = np.zeros((B, len(t), 3 * n))
+    y_tmp = torch.zeros((B, len(t), 3 * n), dtype=torch.float64, device="cuda")
+    t_out = np.zeros((B, len(t)))
+    flags = np.zeros((B, len(t)), dtype=np.int32)
+    st = (_lib.Stats * B)()
+    tc = np.zeros(1)
+    rc = _lib.lib().mt_batch_integrate_host(bs._h, t.ctypes.data_as(_lib.D), len(t), ctypes.c_void_p(m0.data_ptr()),
+                                            1e-6, 1e-6, tc.ctypes.data_as(_lib.D), 0, 1e-4,
+                                            t_out.ctypes.data_as(_lib.D), ctypes.c_void_p(y_tmp.data_ptr()),
+                                            ctypes.c_void_p(pageable.ctypes.data), flags.ctypes.data_as(_lib.I), st,
+                                            ctypes.c_void_p(0))
+    assert rc == -1   # MT_ERR_ARG
+    bs.close()
