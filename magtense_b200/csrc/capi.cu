@@ -116,6 +116,20 @@ void axis_setup(int nn, double L, double* d)
     *d = (nn > 1) ? L / nn : L;
 }
 
+// Fraction of a dense tensor of `bytes` that the streaming demag loads mark L2 evict_last:
+// enough of it to fill 80 % of one die's half of L2, so that the lines kept survive the
+// evaluation's sweep over the rest; 0 when that is under 5 % of the tensor.
+float l2_keep_fraction(int device, double bytes)
+{
+    int l2 = 0;
+    if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device) != cudaSuccess || l2 <= 0 || bytes <= 0.0) {
+        cudaGetLastError();
+        return 0.f;
+    }
+    const double f = std::min(1.0, 0.8 * 0.5 * (double)l2 / bytes);
+    return f < 0.05 ? 0.f : (float)f;
+}
+
 DevProb make_prob(const mt_handle* h)
 {
     DevProb P;
@@ -135,6 +149,7 @@ DevProb make_prob(const mt_handle* h)
     P.hext = h->hext; P.alpha_tab = h->alpha_tab;
     P.gamma = h->gamma; P.alpha0 = h->alpha0;
     P.sp_rowptr = h->sp_rowptr; P.sp_col = h->sp_col; P.sp_val = h->sp_val;
+    P.l2_keep = l2_keep_fraction(h->device, 24.0 * (double)(h->shard_world > 1 ? h->shard_ncell : h->n) * h->ldk);
     return P;
 }
 
@@ -976,6 +991,8 @@ static int integrate_single(mt_handle* h, const double* t, int nt, const double*
     int prc = integ_prepare(h, t, nt, m0_dev, tol, thres, t_conv, nt_conv, conv_tol, y_out_dev, grid0, R, stats, s);
     if (prc) return prc;
     DevProb P = R.P;
+    // the tensor lines kept in L2 (evict_last) return to normal priority when the run ends
+    struct L2Reset { bool on; ~L2Reset() { if (on) cudaCtxResetPersistingL2Cache(); } } l2r{P.l2_keep > 0.f};
     IntegBufs& B = R.B;
     IntegParams& Q = R.Q;
     const int grid = R.grid;
@@ -1074,6 +1091,12 @@ int mt_integrate_ragged(mt_handle* const* hs, int ninst, const double* t, int nt
         const double t_eval = 24.0 * (double)hs[k]->n * (double)hs[k]->ldk / (ncta[k] * 30.0e9) + 15e-6;
         runs[k]->Q.evals_per_launch = std::min(100000LL, std::max(64LL, (long long)(0.25 / t_eval)));
     }
+    // the L2 evict_last share of the loads, for the tensors of all instances together
+    double tensor_bytes = 0.0;
+    for (int k = 0; k < ninst; ++k) tensor_bytes += 24.0 * (double)hs[k]->n * (double)hs[k]->ldk;
+    const float keep = l2_keep_fraction(hs[0]->device, tensor_bytes);
+    for (int k = 0; k < ninst; ++k) runs[k]->P.l2_keep = keep;
+    struct L2Reset { bool on; ~L2Reset() { if (on) cudaCtxResetPersistingL2Cache(); } } l2r{keep > 0.f};
     std::vector<GroupBack> back;
     long long launches = 0;
     double kernel_ms = 0.0;
@@ -1746,6 +1769,7 @@ static int batch_integrate(mt_batch* bt, const double* t, int nt, const double* 
     const int n = h->n, B = bt->B;
     const size_t n3 = 3 * (size_t)n;
     for (int b = 0; b < B; ++b) { memset(&stats[b], 0, sizeof(mt_stats)); stats[b].converged_at = -1; }
+    cudaCtxResetPersistingL2Cache();   // no tensor lines of an earlier single-instance field call stay kept in L2
     const double eps = 2.220446049250313e-16;
     const double round_off = 10.0 * eps, sqrrmc = sqrt(eps), cubrmc = pow(eps, 1.0 / 3.0);
     const double sqtiny = sqrt(2.2250738585072014e-308);
