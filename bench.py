@@ -36,9 +36,11 @@ on the same workload, rank 0 only: the instances side by side on the host cores,
 one single-threaded process each, as the reference runs one problem per thread.
 
 Besides the headline, the default film-batch line carries the FP64 error of
-<m>(t) for a seeded sample of instances ("m_err_vs_fp64"), the large-plain HBM
-record ("large_plain") and the split 16-bit product next to int8 on a short
-window ("split16_short_window").
+<m>(t) for a seeded sample of instances ("m_err_vs_fp64"), the film-plain path on
+those instances ("plain_fp32_same_workload"), the large-plain HBM record
+("large_plain"), the ragged and adjoint configurations ("ragged", "adjoint")
+and the split 16-bit product next to int8 on a short window
+("split16_short_window").
 """
 from __future__ import annotations
 
@@ -94,6 +96,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3, help="end-to-end repetitions (median reported)")
     ap.add_argument("--no-fp64", action="store_true", help="film-batch: skip the FP64 error statement")
     ap.add_argument("--no-large", action="store_true", help="film-batch: skip the large-plain sub-record")
+    ap.add_argument("--no-others", action="store_true",
+                    help="film-batch: skip the ragged, adjoint and precision-study sub-records")
     ap.add_argument("--no-tune", action="store_true", help="film-batch: keep the default GEMM schedule")
     ap.add_argument("--no-split16", action="store_true",
                     help="film-batch: skip the short-window record of the split 16-bit product")
@@ -484,6 +488,177 @@ def large_plain_record(torch, hbm, src, local, reps=3):
             "clocks": clocks}
 
 
+def ragged_record(torch, hbm, src, local, window_ns=0.05, reps=2):
+    """The ragged configuration (64 films of the seeded sizes, each its own tensor and
+    field, one graph-replayed persistent launch on per-instance SM groups): device time
+    of whole integrations of the set after a warm-up, as tensor GB/s."""
+    from magtense_b200 import Solver, integrate_ragged
+    sizes = ragged_sizes(2, 64)
+    fields = instance_fields(1000, 64)
+    win = window_ns * 1e-9
+    t = np.linspace(0, win, int(round(window_ns / 1e-3)) + 1)
+    solvers, m0s = [], []
+    try:
+        for (res, L), h in zip(sizes, fields):
+            s = Solver(res, L)
+            solvers.append(s)
+            s.assemble()
+            s.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.02, hext=np.array([[0.0, *h], [win, *h]]))
+            m0s.append(torch.as_tensor(start_state(int(np.prod(res))), device="cuda"))
+        integrate_ragged(solvers, t, m0s, tol=1e-6, graph=True)   # warm-up (graph capture)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        runs = []
+        with Clocks(local) as clk:
+            for _ in range(reps):
+                torch.cuda.synchronize()
+                ev0.record()
+                _, ys, _, st = integrate_ragged(solvers, t, m0s, tol=1e-6, graph=True)
+                ev1.record()
+                torch.cuda.synchronize()
+                runs.append((ev0.elapsed_time(ev1), st))
+                del ys
+        clocks = clk.summary()
+        ns = [s.n for s in solvers]
+    finally:
+        for s in solvers:
+            s.close()
+    step_ms = statistics.median(r[0] for r in runs)
+    st = runs[-1][1]
+    evals = [x["f_evals"] for x in st]
+    kms = st[0]["kernel_ms"]
+    gbs = sum(24.0 * x * x * e for x, e in zip(ns, evals)) / (kms / 1e3) / 1e9
+    return {"workload": f"ragged: 64 films, nx ~ U{{20..120}}, ny = nx/4, 6.25x6.25x3 nm cells (n {min(ns)}..{max(ns)},"
+                        f" {sum(24 * x * x for x in ns) / 1e9:.2f} GB of FP32 tensors), seeded in-plane fields, "
+                        f"{window_ns} ns each, tol 1e-6, output every 1 ps; one persistent launch sequence on "
+                        "per-instance SM groups, replayed from a CUDA graph",
+            "value": 64 * window_ns / (step_ms / 1e3), "unit": "simulated ns/s", "ms_per_step": step_ms,
+            "rhs_evals_per_instance": {"min": int(min(evals)), "median": float(np.median(evals)), "max": int(max(evals))},
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                         "traffic": None,
+                         "note": f"integrate_ragged_kernel: sum over instances of 24*n_k^2 tensor bytes x evaluations "
+                                 f"over {kms:.1f} ms of device time; peak {src} HBM copy"},
+            "gpu_launches": int(st[0]["launches"]), "clocks": clocks}
+
+
+def adjoint_record(torch, hbm, src, local, reps=2):
+    """The differentiation configuration: forward and adjoint backward of the 2 ns
+    fixed-step RK4 trajectory (200 field segments, per-cell Ms), CUDA-event time of whole
+    steps after a warm-up."""
+    from magtense_b200 import TrajectoryProblem, mean_m_trajectory
+    n = int(np.prod(FILM_RES))
+    hseg, Ms, m0, tg = adjoint_config(4)
+    prob = TrajectoryProblem(FILM_RES, FILM_L, gamma=GAMMA, alpha=GAMMA * 0.02, m0=m0, t_seg=10e-12,
+                             steps_per_segment=10, sample_every=10, checkpoint_every=50)
+    steps = hseg.shape[0] * prob.steps_per_segment
+    tt = prob.dt * prob.sample_every * np.arange(1, steps // prob.sample_every + 1)
+    tgt = torch.as_tensor(adjoint_target(tt, tg), device="cuda")
+
+    def step():
+        hs = torch.as_tensor(hseg, device="cuda").requires_grad_(True)
+        ms = torch.as_tensor(Ms, device="cuda").requires_grad_(True)
+        loss = ((mean_m_trajectory(hs, ms, prob)[:, 0] - tgt) ** 2).sum()
+        loss.backward()
+        return hs.grad, ms.grad
+
+    step()   # warm-up (graph capture of the replayed steps)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times = []
+    with Clocks(local) as clk:
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            ev0.record()
+            step()
+            ev1.record()
+            torch.cuda.synchronize()
+            times.append(ev0.elapsed_time(ev1))
+    clocks = clk.summary()
+    step_ms = statistics.median(times)
+    rhs_like = steps * (4 + 4 + 2 * 4)
+    gbs = 24.0 * n * n * rhs_like / (step_ms / 1e3) / 1e9
+    return {"workload": "adjoint: 80x20x1 film, per-cell Ms ~ U[7.5e5, 8.5e5], 200 piecewise-constant in-plane field "
+                        "segments over 2 ns, fixed-step RK4 dt = 1 ps; one step = forward + adjoint backward "
+                        "(gradients for the 600 field values and 1600 Ms values)",
+            "value": 2.0 / (step_ms / 1e3), "unit": "simulated ns/s", "ms_per_step": step_ms,
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                         "traffic": None,
+                         "note": f"field_kernel streaming demag: 24*n^2 bytes x {rhs_like} products per step over the "
+                                 f"whole step time (the 61 MB tensor sits in L2); peak {src} HBM copy"},
+            "clocks": clocks}
+
+
+def sweep_state(seed, B=512, n=4096):
+    """The precision configuration's inputs: mu0 H along x swept from -100 to +100 mT over
+    the B instances, each tilted in plane by a seeded +-1 degree, and a shared seeded state
+    (1, 0.2, 0) + N(0, 0.1^2) per component, renormalised."""
+    rng = np.random.default_rng(seed)
+    mag = np.linspace(-100e-3, 100e-3, B) / MU0
+    tilt = np.deg2rad(1.0) * rng.choice([-1.0, 1.0], B)
+    fields = np.stack([mag * np.cos(tilt), mag * np.sin(tilt), np.zeros(B)], 1)
+    m = np.array([1.0, 0.2, 0.0])[:, None] + 0.1 * rng.standard_normal((3, n))
+    return fields, (m / np.linalg.norm(m, axis=0)).reshape(-1)
+
+
+def precision_record(torch, local, window_ns=0.005, precisions=("int8", "fp16s", "bf16x3", "fp32")):
+    """The precision configuration (128x32x1 film of 4x4x3 nm cells, n = 4096, 512
+    quasi-static field steps relaxing at alpha_G = 1 from a shared state): the batched
+    integration with each demag precision over a short window, simulated ns/s from device
+    time, and the H_d error of each precision's product against FP64 on seeded rows."""
+    from magtense_b200 import BatchSolver
+    from oracle import oracle as O
+    res, L = (128, 32, 1), (512e-9, 128e-9, 3e-9)
+    n, B = 4096, 512
+    fields, m_sh = sweep_state(3, B, n)
+    win = window_ns * 1e-9
+    t = np.linspace(0, win, int(round(window_ns / 1e-3)) + 1)
+    hext = np.zeros((B, 2, 4))
+    hext[:, 1, 0] = win
+    hext[:, :, 1:] = fields[:, None, :]
+    m0 = torch.as_tensor(np.tile(m_sh, (B, 1)), device="cuda")
+    # H_d check: per instance the shared state rotated in plane by a seeded angle; 256 seeded
+    # receiver rows of the FP64 tensor, 8 of the instances
+    rng = np.random.default_rng(4)
+    ang = rng.uniform(-np.pi, np.pi, B)
+    base = m_sh.reshape(3, n)
+    c, s = np.cos(ang)[:, None], np.sin(ang)[:, None]
+    mh = np.stack([c * base[0] - s * base[1], s * base[0] + c * base[1], np.broadcast_to(base[2], (B, n))], 1)
+    rows = np.sort(rng.choice(n, 256, replace=False))
+    check = np.linspace(0, B - 1, 8).astype(int)
+    _, K64 = O.assemble(list(res), list(L), rows=rows, fp32=False, fp64=True)
+    Href = np.stack([O.demag_rows(None, K64, mh[b], 8e5, mode=1) for b in check])
+    mh_dev = torch.as_tensor(mh.reshape(B, -1), device="cuda")
+    out = {}
+    with Clocks(local) as clk:
+        for prec in precisions:
+            bs = BatchSolver(res, L, B, precision=prec)
+            try:
+                bs.assemble()
+                H = bs.demag_field(mh_dev).cpu().numpy().reshape(B, 3, n)
+                herr = float(np.abs(H[check][:, :, rows] - Href).max() / np.abs(Href).max())
+                bs.set_dynamics(hext=hext, alpha=GAMMA * 1.0, gamma=GAMMA)
+                bs.integrate(t, m0, tol=1e-6)   # warm-up
+                torch.cuda.synchronize()
+                _, y, _, st = bs.integrate(t, m0, tol=1e-6)
+                torch.cuda.synchronize()
+                del y
+            finally:
+                bs.close()
+            ev = [x["f_evals"] for x in st]
+            kms = st[0]["kernel_ms"]
+            out[prec] = {"value": B * window_ns / (kms / 1e3), "unit": "simulated ns/s", "kernel_ms": kms,
+                         "rhs_evals_per_instance": {"min": int(min(ev)), "median": float(np.median(ev)),
+                                                    "max": int(max(ev))},
+                         "h_d_err_vs_fp64": herr}
+    out["workload"] = (f"precision: 128x32x1 film of 4x4x3 nm cells (n = 4096), {B} instances, mu0 H along x swept "
+                       f"-100..+100 mT, each tilted by a seeded 1 degree, relaxing at alpha_G = 1 from a shared seeded "
+                       f"state, tol 1e-6, {window_ns} ns, output every 1 ps")
+    out["note"] = ("device time of one integration per precision after a warm-up; h_d_err_vs_fp64 = max over 8 "
+                   "instances, 3 components and 256 seeded receiver rows of |H - H_FP64| / max |H_FP64| for a "
+                   "seeded in-plane rotation of the state per instance (FP64 rows from the oracle, outside the "
+                   "timed region); the <m>(t) error of these precisions on this geometry is checked in the tests")
+    out["clocks"] = clk.summary()
+    return out
+
+
 def split16_record(torch, res, L, m_s, fields, window_ns=0.02, precisions=("fp16s", "int8")):
     """The split 16-bit form of the batched product next to int8 on the same instances
     over a short window: simulated ns/s from device time, RHS evaluations per instance.
@@ -556,7 +731,7 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
     # of this rank's set, each integrated over the same window, one after another (before the
     # batched timing, on an idle device)
     pick = sorted(int(k) for k in np.random.default_rng(7).choice(B, size=min(args.plain_sample, B), replace=False))
-    plain_s, plain_evals, plain_m = 0.0, 0, []
+    plain_s, plain_evals, plain_kms, plain_m = 0.0, 0, 0.0, []
     for k in pick:
         plain.set_dynamics(solver=2, gamma=GAMMA, alpha=GAMMA * 0.02,
                            hext=np.array([[0.0, *fields[k]], [win, *fields[k]]]))
@@ -566,6 +741,7 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
         torch.cuda.synchronize()
         plain_s += time.perf_counter() - t0
         plain_evals += pst["f_evals"]
+        plain_kms += pst["kernel_ms"]
         plain_m.append((tp, yp.view(nt, 3, n).mean(dim=2).cpu().numpy()))
         del yp
     plain_rate = len(pick) * window / plain_s
@@ -621,9 +797,19 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
                                    "median": float(np.median([x["f_evals"] for x in stats[-1]])),
                                    "max": int(max(x["f_evals"] for x in stats[-1]))},
         "plain_fp32_same_workload": {"value": plain_rate, "unit": "simulated ns/s",
-                                     "rhs_evals": plain_evals, "instances": pick,
-                                     "note": f"single-instance FP32 path (the reference's arithmetic) on {len(pick)} "
-                                             f"seeded instances of the same set, {window} ns each, one after another"},
+                                     "rhs_evals": plain_evals, "instances": pick, "kernel_ms": plain_kms,
+                                     "us_per_eval": plain_kms * 1e3 / plain_evals,
+                                     "roofline": {"bound": "hbm", "unit": "GB/s", "peak": hbm,
+                                                  "achieved": 24.0 * n * n * plain_evals / (plain_kms / 1e3) / 1e9,
+                                                  "frac": 24.0 * n * n * plain_evals / (plain_kms / 1e3) / 1e9 / hbm,
+                                                  "traffic": None,
+                                                  "note": f"integrate_kernel (film-plain): 24*n^2 tensor bytes per "
+                                                          f"RHS evaluation over {plain_kms:.1f} ms of device time; the "
+                                                          f"61.4 MB tensor is served mostly from L2 (part of its lines "
+                                                          f"kept with evict_last); peak {src} HBM copy"},
+                                     "note": f"film-plain: the single-instance FP32 path (the reference's arithmetic) "
+                                             f"on {len(pick)} seeded instances of the same set, {window} ns each, one "
+                                             f"after another"},
         "batched_over_plain": value / ws / plain_rate,
         "gemm_schedule": {"tuned": not args.no_tune, "tuning_s": round(tune_s, 3),
                           "per_active_tiles": [{"tiles": k, "streamk_ctas": g, "order": o} for k, g, o in sched],
@@ -647,6 +833,10 @@ def bench_film_batch(torch, args, ws, rank, local, dist, hbm, peak_tf, src):
                     "the FP64 tensor and FP64 demag product, same s-state, field and tolerances, run after timing"}
     if not args.no_large:
         line["large_plain"] = large_plain_record(torch, hbm, src, local)
+    if not args.no_others:
+        line["ragged"] = ragged_record(torch, hbm, src, local)
+        line["adjoint"] = adjoint_record(torch, hbm, src, local)
+        line["precision_study"] = precision_record(torch, local)
     if not args.no_split16 and args.precision == "int8":
         bs.close()
         line["split16_short_window"] = split16_record(torch, res, L, m_s, fields)

@@ -7,9 +7,10 @@ product, all against the FP64 oracle:
 
 - H_d error: 256 seeded receiver rows of the FP64 tensor, for 16 of the 512
   instances, relative to the largest component;
-- <m>(t) error: the same sweep on the 20x5x1 film (the FP64 oracle integrates
-  it in seconds), 0.05 ns at alpha_G = 1 from a shared seeded state, every
-  output sample of 4 instances.
+- <m>(t) error: the same sweep on the 20x5x1 film, 0.05 ns at alpha_G = 1 from
+  a shared seeded state, every output sample of 4 instances (all five
+  precisions); and on the 128x32x1 film itself, all 512 instances over
+  0.005 ns, both ends of the sweep against the FP64 oracle (all but bf16x2).
 
 Bounds (the measured values are printed): H_d fp32 2e-5 (the reference's own
 FP32 arithmetic), bf16x3 1e-4, bf16x2 1e-2, fp16s 1e-4 (small entries of a row
@@ -168,3 +169,54 @@ def test_headline_geometry_mean_m_error_vs_fp64(torch_cuda, oracle):
             worst[name] = max(worst[name], float(np.abs(yg[same] - y_r[same]).max()))
     print(f"80x20x1, 4 instances, 0.1 ns: max |<m> - <m>_FP64| {worst}")
     assert worst["int8"] <= 1e-4 and worst["fp32"] <= 1e-4, worst
+
+
+def test_precision_config_geometry_mean_m_error(torch_cuda, oracle):
+    """<m>(t) error on the precision configuration's own geometry: the 128x32x1 film
+    (n = 4096), all 512 sweep instances relaxing at alpha_G = 1 from the shared state
+    over 0.005 ns (output every 1 ps), each batched precision against the FP64 oracle
+    at both ends of the sweep (-100 and +100 mT).  bf16x2 (1e-2 class) is covered on
+    the 20x5x1 film above."""
+    from magtense_b200 import BatchSolver
+    res, L = [128, 32, 1], [512e-9, 128e-9, 3e-9]
+    n, B = 4096, 512
+    win = 0.005e-9
+    Hf = sweep_fields(B, 5)
+    m_sh = shared_state(n, 6).reshape(-1)
+    hext = np.zeros((B, 2, 4))
+    hext[:, 1, 0] = win
+    hext[:, :, 1:] = Hf[:, None, :]
+    t = np.linspace(0, win, 6)
+    check = [0, B - 1]
+    _, K64 = oracle.assemble(res, L, fp32=False, fp64=True)
+    ref = {}
+    for b in check:
+        P = oracle.Problem(res, L, mode=1, gamma=GAMMA, alpha=GAMMA * 1.0, hext=hext[b], K64=K64)
+        to, yo, _, _ = P.solve(t, m_sh, tol=1e-6)
+        ref[b] = (to, yo.reshape(len(t), 3, n).mean(axis=2))
+    del K64
+    m0 = torch_cuda.as_tensor(np.tile(m_sh, (B, 1)), device="cuda")
+    errs, matched = {}, {}
+    for prec in ("fp32", "bf16x3", "fp16s", "int8"):
+        bs = BatchSolver(res, L, B, precision=prec)
+        bs.assemble()
+        bs.set_dynamics(hext=hext, alpha=GAMMA * 1.0, gamma=GAMMA)
+        t_out, y, _, _ = bs.integrate(t, m0, tol=1e-6)
+        y = y.view(B, len(t), 3, n)[check].mean(dim=3).cpu().numpy()
+        bs.close()
+        e = 0.0
+        for k, b in enumerate(check):
+            to, mref = ref[b]
+            same = t_out[b] == to
+            matched[prec] = min(matched.get(prec, 1.0), float(same.mean()))
+            # bf16x3's FP32-accumulated rounding noise drives the step size down on this
+            # geometry (about 10^4 evaluations per instance against 600 for int8), so
+            # RKSUITE's 5000-evaluation return displaces the later samples (flag 3): only
+            # the samples at equal times compare
+            assert same.mean() > (0.5 if prec == "bf16x3" else 0.8), (prec, b)
+            e = max(e, float(np.abs(y[k][same] - mref[same]).max()))
+        errs[prec] = e
+    print("\n<m>(t) error vs FP64 (128x32x1, 512 instances, 0.005 ns, alpha_G = 1):",
+          {k: f"{v:.2e}" for k, v in errs.items()}, "samples at the requested times:", matched)
+    for prec, e in errs.items():
+        assert e <= M_BOUND[prec], (prec, e)
