@@ -10,8 +10,9 @@
 enum { KERR_NONE = 0, KERR_BARRIER_TIMEOUT = 1, KERR_BAD_CONFIG = 2, KERR_RANGE = 3, KERR_PEER_TIMEOUT = 4,
        KERR_PEER_ABORT = 5 };
 
-// Grid-wide barrier state for the persistent cooperative kernels.  count is
-// reset to 0 by the host before every launch.
+// Grid-wide barrier state for the persistent cooperative kernels.  The host
+// zeroes it before every launch (count then holds the arrivals of the launch so
+// far; gen is unused).
 struct GridSync {
     unsigned int count;
     unsigned int gen;
@@ -67,17 +68,17 @@ MT_DEV bool group_sync(GridSync* gs, unsigned nctas, int where)
         if (ld_volatile_i32(&gs->abort)) {
             ok = 0;
         } else {
-            unsigned g = ld_acquire_u32(&gs->gen);
+            // count only grows within a launch: every CTA arrives at barrier k before any
+            // CTA can arrive at barrier k + 1, so the arrivals at barrier k return values in
+            // [k nctas, (k + 1) nctas) and the barrier is complete once count reaches
+            // (k + 1) nctas; the last arriver needs no reset and no second store
             __threadfence();
-            unsigned prev = atomicAdd(&gs->count, 1u);
-            if (prev == nctas - 1) {
-                atomicExch(&gs->count, 0u);
-                __threadfence();
-                st_release_u32(&gs->gen, g + 1u);
-            } else {
+            const unsigned prev = atomicAdd(&gs->count, 1u);
+            const unsigned target = (prev / nctas + 1u) * nctas;
+            if (prev + 1u != target) {
                 long long it = 0;
                 uint64_t t0 = globaltimer_ns();
-                while (ld_acquire_u32(&gs->gen) == g) {
+                while (ld_acquire_u32(&gs->count) < target) {
                     if (ld_volatile_i32(&gs->abort)) { ok = 0; break; }
                     if (++it > kSpinLimit || (it & 1023) == 0 && globaltimer_ns() - t0 > kTimeoutNs) {
                         if (atomicCAS(&gs->err, 0, KERR_BARRIER_TIMEOUT) == 0) gs->err_where = where;
