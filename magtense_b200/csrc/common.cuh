@@ -42,6 +42,12 @@ MT_DEV void st_release_sys_u32(unsigned* p, unsigned v)
 {
     asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+MT_DEV unsigned atom_add_acq_rel_u32(unsigned* p, unsigned v)
+{
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
 MT_DEV int ld_volatile_i32(const int* p) { return *(volatile const int*)p; }
 MT_DEV uint64_t globaltimer_ns()
 {
@@ -72,8 +78,9 @@ MT_DEV bool group_sync(GridSync* gs, unsigned nctas, int where)
             // CTA can arrive at barrier k + 1, so the arrivals at barrier k return values in
             // [k nctas, (k + 1) nctas) and the barrier is complete once count reaches
             // (k + 1) nctas; the last arriver needs no reset and no second store
-            __threadfence();
-            const unsigned prev = atomicAdd(&gs->count, 1u);
+            // acq_rel: releases the CTA's writes (ordered before by the __syncthreads above)
+            // and, for the last arriver, acquires everyone else's
+            const unsigned prev = atom_add_acq_rel_u32(&gs->count, 1u);
             const unsigned target = (prev / nctas + 1u) * nctas;
             if (prev + 1u != target) {
                 long long it = 0;
@@ -89,7 +96,6 @@ MT_DEV bool group_sync(GridSync* gs, unsigned nctas, int where)
                     __nanosleep(32);
                 }
             }
-            __threadfence();
         }
         s_ok = ok;
     }
