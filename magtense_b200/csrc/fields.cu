@@ -86,7 +86,7 @@ field_kernel(DevProb P, const double* __restrict__ m, const float* __restrict__ 
     const int c0 = blockIdx.x * cells_per_cta;
     const int nc = min(cells_per_cta, P.n - c0);
     if (nc <= 0) return;
-    demag_cta(P, m32, c0, nc, sm_m, sm_part, sm_S);
+    demag_cta(P, m32, c0, nc, sm_m, sm_part, sm_S, 2);
     const int n = P.n;
     if (MODE == 3) {   // raw product H = pref * K m (FP32), reference shim
         for (int e = threadIdx.x; e < 3 * nc; e += blockDim.x) {

@@ -176,7 +176,7 @@ MT_DEV void feval(Ctx& X, RKS& s, double t, int argi, double* out)
 {
     const double* arg = X.B.pool[argi];
     const float* arg32 = X.B.pool32[argi];
-    demag_cta(X.P, arg32, X.c0, X.nc, X.sm_m, X.sm_part, X.sm_S);
+    demag_cta(X.P, arg32, X.c0, X.nc, X.sm_m, X.sm_part, X.sm_S, 5);
     const TimeScalars ts = time_scalars(X.P, t);
     const int n = X.P.n;
     for (int cell = threadIdx.x; cell < X.nc; cell += blockDim.x) {

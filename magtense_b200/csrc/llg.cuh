@@ -349,8 +349,12 @@ MT_DEV void demag_units(const DevProb& P, int c0, int ch0, int len, int nseg, in
     }
 }
 
+// units_per_warp sets how many (cell, segment) units a chunk aims for per warp: more,
+// shorter segments cost more rounds of the unit loop but shorten the FP32 running sums
+// of every lane.  The integrators take 5 (the noise of the product sets RKSUITE's
+// step size), the stand-alone field kernel 2.
 MT_DEV void demag_cta(const DevProb& P, const float* __restrict__ m32, int c0, int nc, float* sm_m,
-                      float* sm_part, float* S_out)
+                      float* sm_part, float* S_out, int units_per_warp)
 {
     if (P.sp_rowptr) { demag_cta_sparse(P, m32, c0, nc, sm_m, S_out); return; }
     const int ldk = P.ldk;
@@ -360,7 +364,7 @@ MT_DEV void demag_cta(const DevProb& P, const float* __restrict__ m32, int c0, i
     for (int ch0 = 0; ch0 < ldk; ch0 += JC) {
         const int len = min(JC, ldk - ch0);          // multiple of 4
         // segments: enough units to keep all warps busy, each a multiple of 128 floats
-        int nseg = (2 * nwarps + nc - 1) / max(nc, 1);
+        int nseg = (units_per_warp * nwarps + nc - 1) / max(nc, 1);
         if (nseg < 1) nseg = 1;
         int seglen = (len + nseg - 1) / nseg;
         seglen = (seglen + 127) & ~127;
