@@ -1395,6 +1395,17 @@ MT_DEV void gemm_tile_simt(const BCtx& X)
 
 constexpr int kMaxInstPerWarp = 8;
 
+// Estimated work of advancing a served coroutine to its next request, in FP64 vectors its
+// loops stream: after stage i of a step the stage-(i+1) argument (i + 2 vectors); after
+// the last stage the error estimate, the step's end and the next step's first argument;
+// after an interpolation stage the next one, or the interpolant and its outputs.
+MT_DEV int advance_weight(const BInst& I)
+{
+    if (I.pc == L_STAGE) return I.i_stage >= 8 ? 24 : I.i_stage + 3;
+    if (I.pc >= L_INTERP + 1000) return 16;
+    return 8;
+}
+
 // Publish the state of the warp's coroutines for tick tk: active instances and
 // right-hand-side requests (per 64-instance tile, and as request bits for the int8
 // packing), counted once per instance by its cell block 0.  Slot tk % 3 was cleared
@@ -1477,7 +1488,7 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
     BInst L_loc[kMaxInstPerWarp];
     BInst* Lsm = Q.inst_smem_off ? reinterpret_cast<BInst*>(smem_raw + Q.inst_smem_off) : nullptr;
     BInst* L = Lsm ? Lsm + (size_t)X.warp * Q.inst_per_warp : L_loc;
-    __shared__ int s_adv[kInstBlock], s_nadv;
+    __shared__ int s_adv[kInstBlock], s_adv_w[kInstBlock], s_wt[kInstBlock], s_nadv;
     int mine = 0;
     for (int li = X.warp; li < X.ni && mine < kMaxInstPerWarp; li += X.nwarps, ++mine) {
         const long long* src = reinterpret_cast<const long long*>(&F.inst[(size_t)X.cb * Q.Bp + X.i0 + li]);
@@ -1572,13 +1583,31 @@ batch_kernel(DevProb P, BatchBufs F, BatchParams Q, const __grid_constant__ TcMa
                     const bool need = li < X.ni && X.i0 + li < Q.B &&
                                       Lsm[(li % X.nwarps) * Q.inst_per_warp + li / X.nwarps].req == 0;
                     const unsigned bal = __ballot_sync(0xffffffffu, need);
-                    if (need) s_adv[cnt + __popc(bal & ((1u << X.lane) - 1u))] = li;
+                    if (need) s_adv_w[cnt + __popc(bal & ((1u << X.lane) - 1u))] = li;
                     cnt += __popc(bal);
+                }
+                __syncwarp();
+                // Heaviest first: each coroutine's work up to its next request, estimated from
+                // where it resumes (the vectors its next loops stream), ranks the served ones;
+                // ties keep index order.  The states, and so the order, are the same in every
+                // cell-block copy of the instances.
+                for (int k = X.lane; k < cnt; k += 32) s_wt[k] = advance_weight(Lsm[(s_adv_w[k] % X.nwarps) *
+                                                                                    Q.inst_per_warp + s_adv_w[k] / X.nwarps]);
+                __syncwarp();
+                for (int k = X.lane; k < cnt; k += 32) {
+                    int r = 0;
+                    for (int o = 0; o < cnt; ++o)
+                        r += (s_wt[o] > s_wt[k]) || (s_wt[o] == s_wt[k] && o < k);
+                    s_adv[r] = s_adv_w[k];
                 }
                 if (X.lane == 0) s_nadv = cnt;
             }
             __syncthreads();
-            for (int j = X.warp; j < s_nadv; j += X.nwarps) {
+            // dealt in snake order (warp w takes ranks w, 2 nw - 1 - w, 2 nw + w, ...), so a
+            // warp's heavy coroutine of one round pairs with a light one of the next
+            for (int r = 0; r * X.nwarps < s_nadv; ++r) {
+                const int j = r * X.nwarps + ((r & 1) ? X.nwarps - 1 - X.warp : X.warp);
+                if (j >= s_nadv) continue;
                 const int li = s_adv[j];
                 BInst& I = Lsm[(li % X.nwarps) * Q.inst_per_warp + li / X.nwarps];
                 const uint64_t ta = (F.prof && t == 0 && threadIdx.x == 0) ? globaltimer_ns() : 0;
