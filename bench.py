@@ -69,8 +69,8 @@ FILM_L = (500e-9, 125e-9, 3e-9)
 TRAFFIC_PER_TENSOR_BYTE = (43.906 + 0.065) / 43.89
 # DRAM bytes (read + write) per lock-step tick of the batched integrator with all four
 # 64-instance tiles active, from an ncu capture of the first 200 ticks of the headline
-# workload (39.440 GB read + 11.873 GB written); ticks per full launch of the kernel
-BATCH_TRAFFIC_PER_TICK = (39.440e9 + 11.873e9) / 200
+# workload (38.142 GB read + 11.452 GB written); ticks per full launch of the kernel
+BATCH_TRAFFIC_PER_TICK = (38.142e9 + 11.452e9) / 200
 BATCH_TICKS_PER_LAUNCH = 4000
 LARGE_RES = (64, 64, 8)
 LARGE_L = (320e-9, 320e-9, 40e-9)
